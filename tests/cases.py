@@ -1,0 +1,98 @@
+"""Shared construction of the golden cases from the committed fixture specs."""
+
+from __future__ import annotations
+
+import json
+from pathlib import Path
+
+import numpy as np
+
+from proton_dose_m1_b200 import Beam, Box, Geometry, Numerics, Physics, SolverConfig
+from proton_dose_m1_b200.enums import (CoefficientInterpolation, EnergyScheme, Material,
+                                       Scattering, SpatialScheme, WaveSpeeds)
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+# Dose parity bar against the reference's own fixtures, relative to the maximum
+# dose.  Two builds of the oracle that differ only in FMA contraction disagree
+# by 4.9e-10 on kat2mm_reduced_water: the M1 closure near free streaming
+# (chi -> 1, isotropic part 0.5*(1-chi) -> 1e-10) amplifies one-ulp differences,
+# and the reference runs its HLL loop under Numba fastmath.  The bar is four
+# times that measured floor.
+REFERENCE_DOSE_RTOL = 2e-9
+
+
+def load(name: str):
+    return np.load(GOLDEN / name)
+
+
+def march_specs() -> dict:
+    return json.loads((GOLDEN / "marches.json").read_text())
+
+
+def march_config(spec: dict) -> SolverConfig:
+    objects = [Box(*o[:6], Material[o[6]]) for o in spec["objects"]]
+    beam_kw = {"n_protons": 1e6, "energy": 150.0, "energy_spread": 1.0, "sigma": (0.002, 0.002)}
+    beam_kw.update({k: tuple(v) if isinstance(v, list) else v for k, v in spec["beam"].items()})
+    phys = Physics(**{k: Scattering[v] if k == "scattering" else v for k, v in spec["physics"].items()})
+    num_kw = {"energy_scheme": EnergyScheme.IF_SSPRK3, "cfl": 0.9, "max_energy_step": 0.25}
+    num_kw.update(spec["numerics"])
+    geo = Geometry(size=tuple(spec["size"]), resolution=tuple(spec["resolution"]), objects=objects)
+    return SolverConfig(geometry=geo, beam=Beam(**beam_kw), physics=phys, numerics=Numerics(**num_kw))
+
+
+def published_kats() -> dict:
+    return json.loads((GOLDEN / "published_kats.json").read_text())
+
+
+def published_config(case: dict) -> SolverConfig:
+    c = case["config"]
+    g, b, n, p = c["geometry"], c["beam"], c["numerics"], c["physics"]
+    objects = [Box(o["x_min"], o["x_max"], o["y_min"], o["y_max"], o["z_min"], o["z_max"],
+                   Material[o["material"]]) for o in g["objects"]]
+    geo = Geometry(size=tuple(g["size"]), resolution=tuple(g["resolution"]),
+                   background_material=Material[g["background_material"]], objects=objects)
+    beam = Beam(n_protons=b["n_protons"], energy=b["energy"], energy_spread=b["energy_spread"],
+                sigma=tuple(b["sigma"]), center=tuple(b["center"]),
+                angular_spread=b["angular_spread"], cutoff_sigma=b["cutoff_sigma"])
+    phys = Physics(scattering=Scattering[p["scattering"]], nuclear=p["nuclear"],
+                   coefficient_interpolation=CoefficientInterpolation[p["coefficient_interpolation"]])
+    num = Numerics(spatial_scheme=SpatialScheme[n["spatial_scheme"]],
+                   energy_scheme=EnergyScheme[n["energy_scheme"]],
+                   wave_speeds=WaveSpeeds[n["wave_speeds"]], max_energy_step=n["max_energy_step"],
+                   cfl=n["cfl"], energy_min=n["energy_min"],
+                   energy_window_sigma=n["energy_window_sigma"],
+                   moving_active_domain=n["moving_active_domain"],
+                   vacuum_aware_cfl=n["vacuum_aware_cfl"],
+                   active_truncation_sigma=n["active_truncation_sigma"],
+                   active_guard_cells=n["active_guard_cells"])
+    return SolverConfig(geometry=geo, beam=beam, physics=phys, numerics=num)
+
+
+OPERATOR_CASES = {
+    "if_full": (Physics(scattering=Scattering.WENTZEL, nuclear=True), EnergyScheme.IF_SSPRK3),
+    "if_rossi_pchip": (Physics(scattering=Scattering.ROSSI, nuclear=True,
+                               coefficient_interpolation=CoefficientInterpolation.PCHIP),
+                       EnergyScheme.IF_SSPRK3),
+    "if_nuclear_only": (Physics(nuclear=True), EnergyScheme.IF_SSPRK3),
+    "ssprk3_csda": (Physics(), EnergyScheme.SSPRK3),
+    "strang_ssprk3": (Physics(scattering=Scattering.WENTZEL, nuclear=True), EnergyScheme.SSPRK3),
+    "strang_euler": (Physics(scattering=Scattering.WENTZEL, nuclear=True), EnergyScheme.FORWARD_EULER),
+    "euler_csda": (Physics(), EnergyScheme.FORWARD_EULER),
+}
+
+
+def operator_geometry():
+    g = load("operators.npz")
+    mats = tuple(next(m for m in Material if m.value == n) for n in g["material_names"])
+    geo = Geometry.from_ids(tuple(float(s) for s in g["size"]), g["ids"], mats)
+    beam = Beam(n_protons=1e6, energy=100.0, energy_spread=1.5, sigma=(0.003, 0.0025),
+                center=(0.001, -0.0005), angular_spread=0.05)
+    return g, geo, beam
+
+
+def operator_config(name: str | None = None, **numerics) -> SolverConfig:
+    _, geo, beam = operator_geometry()
+    phys, scheme = OPERATOR_CASES[name] if name else (Physics(), EnergyScheme.IF_SSPRK3)
+    num = Numerics(**{"energy_scheme": scheme, "cfl": 0.8, "max_energy_step": 0.5, **numerics})
+    return SolverConfig(geometry=geo, beam=beam, physics=phys, numerics=num)

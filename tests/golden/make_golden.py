@@ -1,0 +1,270 @@
+"""Generate the golden fixtures in tests/golden/ from the reference itself.
+
+Runs the unmodified reference ``proton_solver`` (imported from its source
+tree, FP64 NumPy/Numba CPU path) on seeded inputs and stores inputs and
+outputs as small ``.npz`` files; also collects the deterministic maxima the
+reference publishes for its 2 mm coarse-grid runs.  Only this script reads
+the reference; the tests read the fixtures.
+
+Usage:  NUMBA_CACHE_DIR=/tmp/numba_cache python tests/golden/make_golden.py <reference root>
+
+The reference imports plotting and gamma modules at import time that are not
+on the energy-march path (matplotlib, pymedphys); they are replaced by empty
+stub modules here.
+"""
+
+from __future__ import annotations
+
+import json
+import os
+import sys
+import types
+from pathlib import Path
+
+import numpy as np
+
+OUT = Path(__file__).resolve().parent
+
+
+def import_reference(root: Path):
+    os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/numba_cache")
+    for name in ["matplotlib", "matplotlib.pyplot", "matplotlib.lines", "matplotlib.patches",
+                 "mpl_toolkits", "mpl_toolkits.mplot3d", "mpl_toolkits.mplot3d.art3d", "pymedphys"]:
+        sys.modules[name] = types.ModuleType(name)
+    sys.modules["matplotlib.lines"].Line2D = object
+    sys.modules["matplotlib.patches"].Patch = object
+    sys.modules["mpl_toolkits.mplot3d.art3d"].Poly3DCollection = object
+    sys.path.insert(0, str(root / "src"))
+    import proton_solver  # noqa: F401
+    return proton_solver
+
+
+def unit_vectors(ps, rng):
+    from proton_solver.numerics.reconstruction_methods.weno_z import _weno_z_left_scalar
+    from proton_solver.numerics.realizability import project_realizable
+    from proton_solver.numerics.wave_speeds import eigenvalues
+    from proton_solver.numerics.flux import hll_flux
+    from proton_solver.enums import WaveSpeeds, Material, CoefficientInterpolation as CI
+    from proton_solver.physics.stopping_power import stopping_power
+    from proton_solver.physics.scattering import first_transport_coefficient, rossi_transport_coefficient
+    from proton_solver.physics.nuclear import nuclear_removal_coefficient
+
+    out = {}
+    n = 600
+    # WENO-Z stencils: smooth, steps, zeros, huge and tiny magnitudes
+    smooth = np.cumsum(rng.normal(size=(n, 5)), axis=1)
+    steps = np.where(rng.random((n, 5)) < 0.5, 0.0, 1.0) * rng.lognormal(0, 3, size=(n, 1))
+    scale = 10.0 ** rng.uniform(-12, 12, size=(n, 1))
+    w = np.concatenate([smooth, steps, smooth * scale, np.zeros((4, 5)), np.ones((4, 5))])
+    out["weno_in"] = w
+    out["weno_out"] = np.array([_weno_z_left_scalar(*row) for row in w])
+
+    def states(m):
+        phi = 10.0 ** rng.uniform(-6, 12, size=m)
+        d = rng.normal(size=(m, 3))
+        d /= np.linalg.norm(d, axis=1)[:, None]
+        f = rng.choice([0.0, 1e-12, 0.3, 0.9, 0.999999, 1.0 - 1e-10, 1.2], size=m)
+        J = d * (f * phi)[:, None]
+        s = np.column_stack([phi, J])
+        s[: m // 20, 0] *= -1.0          # negative densities
+        s[m // 20: m // 10] = 0.0        # vacuum
+        return s
+
+    P = states(n)
+    out["proj_in"] = P
+    out["proj_out"] = project_realizable(P.T.reshape(4, n, 1, 1).copy(), np).reshape(4, n).T
+    R = out["proj_out"]
+    eig = np.zeros((n, 3, 2))
+    for ax in range(3):
+        lo, hi = eigenvalues(R.T.reshape(4, n, 1, 1).copy(), ax, np)
+        eig[:, ax, 0], eig[:, ax, 1] = lo.ravel(), hi.ravel()
+    out["eig_in"], out["eig_out"] = R, eig
+    L = project_realizable(states(n).T.reshape(4, n, 1, 1).copy(), np).reshape(4, n).T
+    Rr = project_realizable(states(n).T.reshape(4, n, 1, 1).copy(), np).reshape(4, n).T
+    hll = np.zeros((n, 3, 4))
+    hllu = np.zeros((n, 3, 4))
+    for ax in range(3):
+        a = L.T.reshape(4, n, 1, 1).copy()
+        b = Rr.T.reshape(4, n, 1, 1).copy()
+        hll[:, ax] = hll_flux(a, b, ax, WaveSpeeds.EXACT, np).reshape(4, n).T
+        hllu[:, ax] = hll_flux(a, b, ax, WaveSpeeds.UNIT, np).reshape(4, n).T
+    out["hll_left"], out["hll_right"], out["hll_exact"], out["hll_unit"] = L, Rr, hll, hllu
+
+    class M(__import__("enum").Enum):   # all five data/ materials by Geant4 name
+        WATER = "G4_WATER"
+        BONE_COMPACT = "G4_BONE_COMPACT_ICRU"
+        LUNG = "G4_LUNG_ICRP"
+        AIR = "G4_AIR"
+        MUSCLE_SKELETAL = "G4_MUSCLE_SKELETAL_ICRP"
+    mats = list(M)
+    E = np.concatenate([10.0 ** rng.uniform(-4, np.log10(300.0), size=300),
+                        [1e-4, 300.0, 150.0, 70.0, 1.0]])
+    out["coef_energy"] = E
+    out["coef_materials"] = np.array([m.value for m in mats])
+    out["sp"] = np.array([[stopping_power(m, e) for e in E] for m in mats])
+    out["tr_linear"] = np.array([[first_transport_coefficient(m, e, CI.LINEAR) for e in E] for m in mats])
+    out["tr_pchip"] = np.array([[first_transport_coefficient(m, e, CI.PCHIP) for e in E] for m in mats])
+    out["nuc_linear"] = np.array([[nuclear_removal_coefficient(m, e, CI.LINEAR) for e in E] for m in mats])
+    out["nuc_pchip"] = np.array([[nuclear_removal_coefficient(m, e, CI.PCHIP) for e in E] for m in mats])
+    out["rossi"] = np.array([[rossi_transport_coefficient(m, e) for e in E] for m in mats])
+    np.savez_compressed(OUT / "unit_vectors.npz", **out)
+
+
+def _config(ps, *, size, resolution, objects=(), beam=None, physics=None, numerics=None):
+    from proton_solver import (Geometry, Box, Beam, SolverConfig, Physics, Numerics, References,
+                               Reference, Backend)
+    geo = Geometry(size=size, resolution=resolution, objects=list(objects))
+    return SolverConfig(geometry=geo, beam=beam or Beam(), physics=physics or Physics(),
+                        numerics=numerics or Numerics(), backend=Backend.CPU,
+                        references=References(reference=Reference.NONE))
+
+
+def operators(ps, rng):
+    """Operator-level fixtures on a small heterogeneous grid."""
+    from proton_solver import (Box, Beam, Material, Physics, Numerics, Scattering, EnergyScheme,
+                               CoefficientInterpolation as CI, WaveSpeeds, SpatialScheme)
+    from proton_solver.numerics.grid import Grid
+    from proton_solver.numerics.boundary import BeamInflow
+    from proton_solver.physics.materials import MaterialMap
+    from proton_solver.numerics.spatial import spatial_operator
+    from proton_solver.numerics import energy as en
+
+    size, res = (0.018, 0.02, 0.024), (9, 10, 12)
+    objects = [Box(-0.009, 0.0, -0.01, 0.01, 0.008, 0.016, Material.BONE_COMPACT),
+               Box(0.002, 0.009, -0.01, 0.0, 0.0, 0.024, Material.LUNG)]
+    beam = Beam(n_protons=1e6, energy=100.0, energy_spread=1.5, sigma=(0.003, 0.0025),
+                center=(0.001, -0.0005), angular_spread=0.05)
+    cases = {
+        "if_full": (Physics(scattering=Scattering.WENTZEL, nuclear=True), EnergyScheme.IF_SSPRK3),
+        "if_rossi_pchip": (Physics(scattering=Scattering.ROSSI, nuclear=True,
+                                   coefficient_interpolation=CI.PCHIP), EnergyScheme.IF_SSPRK3),
+        "if_nuclear_only": (Physics(nuclear=True), EnergyScheme.IF_SSPRK3),
+        "ssprk3_csda": (Physics(), EnergyScheme.SSPRK3),
+        "strang_ssprk3": (Physics(scattering=Scattering.WENTZEL, nuclear=True), EnergyScheme.SSPRK3),
+        "strang_euler": (Physics(scattering=Scattering.WENTZEL, nuclear=True), EnergyScheme.FORWARD_EULER),
+        "euler_csda": (Physics(), EnergyScheme.FORWARD_EULER),
+    }
+    # random realizable state: smooth bump plus noise, some vacuum
+    x = np.linspace(-1, 1, res[0])[:, None, None]
+    y = np.linspace(-1, 1, res[1])[None, :, None]
+    z = np.linspace(0, 1, res[2])[None, None, :]
+    phi = 1e9 * np.exp(-3 * (x ** 2 + y ** 2) - 5 * (z - 0.4) ** 2) * (1 + 0.3 * rng.random(res))
+    phi[:, :, -2:] = 0.0
+    d = rng.normal(size=(3, *res)) * 0.15
+    d[2] += 1.0
+    d /= np.linalg.norm(d, axis=0)
+    f = rng.uniform(0.2, 1.0 - 1e-10, size=res)
+    U = np.concatenate([phi[None], d * (f * phi)[None]], axis=0)
+    bc_custom = np.abs(rng.normal(size=(4, res[0], res[1]))) * 1e8
+    bc_custom[1:3] *= 0.1
+    out = {"U": U, "size": np.array(size), "res": np.array(res), "bc_custom": bc_custom}
+    E, dE = 90.0, 0.21
+    out["E"], out["dE"] = E, dE
+    base = _config(ps, size=size, resolution=res, objects=objects, beam=beam,
+                   numerics=Numerics(energy_scheme=EnergyScheme.IF_SSPRK3, cfl=0.8, max_energy_step=0.5))
+    grid = Grid.from_geometry(base.geometry, np)
+    mm = MaterialMap.from_geometry(base.geometry, grid, np)
+    inflow = BeamInflow.from_beam(beam, grid, np)
+    out["ids"] = np.asarray(mm.ids)
+    out["material_names"] = np.array([m.value for m in mm.materials])
+    out["inflow_spatial"] = inflow.spatial
+    out["inflow_state"] = inflow.state(E, np)
+    out["rhs"] = spatial_operator(U.copy(), E, grid, inflow, SpatialScheme.WENO_Z, WaveSpeeds.EXACT, np)
+    out["rhs_bc"] = spatial_operator(U.copy(), E, grid, inflow, SpatialScheme.WENO_Z,
+                                     WaveSpeeds.EXACT, np, boundary_state=bc_custom)
+    out["rhs_unit"] = spatial_operator(U.copy(), E, grid, inflow, SpatialScheme.WENO_Z, WaveSpeeds.UNIT, np)
+    out["dE_exact"] = en.compute_energy_step(U.copy(), E, mm, grid, inflow, base, np)
+    unit_cfg = _config(ps, size=size, resolution=res, objects=objects, beam=beam,
+                       numerics=Numerics(wave_speeds=WaveSpeeds.UNIT, cfl=0.8, max_energy_step=0.5))
+    out["dE_unit"] = en.compute_energy_step(U.copy(), E, mm, grid, inflow, unit_cfg, np)
+    for name, (phys, scheme) in cases.items():
+        cfg = _config(ps, size=size, resolution=res, objects=objects, beam=beam, physics=phys,
+                      numerics=Numerics(energy_scheme=scheme, cfl=0.8, max_energy_step=0.5))
+        if scheme is EnergyScheme.IF_SSPRK3:
+            Un, ed = en.if_ssprk3(U.copy(), E, dE, mm, grid, inflow, cfg, np)
+        elif phys.scattering is not Scattering.OFF or phys.nuclear:
+            Un, ed = en.strang_energy_step(U.copy(), E, dE, mm, grid, inflow, cfg, np)
+        else:
+            Un, ed = en.advance_energy_step(U.copy(), E, dE, mm, grid, inflow, cfg, np)
+        out[f"step_{name}_U"], out[f"step_{name}_edep"] = Un, ed
+    np.savez_compressed(OUT / "operators.npz", **out)
+
+
+MARCHES = {
+    # name: (size, resolution, objects, beam kwargs, physics kwargs, numerics kwargs, snapshots)
+    "kat2mm_reduced_water": ((0.024, 0.024, 0.2), (12, 12, 100), [], {}, {}, {}, ()),
+    "kat2mm_extended_transversal": ((0.024, 0.024, 0.2), (12, 12, 100),
+                                    [(-0.012, 0.0, -0.012, 0.012, 0.0, 0.2, "BONE_COMPACT")], {},
+                                    {"scattering": "WENTZEL", "nuclear": True}, {}, ()),
+    "hetero_snapshots": ((0.02, 0.016, 0.06), (10, 8, 30),
+                         [(-0.01, 0.01, -0.008, 0.008, 0.02, 0.03, "BONE_COMPACT"),
+                          (0.0, 0.01, -0.008, 0.0, 0.035, 0.06, "LUNG")],
+                         {"energy": 60.0, "energy_spread": 0.8, "sigma": (0.003, 0.002),
+                          "center": (0.0015, 0.0), "angular_spread": 0.02},
+                         {"scattering": "WENTZEL", "nuclear": True}, {"max_energy_step": 0.5},
+                         (55.0, 30.0, 10.0)),
+    "moving_box_extended": ((0.032, 0.032, 0.16), (16, 16, 64),
+                            [(0.0, 0.016, -0.016, 0.016, 0.0, 0.16, "BONE_COMPACT")],
+                            {"energy": 120.0, "sigma": (0.003, 0.003)},
+                            {"scattering": "WENTZEL", "nuclear": True},
+                            {"moving_active_domain": True, "max_energy_step": 0.5}, (60.0,)),
+    "moving_box_vacuum_cfl": ((0.04, 0.04, 0.1), (20, 20, 50), [],
+                              {"energy": 80.0, "sigma": (0.003, 0.003)}, {},
+                              {"moving_active_domain": True, "vacuum_aware_cfl": True,
+                               "max_energy_step": 0.5}, ()),
+}
+
+
+def marches(ps):
+    from proton_solver import (Box, Beam, Material, Physics, Numerics, Scattering, EnergyScheme,
+                               Solver)
+    for name, (size, res, objs, bk, pk, nk, snaps) in MARCHES.items():
+        objects = [Box(*o[:6], Material[o[6]]) for o in objs]
+        beam = Beam(**{"n_protons": 1e6, "energy": 150.0, "energy_spread": 1.0,
+                       "sigma": (0.002, 0.002), **bk})
+        phys = Physics(**{k: (Scattering[v] if k == "scattering" else v) for k, v in pk.items()})
+        num = Numerics(**{"energy_scheme": EnergyScheme.IF_SSPRK3, "cfl": 0.9,
+                          "max_energy_step": 0.25, **nk})
+        cfg = _config(ps, size=size, resolution=res, objects=objects, beam=beam, physics=phys,
+                      numerics=num)
+        r = Solver(cfg).solve(snapshot_energies=snaps)
+        out = {"dose": r.dose, "energies": r.energies}
+        if r.dose.size <= 5000:          # final states only for the smallest grid
+            out["phi"], out["J"] = r.phi, r.J
+        for k, (e, s) in enumerate(sorted(r.snapshots.items(), reverse=True)):
+            out[f"snap{k}_energy"] = e
+            out[f"snap{k}"] = s
+        np.savez_compressed(OUT / f"march_{name}.npz", **out)
+    spec = {n: {"size": v[0], "resolution": v[1], "objects": v[2], "beam": v[3], "physics": v[4],
+                "numerics": v[5], "snapshots": v[6]} for n, v in MARCHES.items()}
+    (OUT / "marches.json").write_text(json.dumps(spec, indent=1))
+
+
+def published(root: Path):
+    """Deterministic maxima/R80 the reference publishes for the 2 mm grids."""
+    base = root / "thesis_results" / "robustness" / "coarse_grid_2mm"
+    cases = {}
+    for model in ("reduced_physics", "scattering_nuclear"):
+        for case in ("homogeneous_water", "longitudinal_slabs", "transversal_slabs"):
+            d = base / model / case / "weno_z"
+            cfg = json.loads((d / "config.json").read_text())
+            met = json.loads((d / "metrics.json").read_text())
+            cases[f"{model}/{case}"] = {
+                "source": f"thesis_results/robustness/coarse_grid_2mm/{model}/{case}/weno_z",
+                "config": {k: cfg[k] for k in ("beam", "geometry", "numerics", "physics")},
+                "maximum_dose_Gy": met["maximum_dose"]["deterministic_Gy"],
+                "r80_mm": met["range"]["deterministic_r80_mm"],
+                "dfw_mm": met["range"]["deterministic_dfw_mm"],
+                "peak_search_from_mm": met["range"]["peak_search_from_mm"],
+            }
+    (OUT / "published_kats.json").write_text(json.dumps(cases, indent=1))
+
+
+if __name__ == "__main__":
+    root = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ps = import_reference(root)
+    rng = np.random.default_rng(20261203)
+    published(root)
+    unit_vectors(ps, rng)
+    operators(ps, rng)
+    marches(ps)

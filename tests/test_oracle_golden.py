@@ -1,0 +1,135 @@
+"""Pin the CPU oracle against the reference's own outputs (tests/golden/).
+
+The fixtures were produced by tests/golden/make_golden.py from the
+unmodified reference proton_solver; the published maxima come from its
+thesis_results/robustness/coarse_grid_2mm runs.
+"""
+
+import numpy as np
+import pytest
+
+import oracle.oracle as O
+from proton_dose_m1_b200 import Geometry, SolverConfig, Beam, Physics, Numerics
+from proton_dose_m1_b200.enums import CoefficientInterpolation, Material, Scattering
+from tests import cases
+
+
+@pytest.fixture(scope="module")
+def unit():
+    return cases.load("unit_vectors.npz")
+
+
+def test_weno_bit_exact(unit):
+    got = np.array([O.weno_left(r) for r in unit["weno_in"]])
+    np.testing.assert_array_equal(got, unit["weno_out"])
+
+
+def test_projection_bit_exact(unit):
+    got = np.array([O.project(r) for r in unit["proj_in"]])
+    np.testing.assert_array_equal(got, unit["proj_out"])
+
+
+def test_eigenvalues_bit_exact(unit):
+    got = np.array([[O.eigenvalues(r, ax) for ax in range(3)] for r in unit["eig_in"]])
+    np.testing.assert_array_equal(got, unit["eig_out"])
+
+
+def test_hll_flux(unit):
+    L, R = unit["hll_left"], unit["hll_right"]
+    exact = np.array([[O.hll_flux(l, r, ax) for ax in range(3)] for l, r in zip(L, R)])
+    unit_speeds = np.array([[O.hll_flux(l, r, ax, True) for ax in range(3)] for l, r in zip(L, R)])
+    # The reference evaluates this kernel under Numba fastmath; near free
+    # streaming the closure amplifies reassociation differences, so the bar is
+    # relative to the state's density.
+    scale = np.maximum(np.abs(L[:, 0]), np.abs(R[:, 0]))[:, None, None] + 1e-300
+    assert np.max(np.abs(exact - unit["hll_exact"]) / scale) < 1e-10
+    assert np.max(np.abs(unit_speeds - unit["hll_unit"]) / scale) < 1e-14
+
+
+@pytest.mark.parametrize("material", list(Material))
+def test_coefficients_bit_exact(unit, material):
+    E = unit["coef_energy"]
+    mi = list(unit["coef_materials"]).index(material.value)
+    for interp, tr_key, nuc_key in ((CoefficientInterpolation.LINEAR, "tr_linear", "nuc_linear"),
+                                    (CoefficientInterpolation.PCHIP, "tr_pchip", "nuc_pchip")):
+        cfg = SolverConfig(geometry=Geometry(size=(0.01, 0.01, 0.01), resolution=(4, 4, 4),
+                                             background_material=material),
+                           beam=Beam(energy=100.0),
+                           physics=Physics(scattering=Scattering.WENTZEL, nuclear=True,
+                                           coefficient_interpolation=interp))
+        p = O.OracleProblem(cfg)
+        np.testing.assert_array_equal([p.stopping_power(0, e) for e in E], unit["sp"][mi])
+        np.testing.assert_array_equal([p.transport_coefficient(0, e) for e in E], unit[tr_key][mi])
+        np.testing.assert_array_equal([p.nuclear_coefficient(0, e) for e in E], unit[nuc_key][mi])
+    cfg = SolverConfig(geometry=Geometry(size=(0.01, 0.01, 0.01), resolution=(4, 4, 4),
+                                         background_material=material),
+                       beam=Beam(energy=100.0), physics=Physics(scattering=Scattering.ROSSI))
+    p = O.OracleProblem(cfg)
+    np.testing.assert_allclose([p.transport_coefficient(0, e) for e in E], unit["rossi"][mi],
+                               rtol=4e-16, atol=0)
+
+
+def test_energy_outside_table_raises():
+    cfg = SolverConfig(geometry=Geometry(size=(0.01, 0.01, 0.01), resolution=(4, 4, 4)),
+                       beam=Beam(energy=100.0))
+    p = O.OracleProblem(cfg)
+    with pytest.raises(ValueError):
+        p.stopping_power(0, 301.0)
+    with pytest.raises(ValueError):
+        p.stopping_power(0, 0.0)
+    assert p.stopping_power(0, 1e-4 * (1 - 1e-12)) > 0   # within numpy.isclose of the first node
+
+
+def test_inflow_and_operators():
+    g, geo, beam = cases.operator_geometry()
+    p = O.OracleProblem(cases.operator_config())
+    np.testing.assert_array_equal(p.inflow_spatial(), g["inflow_spatial"])
+    E = float(g["E"])
+    np.testing.assert_array_equal(p.inflow_state(E), g["inflow_state"])
+    for key, bc in (("rhs", None), ("rhs_bc", g["bc_custom"])):
+        scale = np.abs(g[key][0]).max()
+        assert np.abs(p.spatial_operator(g["U"], E, bc) - g[key]).max() / scale < 1e-10
+    assert p.energy_step(g["U"], E) == float(g["dE_exact"])
+    pu = O.OracleProblem(cases.operator_config(wave_speeds=cases.WaveSpeeds.UNIT))
+    assert pu.energy_step(g["U"], E) == float(g["dE_unit"])
+    scale = np.abs(g["rhs_unit"][0]).max()
+    assert np.abs(pu.spatial_operator(g["U"], E) - g["rhs_unit"]).max() / scale < 1e-14
+
+
+@pytest.mark.parametrize("name", list(cases.OPERATOR_CASES))
+def test_one_step(name):
+    g = cases.load("operators.npz")
+    p = O.OracleProblem(cases.operator_config(name))
+    U, edep = p.advance(g["U"], float(g["E"]), float(g["dE"]))
+    ref_U, ref_e = g[f"step_{name}_U"], g[f"step_{name}_edep"]
+    assert np.abs(U - ref_U).max() / np.abs(ref_U[0]).max() < 1e-11
+    assert np.abs(edep - ref_e).max() / np.abs(ref_e).max() < 1e-11
+
+
+@pytest.mark.parametrize("name", list(cases.march_specs()))
+def test_march_matches_reference(name):
+    spec = cases.march_specs()[name]
+    cfg = cases.march_config(spec)
+    p = O.OracleProblem(cfg)
+    U0 = None if cfg.numerics.moving_active_domain else np.zeros((4, *cfg.geometry.resolution))
+    U, dose, energies, snaps = p.march(U0, snapshot_energies=tuple(spec["snapshots"]))
+    g = cases.load(f"march_{name}.npz")
+    np.testing.assert_allclose(energies, g["energies"], rtol=0, atol=1e-12)
+    assert np.abs(dose - g["dose"]).max() <= cases.REFERENCE_DOSE_RTOL * g["dose"].max()
+    assert len(snaps) == len(spec["snapshots"])
+    for k, e in enumerate(sorted(snaps, reverse=True)):
+        assert e == float(g[f"snap{k}_energy"])
+        ref = g[f"snap{k}"]
+        assert np.abs(snaps[e] - ref).max() <= cases.REFERENCE_DOSE_RTOL * np.abs(ref[0]).max()
+    if "phi" in g:
+        assert np.abs(U[0] - g["phi"]).max() <= cases.REFERENCE_DOSE_RTOL * np.abs(g["phi"]).max()
+
+
+@pytest.mark.parametrize("case", ["reduced_physics/homogeneous_water",
+                                  "scattering_nuclear/transversal_slabs"])
+def test_published_maximum_dose(case):
+    kat = cases.published_kats()[case]
+    cfg = cases.published_config(kat)
+    p = O.OracleProblem(cfg)
+    _, dose, _, _ = p.march(np.zeros((4, *cfg.geometry.resolution)))
+    assert abs(dose.max() - kat["maximum_dose_Gy"]) <= cases.REFERENCE_DOSE_RTOL * kat["maximum_dose_Gy"]
