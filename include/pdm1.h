@@ -1,0 +1,155 @@
+/*
+ * pdm1.h -- C ABI of the B200 (sm_100a) M1 proton dose march.
+ *
+ * One shared library, libpdm1.so, implements the energy march of
+ * proton_solver/numerics/energy.py (WENO-Z reconstruction, HLL fluxes with
+ * exact M1 speeds, realizability projection, IF-SSPRK3 / SSPRK3 / Strang /
+ * forward-Euler integrators, CSDA stopping power, dose deposit) as CUDA
+ * kernels.  Plain C types only: host pointers, device pointers, sizes and a
+ * CUDA stream handle.  Every entry point returns a status (PDM1_OK == 0);
+ * pdm1_last_error() describes the last failure on the calling thread.
+ *
+ * Layouts follow the reference: a state U is (4, nx, ny, nz) float64 in C
+ * order (z fastest), components (phi, Jx, Jy, Jz); a dose is (nx, ny, nz);
+ * a boundary plane is (4, nx, ny); material ids are int32 (nx, ny, nz).
+ */
+#ifndef PDM1_H
+#define PDM1_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *pdm1_stream_t;   /* same type as cudaStream_t */
+
+enum pdm1_status {
+    PDM1_OK = 0,
+    PDM1_ERR_ARGUMENT = 1,      /* bad shape, pointer or option (reference: ValueError) */
+    PDM1_ERR_RANGE = 2,         /* energy outside a coefficient table (ValueError) */
+    PDM1_ERR_CUDA = 3,          /* a CUDA runtime call failed */
+    PDM1_ERR_MAX_STEPS = 4,     /* the energies buffer is shorter than the march */
+    PDM1_ERR_NO_BEAM = 5,       /* the inflow profile is empty (ValueError) */
+    PDM1_ERR_UNSUPPORTED = 6,   /* option without a GPU kernel (NotImplementedError) */
+    PDM1_ERR_NONFINITE = 7      /* a non-finite energy step was produced */
+};
+
+enum { PDM1_SCATTERING_OFF = 0, PDM1_SCATTERING_ROSSI = 1, PDM1_SCATTERING_WENTZEL = 2 };
+enum { PDM1_INTERP_LINEAR = 0, PDM1_INTERP_PCHIP = 1 };
+enum { PDM1_SCHEME_FORWARD_EULER = 0, PDM1_SCHEME_SSPRK3 = 1, PDM1_SCHEME_IF_SSPRK3 = 2 };
+enum { PDM1_SPEEDS_EXACT = 0, PDM1_SPEEDS_UNIT = 1 };
+enum { PDM1_FP64 = 0, PDM1_FP32_FP64 = 1 };
+
+/* One tabulated coefficient, host memory, strictly increasing energies. */
+typedef struct {
+    int n_nodes;
+    const double *energy;     /* MeV */
+    const double *value;
+} pdm1_table;
+
+/* One material: physics/stopping_power.py, physics/scattering.py,
+ * physics/nuclear.py and physics/materials.py tables. */
+typedef struct {
+    pdm1_table stopping_power;   /* MeV/m, interpolated by PCHIP */
+    pdm1_table transport;        /* Wentzel-VI first transport coefficient, 1/m */
+    pdm1_table nuclear;          /* primary nuclear removal coefficient, 1/m */
+    double density;              /* kg/m^3 */
+    double radiation_length;     /* m (Rossi scattering) */
+} pdm1_material;
+
+/* One pencil beam on one voxel phantom.  Mirrors the arguments the reference
+ * passes to energy_march (numerics/energy.py:1497-1505): Grid, MaterialMap,
+ * BeamInflow and SolverConfig.  All pointers are host memory and are copied
+ * into the plan. */
+typedef struct {
+    int nx, ny, nz;
+    double dx, dy, dz;                 /* m */
+    int n_materials;                   /* 1 .. 16 */
+    const pdm1_material *materials;
+    const int32_t *ids;                /* (nx, ny, nz) */
+    const double *inflow_spatial;      /* (nx, ny): n_protons * normalised profile,
+                                          numerics/boundary.py:30-80 */
+    double beam_energy;                /* MeV */
+    double energy_spread;              /* MeV, > 0 */
+    double angular_spread;             /* rad */
+    int scattering, nuclear, interpolation;
+    int energy_scheme, wave_speeds;
+    double max_energy_step, cfl, energy_min, energy_window_sigma;
+    int moving_active_domain;          /* numerics/moving_active_domain.py */
+    int vacuum_aware_cfl;
+    int active_guard_cells;
+    double active_relative_tolerance;  /* exp(-sigma_trunc^2 / 2), energy.py:1305 */
+    int precision;                     /* PDM1_FP64 or PDM1_FP32_FP64 */
+} pdm1_problem;
+
+typedef struct pdm1_plan pdm1_plan;
+
+typedef struct {
+    int n_steps;              /* energy steps taken; energies holds n_steps + 1 values */
+    int n_snapshots;          /* snapshots written to snap_out */
+    int final_state_valid;    /* U holds the final state (full grid) */
+    int graph_replays;        /* CUDA graph launches used by the march */
+    int kernel_launches;      /* kernels this library launched for the march */
+    int stage_launches;       /* launches of the fused stage kernels */
+    double stage_ms;          /* their summed device time (CUDA events on the march stream) */
+} pdm1_march_info;
+
+/* Plan: copies the problem to the device and allocates the workspace.
+ * Replaces the setup half of energy_march (energy.py:1519-1554). */
+int pdm1_plan_create(const pdm1_problem *problem, pdm1_plan **plan);
+void pdm1_plan_destroy(pdm1_plan *plan);
+size_t pdm1_plan_workspace_bytes(const pdm1_plan *plan);
+
+/* The march: numerics/energy.py:1497-1643 (static domain) and 1262-1494
+ * (moving active box).  Device pointers: U (4,nx,ny,nz) in/out, dose
+ * (nx,ny,nz) out, energies (max_steps+1) out, snap_out (n_snap,4,nx,ny,nz)
+ * out.  Host pointers: snap_targets (n_snap), snap_energies_out (n_snap).
+ * Snapshots are written in descending target order, like the reference's
+ * snapshot dict.  Synchronises `stream` before returning. */
+int pdm1_march(pdm1_plan *plan, double *U, double *dose, double *energies, int max_steps,
+               const double *snap_targets, int n_snap, double *snap_out,
+               double *snap_energies_out, pdm1_march_info *info, pdm1_stream_t stream);
+
+/* The first `step_limit` steps of the march (a bounded prefix, for timing
+ * samples and prefix parity); otherwise as pdm1_march without snapshots. */
+int pdm1_march_steps(pdm1_plan *plan, double *U, double *dose, double *energies, int max_steps,
+                     int step_limit, pdm1_march_info *info, pdm1_stream_t stream);
+
+/* Building blocks on the full grid, for operator-level parity checks. */
+
+/* numerics/spatial.py:104-252: rhs = -div F(U), boundary_state (4,nx,ny)
+ * device or NULL (then the beam inflow at `energy`). */
+int pdm1_spatial_operator(pdm1_plan *plan, const double *U, double energy,
+                          const double *boundary_state, double *rhs, pdm1_stream_t stream);
+
+/* numerics/energy.py:539-660: the CFL energy step for state U at `energy`. */
+int pdm1_energy_step(pdm1_plan *plan, const double *U, double energy, double *dE_out,
+                     pdm1_stream_t stream);
+
+/* One accepted step of the configured integrator (energy.py:1580-1615):
+ * U advanced in place, edep (nx,ny,nz) receives the energy deposition in MeV
+ * per cell volume and MeV of step (before the MEV_TO_JOULE / rho scaling). */
+int pdm1_advance(pdm1_plan *plan, double *U, double energy, double dE, double *edep,
+                 pdm1_stream_t stream);
+
+/* Device evaluation of the material coefficients at host energies:
+ * out[(e * n_materials + m) * 3 + {0,1,2}] = S, Sigma_tr, Sigma_r (host). */
+int pdm1_coefficients(pdm1_plan *plan, const double *energies, int n, double *out);
+
+/* Scalar device functions over device arrays (unit parity). */
+int pdm1_weno_batch(const double *v5, double *out, int n, pdm1_stream_t stream);
+int pdm1_project_batch(double *u4, int n, pdm1_stream_t stream);
+int pdm1_eigen_batch(const double *u4, int axis, double *lo_hi, int n, pdm1_stream_t stream);
+int pdm1_hll_batch(const double *left4, const double *right4, int axis, int wave_speeds,
+                   double *flux4, int n, pdm1_stream_t stream);
+int pdm1_exp_batch(const double *x, double *y, int n, pdm1_stream_t stream);
+
+const char *pdm1_last_error(void);
+const char *pdm1_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

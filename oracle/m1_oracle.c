@@ -28,6 +28,72 @@
 
 static __thread char g_err[256];
 
+/* ======================================================================
+ * exp in double-double arithmetic
+ *
+ * The reference calls math.exp / numpy.exp.  The oracle evaluates exp with
+ * its own routine so that the CUDA path, which carries an identical routine,
+ * reproduces every bit: Cody-Waite reduction x = k ln2 + r with ln2 held as
+ * a double-double, exp(r / 2^10) by a degree-9 Taylor series in
+ * double-double (Dekker/Knuth error-free sums and FMA products), ten
+ * squarings, and a final scaling by 2^k.  The double-double result is good
+ * to about 1e-29 relative, so the returned double is the correctly rounded
+ * exp except in rare ties.
+ * ==================================================================== */
+
+typedef struct { double hi, lo; } dd_t;
+
+static dd_t dd_quick(double a, double b) { dd_t r; r.hi = a + b; r.lo = b - (r.hi - a); return r; }
+
+static dd_t dd_add(dd_t a, dd_t b)
+{
+    double s = a.hi + b.hi;
+    double bb = s - a.hi;
+    double e = (a.hi - (s - bb)) + (b.hi - bb);
+    e += a.lo + b.lo;
+    return dd_quick(s, e);
+}
+
+static dd_t dd_mul(dd_t a, dd_t b)
+{
+    double p = a.hi * b.hi;
+    double e = fma(a.hi, b.hi, -p);
+    e += a.hi * b.lo + a.lo * b.hi;
+    return dd_quick(p, e);
+}
+
+static dd_t dd_div_d(double a, double b)
+{
+    double q1 = a / b;
+    double p = q1 * b;
+    double e = fma(q1, b, -p);
+    double rem = (a - p) - e;
+    return dd_quick(q1, rem / b);
+}
+
+static double dd_exp(double x)
+{
+    if (x != x) return x;
+    if (x > 709.782712893384) return INFINITY;
+    if (x < -745.2) return 0.0;
+    const double ln2_hi = 0.6931471805599453094;      /* nearest double to ln 2 */
+    const double ln2_lo = 2.3190468138462996e-17;     /* ln 2 - ln2_hi */
+    double k = rint(x * 1.4426950408889634);
+    double p = k * ln2_hi;
+    double pe = fma(k, ln2_hi, -p);
+    double s = x - p;                  /* exact: x and p are within a factor 2 */
+    double t = -pe - k * ln2_lo;
+    dd_t r = dd_quick(s, t);
+    r.hi *= 0x1p-10;
+    r.lo *= 0x1p-10;
+    /* Horner: sum_{n=0..9} r^n / n! */
+    double fact[10] = {1.0, 1.0, 2.0, 6.0, 24.0, 120.0, 720.0, 5040.0, 40320.0, 362880.0};
+    dd_t acc = dd_div_d(1.0, fact[9]);
+    for (int n = 8; n >= 0; --n) acc = dd_add(dd_mul(acc, r), dd_div_d(1.0, fact[n]));
+    for (int q = 0; q < 10; ++q) acc = dd_mul(acc, acc);
+    return ldexp(acc.hi + acc.lo, (int)k);
+}
+
 static int fail(int code, const char *msg)
 {
     snprintf(g_err, sizeof g_err, "%s", msg);
@@ -35,6 +101,8 @@ static int fail(int code, const char *msg)
 }
 
 const char *orc_last_error(void) { return g_err; }
+
+double orc_exp(double x) { return dd_exp(x); }
 
 void orc_set_threads(int n)
 {
@@ -570,7 +638,7 @@ static double energy_density(const orc_problem *p, double E)
 {
     double de = E - p->d.energy;
     double s = p->d.energy_spread;
-    return exp(-(de * de) / (2.0 * (s * s))) / (sqrt(2.0 * M_PI) * s);
+    return dd_exp(-(de * de) / (2.0 * (s * s))) / (sqrt(2.0 * M_PI) * s);
 }
 
 void orc_inflow_spatial(const orc_problem *p, double *spatial)
@@ -595,7 +663,7 @@ typedef struct {
 static void inflow_state(const orc_problem *p, const domain_t *dm, double E, double *st)
 {
     double ed = energy_density(p, E);
-    double rf = exp(-(p->d.angular_spread * p->d.angular_spread));
+    double rf = dd_exp(-(p->d.angular_spread * p->d.angular_spread));
     size_t n2 = (size_t)dm->nx * dm->ny;
     for (size_t c = 0; c < n2; ++c) {
         double phi = dm->spatial[c] * ed;
@@ -757,7 +825,7 @@ static factor_t source_factor(double ts, double tn, int inverse)
     double a = tn < EXP_CLAMP ? tn : EXP_CLAMP;
     double tsum = tn + ts;
     double b = tsum < EXP_CLAMP ? tsum : EXP_CLAMP;
-    factor_t f = {exp(sign * a), exp(sign * b)};
+    factor_t f = {dd_exp(sign * a), dd_exp(sign * b)};
     return f;
 }
 
@@ -1092,14 +1160,14 @@ static int half_source(const orc_problem *p, const domain_t *dm, double *U, cons
     if (p->d.nuclear) {
         for (size_t c = 0; c < n; ++c) {
             double t = 0.5 * taun[dm->ids[c]];
-            double f = exp(-(t < EXP_CLAMP ? t : EXP_CLAMP));
+            double f = dd_exp(-(t < EXP_CLAMP ? t : EXP_CLAMP));
             for (int q = 0; q < 4; ++q) U[q * n + c] *= f;
         }
     }
     if (p->d.scattering != ORC_SCATTER_OFF) {
         for (size_t c = 0; c < n; ++c) {
             double t = 0.5 * eta[dm->ids[c]];
-            double f = exp(-(t < EXP_CLAMP ? t : EXP_CLAMP));
+            double f = dd_exp(-(t < EXP_CLAMP ? t : EXP_CLAMP));
             for (int q = 1; q < 4; ++q) U[q * n + c] *= f;
         }
     }

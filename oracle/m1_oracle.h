@@ -76,6 +76,7 @@ void orc_problem_destroy(orc_problem *p);
 const char *orc_last_error(void);
 
 /* ---- scalar kernels (unit parity) ---------------------------------- */
+double orc_exp(double x);   /* the double-double exp used by the march */
 double orc_weno_left(const double v[5]);
 void   orc_project(double u[4]);
 void   orc_eigenvalues(const double u[4], int axis, double *lmin, double *lmax);

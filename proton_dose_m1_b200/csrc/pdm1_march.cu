@@ -1,0 +1,1320 @@
+// pdm1_march.cu -- the M1 energy march on sm_100a.
+//
+// Per energy step the device runs
+//   prologue   one CTA: CFL step from the previous stage-3 reduction, snapshot
+//              landing, per-material stopping powers, optical depths and
+//              integrating factors at the stage energies
+//              (numerics/energy.py:539-660, 234-455, 878-1130)
+//   stage A/B/C  the three IF-SSPRK3 stages, each ONE fused kernel: stage a
+//              tile of the stencil source plus its 3-cell WENO halo in shared
+//              memory (ghost cells of numerics/boundary.py:117-399 patched in
+//              shared memory), WENO-Z + projection + HLL on every face of the
+//              tile, divergence, integrating-factor update and projection in
+//              registers; stage C also accumulates the dose and reduces the
+//              next CFL bound with warp shuffles and one atomic per CTA.
+// No host synchronisation inside a step: the energy, dE and all per-step
+// coefficients live in device memory, so chunks of steps are captured once
+// into a CUDA graph and replayed until the device flags the march done.
+#include "../../include/pdm1.h"
+#include "pdm1_math.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace pdm1;
+
+namespace {
+
+constexpr int kMaxMat = 16;
+constexpr int kStepsPerGraph = 32;
+
+thread_local std::string g_error;
+
+int set_error(int code, const std::string &msg) {
+    g_error = msg;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                    \
+    do {                                                                                  \
+        cudaError_t e_ = (expr);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return set_error(PDM1_ERR_CUDA, std::string(#expr ": ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// Device-side plan data
+// ---------------------------------------------------------------------------
+struct MatDev {
+    TableView sp, tr, nuc;
+    double density, X0;
+};
+
+struct ConfigDev {
+    int nx, ny, nz;
+    double dx, dy, dz;
+    int nm;
+    int scattering, nuclear, interp, scheme, unit_speeds;
+    int use_if;          // integrating factors active (IF_SSPRK3 with sources)
+    int strang;          // Strang-split sources around an SSPRK3 / Euler step
+    double cfl, max_dE, Emin, E_beam, sigma_E, rf;
+    int max_steps;
+    int step_limit;      // >= 0: stop (without error) after this many steps
+    int n_targets;
+    const int32_t *ids;
+    const double *spatial;
+    const double *targets;      // descending
+    MatDev mats[kMaxMat];
+};
+
+struct Coeffs {
+    double E, dE, E_next;
+    int active;
+    int snap_slot;
+    double S0[kMaxMat], S1[kMaxMat], S2[kMaxMat];
+    double c1p[kMaxMat], c1c[kMaxMat], c1ip[kMaxMat], c1ic[kMaxMat];
+    double c2p[kMaxMat], c2c[kMaxMat], c2ip[kMaxMat], c2ic[kMaxMat];
+    double Sb[4][kMaxMat];                  // S at E, E-dE/3, E-2dE/3, E-dE
+    double fip[4][kMaxMat], fic[4][kMaxMat];   // inverse factors at those depths
+    double ed[4];                           // spectrum at those energies
+    double ed_next;                         // spectrum at E_next (CFL inflow)
+    double hn[kMaxMat], hs[kMaxMat];        // Strang half-step factors
+};
+
+struct MarchState {
+    double E;
+    unsigned long long inv_bits;   // CFL max (non-negative double bits)
+    double forced_dE;              // > 0: one step with this dE (pdm1_advance)
+    int step, done, ti, taken, error;
+};
+
+enum { ERR_DEV_RANGE = 1, ERR_DEV_MAXSTEPS = 2, ERR_DEV_NONFINITE = 4 };
+
+// ---------------------------------------------------------------------------
+// Material coefficients (device), mirroring physics/*.py
+// ---------------------------------------------------------------------------
+__device__ bool stopping_power_dev(const MatDev &m, double E, double &out) {
+    if (!clip_energy(m.sp, E)) return false;
+    if (E == m.sp.E[m.sp.n - 1]) { out = m.sp.v[m.sp.n - 1]; return true; }
+    out = pchip_eval(m.sp, E);
+    return true;
+}
+
+__device__ bool transport_dev(const ConfigDev &cf, const MatDev &m, double E, double &out) {
+    if (cf.scattering == PDM1_SCATTERING_OFF) { out = 0.0; return true; }
+    if (cf.scattering == PDM1_SCATTERING_ROSSI) {
+        double e = E > 1.0e-8 ? E : 1.0e-8;
+        double M = kProtonRestMev;
+        double pv = e * (e + 2.0 * M) / (e + M);
+        double r = kRossiEsMev / pv;
+        out = r * r / m.X0;
+        return true;
+    }
+    if (!clip_energy(m.tr, E)) return false;
+    out = cf.interp == PDM1_INTERP_LINEAR ? linear_eval(m.tr, E) : pchip_eval(m.tr, E);
+    return true;
+}
+
+__device__ bool nuclear_dev(const ConfigDev &cf, const MatDev &m, double E, double &out) {
+    if (!clip_energy(m.nuc, E)) return false;
+    out = cf.interp == PDM1_INTERP_LINEAR ? linear_eval(m.nuc, E) : pchip_eval(m.nuc, E);
+    return true;
+}
+
+// numerics/boundary.py:82-114 spectrum factor
+__device__ __forceinline__ double energy_density(const ConfigDev &cf, double E) {
+    double de = E - cf.E_beam;
+    double s = cf.sigma_E;
+    return dd_exp(-(de * de) / (2.0 * (s * s))) / (sqrt(2.0 * 3.141592653589793) * s);
+}
+
+__device__ __forceinline__ void source_factor(double ts, double tn, bool inverse, double &fp, double &fc) {
+    double sign = inverse ? 1.0 : -1.0;
+    double a = tn < kExpClamp ? tn : kExpClamp;
+    double tsum = tn + ts;
+    double b = tsum < kExpClamp ? tsum : kExpClamp;
+    fp = dd_exp(sign * a);
+    fc = dd_exp(sign * b);
+}
+
+// ---------------------------------------------------------------------------
+// init: state at the start energy, S and spectrum for the first CFL
+// ---------------------------------------------------------------------------
+__global__ void init_kernel(const ConfigDev *cfp, Coeffs *co, MarchState *st, double *energies,
+                            double E0, int reset) {
+    const ConfigDev &cf = *cfp;
+    int t = threadIdx.x;
+    if (t < cf.nm) {
+        double s;
+        if (!stopping_power_dev(cf.mats[t], E0, s)) atomicOr(&st->error, ERR_DEV_RANGE);
+        co->S1[t] = s;
+    }
+    if (t == 0) {
+        co->ed_next = energy_density(cf, E0);
+        co->E_next = E0;
+        if (reset) {
+            st->E = E0;
+            st->inv_bits = 0ull;
+            st->forced_dE = 0.0;
+            st->step = 0;
+            st->done = 0;
+            st->ti = 0;
+            st->taken = 0;
+            st->error = 0;
+            if (energies) energies[0] = E0;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// prologue: one CTA per step
+// ---------------------------------------------------------------------------
+constexpr int kEvalPerMat = 13;   // 5 stage energies + 8 Gauss points
+
+__global__ void __launch_bounds__(256) prologue_kernel(const ConfigDev *cfp, Coeffs *co,
+                                                       MarchState *st, double *energies) {
+    const ConfigDev &cf = *cfp;
+    __shared__ double sE, sdE, sEn;
+    __shared__ int sActive, sSlot;
+    __shared__ double eS[kMaxMat][kEvalPerMat], eTr[kMaxMat][8], eNu[kMaxMat][8];
+    __shared__ double gpt[8];
+    int t = threadIdx.x;
+    if (t == 0) {
+        int active = 0, slot = -1;
+        double E = st->E, dE = 0.0, En = E;
+        if (!st->done && st->error == 0) {
+            if (!(E > cf.Emin) || (cf.step_limit >= 0 && st->step >= cf.step_limit)) {
+                st->done = 1;
+            } else if (st->step >= cf.max_steps) {
+                st->error |= ERR_DEV_MAXSTEPS;
+                st->done = 1;
+            } else {
+                if (st->forced_dE > 0.0) {
+                    dE = st->forced_dE;
+                } else {
+                    double inv = __longlong_as_double((long long)st->inv_bits);
+                    dE = cf.cfl / inv;
+                    dE = cf.max_dE < dE ? cf.max_dE : dE;
+                    if (st->ti < cf.n_targets) {
+                        double tg = cf.targets[st->ti];
+                        if (E > tg && tg >= E - dE) dE = E - tg;
+                    }
+                    if (E - cf.Emin < dE) dE = E - cf.Emin;
+                }
+                if (!(dE > 0.0) || !isfinite(dE)) {
+                    st->error |= ERR_DEV_NONFINITE;
+                    st->done = 1;
+                } else {
+                    active = 1;
+                    En = E - dE;
+                    int step = st->step + 1;
+                    if (energies) energies[step] = En;
+                    if (st->ti < cf.n_targets && fabs(En - cf.targets[st->ti]) <= 1e-12) {
+                        slot = st->taken;
+                        st->taken += 1;
+                        st->ti += 1;
+                    }
+                    st->step = step;
+                    st->E = En;
+                    st->inv_bits = 0ull;
+                    if (st->forced_dE > 0.0) st->done = 1;
+                }
+            }
+        }
+        sE = E; sdE = dE; sEn = En; sActive = active; sSlot = slot;
+        co->E = E; co->dE = dE; co->E_next = En; co->active = active; co->snap_slot = slot;
+    }
+    __syncthreads();
+    if (!sActive) return;
+    const double E = sE, dE = sdE;
+    // Gauss points for the depths over dE/3, dE/2, 2dE/3, dE (energy.py:919-949)
+    if (t < 4) {
+        const double width[4] = {dE / 3.0, 0.5 * dE, 2.0 * dE / 3.0, dE};
+        double w = width[t];
+        double mid = E - 0.5 * w;
+        double half = 0.5 * w;
+        double off = half / sqrt(3.0);
+        gpt[2 * t] = mid - off;
+        gpt[2 * t + 1] = mid + off;
+    }
+    __syncthreads();
+    int nm = cf.nm;
+    if (t < nm * kEvalPerMat) {
+        int m = t / kEvalPerMat, q = t % kEvalPerMat;
+        const MatDev &mat = cf.mats[m];
+        bool ok = true;
+        double e;
+        if (q < 5) {
+            const double stage_e[5] = {E, E - dE / 3.0, E - 2.0 * dE / 3.0, E - dE, E - 0.5 * dE};
+            e = stage_e[q];
+        } else {
+            e = gpt[q - 5];
+            double v = 0.0;
+            ok &= transport_dev(cf, mat, e, v);
+            eTr[m][q - 5] = v;
+            v = 0.0;
+            if (cf.nuclear) ok &= nuclear_dev(cf, mat, e, v);
+            eNu[m][q - 5] = v;
+        }
+        double s = 1.0;
+        ok &= stopping_power_dev(mat, e, s);
+        eS[m][q] = s;
+        if (!ok) atomicOr(&st->error, ERR_DEV_RANGE);
+    } else if (t >= 224 && t < 229) {
+        int q = t - 224;
+        const double ed_e[5] = {E, E - dE / 3.0, E - 2.0 * dE / 3.0, E - dE, E - dE};
+        double v = energy_density(cf, ed_e[q]);
+        if (q < 4) co->ed[q] = v; else co->ed_next = v;
+    }
+    __syncthreads();
+    if (t < nm) {
+        int m = t;
+        co->S0[m] = eS[m][0];
+        co->S1[m] = eS[m][3];
+        co->S2[m] = eS[m][4];
+        co->Sb[0][m] = eS[m][0];
+        co->Sb[1][m] = eS[m][1];
+        co->Sb[2][m] = eS[m][2];
+        co->Sb[3][m] = eS[m][3];
+        // optical depths, physics/scattering.py:267-306 and nuclear.py:202-233
+        double ts[4], tn[4];
+        const double width[4] = {dE / 3.0, 0.5 * dE, 2.0 * dE / 3.0, dE};
+        for (int d = 0; d < 4; ++d) {
+            double half = 0.5 * width[d];
+            ts[d] = 0.0;
+            tn[d] = 0.0;
+            if (cf.scattering != PDM1_SCATTERING_OFF)
+                ts[d] = half * (eTr[m][2 * d] / eS[m][5 + 2 * d] + eTr[m][2 * d + 1] / eS[m][6 + 2 * d]);
+            if (cf.nuclear)
+                tn[d] = half * (eNu[m][2 * d] / eS[m][5 + 2 * d] + eNu[m][2 * d + 1] / eS[m][6 + 2 * d]);
+        }
+        // depth index: 0 -> dE/3, 1 -> dE/2, 2 -> 2dE/3, 3 -> dE
+        double u1 = cf.use_if ? ts[3] : 0.0, n1 = cf.use_if ? tn[3] : 0.0;
+        double u2 = cf.use_if ? ts[1] : 0.0, n2 = cf.use_if ? tn[1] : 0.0;
+        source_factor(u1, n1, false, co->c1p[m], co->c1c[m]);
+        source_factor(u1, n1, true, co->c1ip[m], co->c1ic[m]);
+        source_factor(u2, n2, false, co->c2p[m], co->c2c[m]);
+        source_factor(u2, n2, true, co->c2ip[m], co->c2ic[m]);
+        co->fip[0][m] = 1.0;
+        co->fic[0][m] = 1.0;
+        const int didx[4] = {0, 0, 2, 3};
+        for (int q = 1; q < 4; ++q) {
+            double a = cf.use_if ? ts[didx[q]] : 0.0, b = cf.use_if ? tn[didx[q]] : 0.0;
+            source_factor(a, b, true, co->fip[q][m], co->fic[q][m]);
+        }
+        // Strang half steps over the full dE (energy.py:1168-1191, 1194-1260)
+        double th = 0.5 * tn[3];
+        co->hn[m] = (cf.strang && cf.nuclear) ? dd_exp(-(th < kExpClamp ? th : kExpClamp)) : 1.0;
+        th = 0.5 * ts[3];
+        co->hs[m] = (cf.strang && cf.scattering != PDM1_SCATTERING_OFF)
+                        ? dd_exp(-(th < kExpClamp ? th : kExpClamp)) : 1.0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The fused stage kernel
+// ---------------------------------------------------------------------------
+constexpr int TX = 4, TY = 8, TZ = 8;
+constexpr int NT = TX * TY * TZ;
+constexpr int NFX = (TX + 1) * TY * TZ;
+constexpr int NFY = TX * (TY + 1) * TZ;
+constexpr int NFZ = TX * TY * (TZ + 1);
+constexpr int NF = NFX + NFY + NFZ;
+constexpr int SX = (TX + 6) * TY * TZ;   // x-arm including the core
+constexpr int SY = TX * 6 * TZ;          // y halo
+constexpr int SZ = TX * TY * 6;          // z halo
+constexpr size_t kStageSmem = sizeof(double) * 4 * (SX + SY + SZ + NF);
+
+enum StageMode { MODE_A = 0, MODE_B = 1, MODE_C = 2, MODE_EULER = 3, MODE_RHS = 4 };
+
+struct StageArgs {
+    const ConfigDev *cf;
+    const Coeffs *co;
+    MarchState *st;
+    double *U;          // accepted state (in/out)
+    double *U1;         // stage states
+    double *U2;
+    double *V;          // marched variable of stage 1 / 2
+    double *qpart;      // (q0 + q1)/6 quadrature part
+    double *dose;       // accumulated dose (MODE_C / MODE_EULER), or NULL
+    double *edep;       // when non-NULL: energy deposition written instead of dose
+    double *snap;       // snapshot buffer base (slot * 4N)
+    double *rhs_out;    // MODE_RHS output
+    const double *bc_plane;   // MODE_RHS: explicit z-min boundary state (4,nx,ny)
+    double rhs_energy_density;
+};
+
+struct Smem {
+    double *X, *Y, *Z, *F;
+};
+
+__device__ __forceinline__ double sval(const Smem &s, int c, int i, int j, int k) {
+    if (j < 0) return s.Y[((c * TX + i) * 6 + (j + 3)) * TZ + k];
+    if (j >= TY) return s.Y[((c * TX + i) * 6 + (j - TY + 3)) * TZ + k];
+    if (k < 0) return s.Z[((c * TX + i) * TY + j) * 6 + (k + 3)];
+    if (k >= TZ) return s.Z[((c * TX + i) * TY + j) * 6 + (k - TZ + 3)];
+    return s.X[((c * (TX + 6) + (i + 3)) * TY + j) * TZ + k];
+}
+
+template <int MODE>
+__device__ __forceinline__ void load_cell(const StageArgs &a, const ConfigDev &cf, const Coeffs &co,
+                                          const double *src, size_t N, int gi, int gj, int gk,
+                                          double out[4]) {
+    int nx = cf.nx, ny = cf.ny, nz = cf.nz;
+    gi = gi < 0 ? 0 : (gi >= nx ? nx - 1 : gi);
+    gj = gj < 0 ? 0 : (gj >= ny ? ny - 1 : gj);
+    gk = gk >= nz ? nz - 1 : gk;
+    size_t o = ((size_t)gi * ny + gj) * nz + gk;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) out[c] = src[c * N + o];
+    if ((MODE == MODE_A || MODE == MODE_EULER) && cf.strang) {
+        int m = cf.ids[o];
+        double hn = co.hn[m], hs = co.hs[m];
+        if (cf.nuclear)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) out[c] *= hn;
+        if (cf.scattering != PDM1_SCATTERING_OFF)
+#pragma unroll
+            for (int c = 1; c < 4; ++c) out[c] *= hs;
+    }
+}
+
+// z-min boundary value of component c at column (gi, gj) for this stage
+template <int MODE>
+__device__ __forceinline__ double boundary_value(const StageArgs &a, const ConfigDev &cf,
+                                                 const Coeffs &co, int c, int gi, int gj) {
+    if (MODE == MODE_RHS && a.bc_plane)
+        return a.bc_plane[((size_t)c * cf.nx + gi) * cf.ny + gj];
+    if (c == 1 || c == 2) return 0.0;
+    double sp = cf.spatial[(size_t)gi * cf.ny + gj];
+    if (MODE == MODE_A || MODE == MODE_EULER || MODE == MODE_RHS) {
+        double ed = MODE == MODE_RHS ? a.rhs_energy_density : co.ed[0];
+        double phi = sp * ed;
+        return c == 0 ? phi : cf.rf * phi;
+    }
+    // RK-consistent stage traces, numerics/energy.py:348-455 (107-231 without sources)
+    int m = cf.ids[((size_t)gi * cf.ny + gj) * cf.nz];
+    double V[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        double phi = sp * co.ed[q];
+        double x = c == 0 ? phi : cf.rf * phi;
+        double B = co.Sb[q][m] * x;
+        if (q > 0 && cf.use_if) B *= (c == 0 ? co.fip[q][m] : co.fic[q][m]);
+        V[q] = B;
+    }
+    if (MODE == MODE_B) {
+        double vs1 = 0.5 * (-9.0 * V[0] + 18.0 * V[1] - 9.0 * V[2] + 2.0 * V[3]);
+        if (cf.use_if) vs1 *= (c == 0 ? co.c1p[m] : co.c1c[m]);
+        return vs1 / co.S1[m];
+    }
+    double vs2 = 0.25 * (11.0 * V[0] - 27.0 * V[1] + 27.0 * V[2] - 7.0 * V[3]);
+    if (cf.use_if) vs2 *= (c == 0 ? co.c2p[m] : co.c2c[m]);
+    return vs2 / co.S2[m];
+}
+
+__device__ __forceinline__ void cfl_contrib(const ConfigDev &cf, const Coeffs &co, const double u[4],
+                                            int m, int gi, int gj, int gk, double &inv) {
+    double a0, a1, a2;
+    if (cf.unit_speeds) {
+        a0 = a1 = a2 = 1.0;
+    } else {
+        a0 = max_abs_speed(u[0], u[1], u[2], u[3], 0);
+        a1 = max_abs_speed(u[0], u[1], u[2], u[3], 1);
+        a2 = max_abs_speed(u[0], u[1], u[2], u[3], 2);
+        if (gk == 0) {
+            double phi = cf.spatial[(size_t)gi * cf.ny + gj] * co.ed_next;
+            double jz = cf.rf * phi;
+            double ain = max_abs_speed(phi, 0.0, 0.0, jz, 2);
+            if (ain > a2) a2 = ain;
+        }
+    }
+    double s = co.S1[m];
+    inv = a0 / (s * cf.dx) + a1 / (s * cf.dy) + a2 / (s * cf.dz);
+}
+
+__device__ __forceinline__ void block_max_atomic(double v, unsigned long long *target) {
+    // v >= 0 or NaN; NaN never wins (fmax), like the oracle's comparison loop
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    __shared__ double wmax[NT / 32];
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) wmax[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        v = l < NT / 32 ? wmax[l] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (l == 0 && v > 0.0) atomicMax(target, (unsigned long long)__double_as_longlong(v));
+    }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(NT, 2) stage_kernel(StageArgs a) {
+    const ConfigDev &cf = *a.cf;
+    const Coeffs &co = *a.co;
+    if (MODE != MODE_RHS && !co.active) return;
+    extern __shared__ double smem[];
+    Smem s;
+    s.X = smem;
+    s.Y = s.X + 4 * SX;
+    s.Z = s.Y + 4 * SY;
+    s.F = s.Z + 4 * SZ;
+    const int nx = cf.nx, ny = cf.ny, nz = cf.nz;
+    const size_t N = (size_t)nx * ny * nz;
+    const int tiles_y = (ny + TY - 1) / TY, tiles_z = (nz + TZ - 1) / TZ;
+    const int tid = threadIdx.x;
+    const double *src = (MODE == MODE_B) ? a.U1 : (MODE == MODE_C ? a.U2 : a.U);
+    double cta_inv = 0.0;
+
+    int tile = blockIdx.x;
+    const int tz = tile % tiles_z, ty = (tile / tiles_z) % tiles_y, tx = tile / (tiles_z * tiles_y);
+    const int i0 = tx * TX, j0 = ty * TY, k0 = tz * TZ;
+
+    // ---- 1. stage the stencil source + halo ----
+    for (int e = tid; e < SX; e += NT) {
+        int k = e % TZ, j = (e / TZ) % TY, ii = e / (TZ * TY);
+        double u[4];
+        load_cell<MODE>(a, cf, co, src, N, i0 + ii - 3, j0 + j, k0 + k, u);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) s.X[((c * (TX + 6) + ii) * TY + j) * TZ + k] = u[c];
+    }
+    for (int e = tid; e < SY; e += NT) {
+        int k = e % TZ, jj = (e / TZ) % 6, i = e / (TZ * 6);
+        int gj = jj < 3 ? j0 + jj - 3 : j0 + TY + jj - 3;
+        double u[4];
+        load_cell<MODE>(a, cf, co, src, N, i0 + i, gj, k0 + k, u);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) s.Y[((c * TX + i) * 6 + jj) * TZ + k] = u[c];
+    }
+    for (int e = tid; e < SZ; e += NT) {
+        int kk = e % 6, j = (e / 6) % TY, i = e / (6 * TY);
+        int gk = kk < 3 ? k0 + kk - 3 : k0 + TZ + kk - 3;
+        if (gk < 0) continue;   // z-min ghost, filled below
+        double u[4];
+        load_cell<MODE>(a, cf, co, src, N, i0 + i, j0 + j, gk, u);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) s.Z[((c * TX + i) * TY + j) * 6 + kk] = u[c];
+    }
+    __syncthreads();
+    // ---- 2. z-min ghost cells: quartic extrapolation through the inflow ----
+    if (k0 == 0) {
+        for (int e = tid; e < 4 * TX * TY; e += NT) {
+            int j = e % TY, i = (e / TY) % TX, c = e / (TX * TY);
+            int gi = i0 + i, gj = j0 + j;
+            if (gi >= nx || gj >= ny) continue;
+            double ui = boundary_value<MODE>(a, cf, co, c, gi, gj);
+            const double *col = &s.X[((c * (TX + 6) + (i + 3)) * TY + j) * TZ];
+            double u0 = col[0], u1 = col[1], u2 = col[2], u3 = col[3];
+            double *z = &s.Z[((c * TX + i) * TY + j) * 6];
+            z[2] = 5.0 * ui - (77.0 / 12.0) * u0 + (43.0 / 12.0) * u1 - (17.0 / 12.0) * u2 + 0.25 * u3;
+            z[1] = 25.0 * ui - (505.0 / 12.0) * u0 + (335.0 / 12.0) * u1 - (145.0 / 12.0) * u2 + (9.0 / 4.0) * u3;
+            z[0] = 75.0 * ui - (545.0 / 4.0) * u0 + (395.0 / 4.0) * u1 - (181.0 / 4.0) * u2 + (35.0 / 4.0) * u3;
+        }
+        __syncthreads();
+    }
+    // ---- 3. every face of the tile: WENO-Z, projection, HLL ----
+    const bool unit = cf.unit_speeds != 0;
+    for (int f = tid; f < NF; f += NT) {
+        int axis, i, j, k;
+        if (f < NFX) {
+            axis = 0; k = f % TZ; j = (f / TZ) % TY; i = f / (TZ * TY);          // face left of cell i
+        } else if (f < NFX + NFY) {
+            int u = f - NFX;
+            axis = 1; k = u % TZ; j = (u / TZ) % (TY + 1); i = u / (TZ * (TY + 1));
+        } else {
+            int u = f - NFX - NFY;
+            axis = 2; k = u % (TZ + 1); j = (u / (TZ + 1)) % TY; i = u / ((TZ + 1) * TY);
+        }
+        double L[4], R[4];
+        const int di = axis == 0, dj = axis == 1, dk = axis == 2;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            double w[6];
+#pragma unroll
+            for (int q = 0; q < 6; ++q) {
+                int o = q - 3;
+                w[q] = sval(s, c, i + o * di, j + o * dj, k + o * dk);
+            }
+            L[c] = weno_left(w[0], w[1], w[2], w[3], w[4]);
+            R[c] = weno_left(w[5], w[4], w[3], w[2], w[1]);
+        }
+        project(L[0], L[1], L[2], L[3]);
+        project(R[0], R[1], R[2], R[3]);
+        double F[4];
+        hll_flux(L, R, axis, unit, F);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) s.F[c * NF + f] = F[c];
+    }
+    __syncthreads();
+    // ---- 4. divergence and the stage update, one cell per thread ----
+    const int k = tid % TZ, j = (tid / TZ) % TY, i = tid / (TZ * TY);
+    const int gi = i0 + i, gj = j0 + j, gk = k0 + k;
+    const bool valid = gi < nx && gj < ny && gk < nz;
+    if (valid) {
+        const int fx0 = (i * TY + j) * TZ + k, fx1 = ((i + 1) * TY + j) * TZ + k;
+        const int fy0 = NFX + (i * (TY + 1) + j) * TZ + k, fy1 = NFX + (i * (TY + 1) + j + 1) * TZ + k;
+        const int fz0 = NFX + NFY + (i * TY + j) * (TZ + 1) + k, fz1 = fz0 + 1;
+        double L[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const double *F = s.F + c * NF;
+            double gx = (F[fx1] - F[fx0]) / cf.dx;
+            double gy = (F[fy1] - F[fy0]) / cf.dy;
+            double gz = (F[fz1] - F[fz0]) / cf.dz;
+            L[c] = -(gx + gy + gz);
+        }
+        const size_t o = ((size_t)gi * ny + gj) * nz + gk;
+        if (MODE == MODE_RHS) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) a.rhs_out[c * N + o] = L[c];
+        } else {
+            const int m = cf.ids[o];
+            const double dE = co.dE;
+            // the accepted state at this cell (with the Strang half step applied)
+            double un[4];
+            if (MODE == MODE_A || MODE == MODE_EULER) {
+#pragma unroll
+                for (int c = 0; c < 4; ++c) un[c] = s.X[((c * (TX + 6) + (i + 3)) * TY + j) * TZ + k];
+            } else {
+                load_cell<MODE_A>(a, cf, co, a.U, N, gi, gj, gk, un);
+            }
+            const double s0 = co.S0[m];
+            if (MODE == MODE_A) {
+                double u1[4], v1[4];
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    double v0 = s0 * un[c];
+                    double v = L[c] * dE + v0;
+                    v1[c] = v;
+                    double w = v * (c == 0 ? co.c1p[m] : co.c1c[m]);
+                    u1[c] = w / co.S1[m];
+                }
+                project(u1[0], u1[1], u1[2], u1[3]);
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    a.U1[c * N + o] = u1[c];
+                    a.V[c * N + o] = v1[c];
+                }
+                double q0 = un[0] * s0, q1 = u1[0] * co.S1[m];
+                a.qpart[o] = 1.0 / 6.0 * q0 + 1.0 / 6.0 * q1;
+            } else if (MODE == MODE_B) {
+                double u2[4];
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    double r = L[c] * (c == 0 ? co.c1ip[m] : co.c1ic[m]);
+                    r = (r * dE + a.V[c * N + o]) * 0.25;
+                    double v = 0.75 * (s0 * un[c]) + r;
+                    a.V[c * N + o] = v;
+                    double w = v * (c == 0 ? co.c2p[m] : co.c2c[m]);
+                    u2[c] = w / co.S2[m];
+                }
+                project(u2[0], u2[1], u2[2], u2[3]);
+#pragma unroll
+                for (int c = 0; c < 4; ++c) a.U2[c * N + o] = u2[c];
+            } else {
+                double unew[4];
+                double ed;
+                if (MODE == MODE_C) {
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        double r = L[c] * (c == 0 ? co.c2ip[m] : co.c2ic[m]);
+                        r = (r * dE + a.V[c * N + o]) * (2.0 / 3.0);
+                        double v = 1.0 / 3.0 * (s0 * un[c]) + r;
+                        double w = v * (c == 0 ? co.c1p[m] : co.c1c[m]);
+                        unew[c] = w / co.S1[m];
+                    }
+                    project(unew[0], unew[1], unew[2], unew[3]);
+                    double q2 = s.X[((0 * (TX + 6) + (i + 3)) * TY + j) * TZ + k] * co.S2[m];
+                    ed = dE * (a.qpart[o] + 2.0 / 3.0 * q2);
+                } else {   // forward Euler, numerics/energy.py:663-722
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        double w = L[c] * dE + s0 * un[c];
+                        unew[c] = w / co.S1[m];
+                    }
+                    project(unew[0], unew[1], unew[2], unew[3]);
+                    ed = dE * un[0] * s0;
+                }
+                if (cf.strang) {
+                    if (cf.nuclear)
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) unew[c] *= co.hn[m];
+                    if (cf.scattering != PDM1_SCATTERING_OFF)
+#pragma unroll
+                        for (int c = 1; c < 4; ++c) unew[c] *= co.hs[m];
+                }
+                double *dst = MODE == MODE_C ? a.U : a.U1;
+#pragma unroll
+                for (int c = 0; c < 4; ++c) dst[c * N + o] = unew[c];
+                if (a.edep) a.edep[o] = ed;
+                else a.dose[o] += ed * kMevToJoule / cf.mats[m].density;
+                if (MODE == MODE_C) {
+                    if (co.snap_slot >= 0 && a.snap) {
+                        double *sn = a.snap + (size_t)co.snap_slot * 4 * N;
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) sn[c * N + o] = unew[c];
+                    }
+                    cfl_contrib(cf, co, unew, m, gi, gj, gk, cta_inv);
+                }
+            }
+        }
+    }
+    if (MODE == MODE_C) block_max_atomic(cta_inv, &a.st->inv_bits);
+}
+
+// Forward Euler writes U1; this copies it back, snapshots and reduces the CFL.
+__global__ void __launch_bounds__(NT) euler_finish_kernel(StageArgs a) {
+    const ConfigDev &cf = *a.cf;
+    const Coeffs &co = *a.co;
+    if (!co.active) return;
+    const size_t N = (size_t)cf.nx * cf.ny * cf.nz;
+    double inv = 0.0;
+    for (size_t o = (size_t)blockIdx.x * NT + threadIdx.x; o < N; o += (size_t)gridDim.x * NT) {
+        double u[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            u[c] = a.U1[c * N + o];
+            a.U[c * N + o] = u[c];
+        }
+        if (co.snap_slot >= 0 && a.snap) {
+            double *sn = a.snap + (size_t)co.snap_slot * 4 * N;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) sn[c * N + o] = u[c];
+        }
+        int gk = (int)(o % cf.nz), gj = (int)((o / cf.nz) % cf.ny), gi = (int)(o / ((size_t)cf.nz * cf.ny));
+        double v;
+        cfl_contrib(cf, co, u, cf.ids[o], gi, gj, gk, v);
+        inv = fmax(inv, v);
+    }
+    block_max_atomic(inv, &a.st->inv_bits);
+}
+
+// CFL bound of a state (energy.py:539-660) with S and spectrum of co->S1 / ed_next.
+__global__ void __launch_bounds__(NT) cfl_kernel(const ConfigDev *cfp, const Coeffs *co,
+                                                 MarchState *st, const double *U) {
+    const ConfigDev &cf = *cfp;
+    const size_t N = (size_t)cf.nx * cf.ny * cf.nz;
+    double inv = 0.0;
+    for (size_t o = (size_t)blockIdx.x * NT + threadIdx.x; o < N; o += (size_t)gridDim.x * NT) {
+        double u[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) u[c] = U[c * N + o];
+        int gk = (int)(o % cf.nz), gj = (int)((o / cf.nz) % cf.ny), gi = (int)(o / ((size_t)cf.nz * cf.ny));
+        double v;
+        cfl_contrib(cf, *co, u, cf.ids[o], gi, gj, gk, v);
+        inv = fmax(inv, v);
+    }
+    block_max_atomic(inv, &st->inv_bits);
+}
+
+// Scalar batches for unit parity checks
+__global__ void weno_batch_kernel(const double *v, double *out, int n) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) out[t] = weno_left(v[5 * t], v[5 * t + 1], v[5 * t + 2], v[5 * t + 3], v[5 * t + 4]);
+}
+__global__ void project_batch_kernel(double *u, int n) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) project(u[4 * t], u[4 * t + 1], u[4 * t + 2], u[4 * t + 3]);
+}
+__global__ void eigen_batch_kernel(const double *u, int axis, double *out, int n) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) {
+        const double *p = u + 4 * t;
+        double jn = sqrt(p[1] * p[1] + p[2] * p[2] + p[3] * p[3]);
+        double lo, hi;
+        eigen(p[0], p[1], p[2], p[3], jn, axis, lo, hi);
+        out[2 * t] = lo;
+        out[2 * t + 1] = hi;
+    }
+}
+__global__ void hll_batch_kernel(const double *L, const double *R, int axis, int unit, double *F, int n) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) {
+        double l[4], r[4], f[4];
+        for (int c = 0; c < 4; ++c) { l[c] = L[4 * t + c]; r[c] = R[4 * t + c]; }
+        hll_flux(l, r, axis, unit != 0, f);
+        for (int c = 0; c < 4; ++c) F[4 * t + c] = f[c];
+    }
+}
+__global__ void exp_batch_kernel(const double *x, double *y, int n) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) y[t] = dd_exp(x[t]);
+}
+__global__ void coeff_eval_kernel(const ConfigDev *cfp, const double *E, int n, double *out, int *err) {
+    const ConfigDev &cf = *cfp;
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n * cf.nm) return;
+    int e = t / cf.nm, m = t % cf.nm;
+    double s = 0, tr = 0, nu = 0;
+    bool ok = stopping_power_dev(cf.mats[m], E[e], s);
+    ok &= transport_dev(cf, cf.mats[m], E[e], tr);
+    ok &= nuclear_dev(cf, cf.mats[m], E[e], nu);
+    if (!ok) atomicOr(err, 1);
+    out[3 * t] = s;
+    out[3 * t + 1] = tr;
+    out[3 * t + 2] = nu;
+}
+
+// ---------------------------------------------------------------------------
+// Host side: tables, plan
+// ---------------------------------------------------------------------------
+double sign_of(double x) { return (double)((x > 0.0) - (x < 0.0)); }
+
+double pchip_endpoint(double h0, double h1, double d0, double d1) {
+    double slope = ((2.0 * h0 + h1) * d0 - h0 * d1) / (h0 + h1);
+    if (sign_of(slope) != sign_of(d0)) return 0.0;
+    if (sign_of(d0) != sign_of(d1) && std::fabs(slope) > 3.0 * std::fabs(d0)) return 3.0 * d0;
+    return slope;
+}
+
+// physics/stopping_power.py:94-138 (coefficient_interpolation.py:19-48)
+std::vector<double> pchip_slopes(const double *E, const double *v, int n) {
+    std::vector<double> h(n - 1), d(n - 1), s(n, 0.0);
+    for (int i = 0; i < n - 1; ++i) {
+        h[i] = E[i + 1] - E[i];
+        d[i] = (v[i + 1] - v[i]) / h[i];
+    }
+    if (n == 2) {
+        s[0] = s[1] = d[0];
+        return s;
+    }
+    for (int k = 1; k < n - 1; ++k) {
+        if (d[k - 1] * d[k] > 0.0) {
+            double w1 = 2.0 * h[k] + h[k - 1];
+            double w2 = h[k] + 2.0 * h[k - 1];
+            s[k] = (w1 + w2) / (w1 / d[k - 1] + w2 / d[k]);
+        }
+    }
+    s[0] = pchip_endpoint(h[0], h[1], d[0], d[1]);
+    s[n - 1] = pchip_endpoint(h[n - 2], h[n - 3], d[n - 2], d[n - 3]);
+    return s;
+}
+
+}  // namespace
+
+struct pdm1_plan {
+    pdm1_problem p{};
+    ConfigDev cf{};
+    ConfigDev *d_cf = nullptr;
+    Coeffs *d_co = nullptr;
+    MarchState *d_st = nullptr;
+    MarchState *h_st = nullptr;   // pinned
+    double *d_tables = nullptr;
+    int32_t *d_ids = nullptr;
+    double *d_spatial = nullptr;
+    double *d_targets = nullptr;
+    double *d_U1 = nullptr, *d_U2 = nullptr, *d_V = nullptr, *d_q = nullptr;
+    size_t workspace = 0;
+    std::vector<int32_t> h_ids;
+    std::vector<double> h_spatial;
+    // per material: [lo, hi] of the stopping-power, transport, nuclear tables
+    std::vector<double> range[3][2];
+    cudaStream_t own_stream = nullptr;
+    cudaEvent_t ready = nullptr;
+    cudaEvent_t ev[2 * kStepsPerGraph] = {};   // stage-kernel timing, one pair per step of a chunk
+};
+
+namespace {
+
+bool table_ok(const pdm1_table &t) {
+    if (t.n_nodes < 2 || !t.energy || !t.value) return false;
+    for (int i = 0; i + 1 < t.n_nodes; ++i)
+        if (!(t.energy[i + 1] > t.energy[i])) return false;
+    return true;
+}
+
+// Upload one table; return its TableView (device pointers).
+TableView add_table(std::vector<double> &blob, std::vector<std::pair<size_t, int>> &fix,
+                    const pdm1_table &t) {
+    TableView v{};
+    v.n = t.n_nodes;
+    size_t base = blob.size();
+    blob.insert(blob.end(), t.energy, t.energy + t.n_nodes);
+    blob.insert(blob.end(), t.value, t.value + t.n_nodes);
+    std::vector<double> sl = pchip_slopes(t.energy, t.value, t.n_nodes);
+    blob.insert(blob.end(), sl.begin(), sl.end());
+    fix.push_back({base, t.n_nodes});
+    // log-spaced node guess when the spacing in log E is uniform to 1e-9
+    double l0 = std::log(t.energy[0]), l1 = std::log(t.energy[t.n_nodes - 1]);
+    double step = (l1 - l0) / (t.n_nodes - 1);
+    bool uniform = t.energy[0] > 0.0 && step > 0.0;
+    for (int i = 0; uniform && i < t.n_nodes; i += 97)
+        if (std::fabs(std::log(t.energy[i]) - (l0 + step * i)) > 1e-6 * step) uniform = false;
+    v.log_e0 = l0;
+    v.inv_log_step = uniform ? 1.0 / step : 0.0;
+    return v;
+}
+
+int validate_problem(const pdm1_problem *p) {
+    if (!p) return set_error(PDM1_ERR_ARGUMENT, "problem is NULL");
+    if (p->nx <= 0 || p->ny <= 0 || p->nz <= 0) return set_error(PDM1_ERR_ARGUMENT, "grid dimensions must be positive");
+    if (p->nz < 4) return set_error(PDM1_ERR_ARGUMENT, "WENO-Z inflow extrapolation requires at least four z cells.");
+    if (p->n_materials < 1 || p->n_materials > kMaxMat) return set_error(PDM1_ERR_ARGUMENT, "n_materials must be in 1..16");
+    if (!p->materials || !p->ids || !p->inflow_spatial) return set_error(PDM1_ERR_ARGUMENT, "NULL materials/ids/inflow");
+    if (!(p->dx > 0 && p->dy > 0 && p->dz > 0)) return set_error(PDM1_ERR_ARGUMENT, "spacings must be positive");
+    if (!(p->energy_spread > 0.0))
+        return set_error(PDM1_ERR_ARGUMENT, "Zero energy spread is not supported by the Gaussian inflow.");
+    if (!(p->cfl > 0.0 && p->cfl <= 1.0)) return set_error(PDM1_ERR_ARGUMENT, "cfl must lie in (0, 1].");
+    if (!(p->max_energy_step > 0.0)) return set_error(PDM1_ERR_ARGUMENT, "max_energy_step must be positive.");
+    if (p->energy_scheme < 0 || p->energy_scheme > 2) return set_error(PDM1_ERR_UNSUPPORTED, "unknown energy scheme");
+    if (p->precision != PDM1_FP64 && p->precision != PDM1_FP32_FP64) return set_error(PDM1_ERR_ARGUMENT, "unknown precision");
+    if (p->moving_active_domain) return set_error(PDM1_ERR_UNSUPPORTED, "moving_active_domain is not built in this library version");
+    for (int m = 0; m < p->n_materials; ++m) {
+        const pdm1_material &mt = p->materials[m];
+        if (!table_ok(mt.stopping_power) || !table_ok(mt.transport) || !table_ok(mt.nuclear))
+            return set_error(PDM1_ERR_ARGUMENT, "coefficient tables need >= 2 strictly increasing nodes");
+        if (!(mt.density > 0.0)) return set_error(PDM1_ERR_ARGUMENT, "density must be positive");
+    }
+    size_t n = (size_t)p->nx * p->ny * p->nz;
+    for (size_t c = 0; c < n; ++c)
+        if (p->ids[c] < 0 || p->ids[c] >= p->n_materials) return set_error(PDM1_ERR_ARGUMENT, "material id out of range");
+    return PDM1_OK;
+}
+
+bool is_close(double a, double b) { return std::fabs(a - b) <= 1e-8 + 1e-5 * std::fabs(b); }
+
+// Energy range the march will evaluate tables at: [energy_min, E_start]
+int check_energy_range(const pdm1_plan *pl, double e_hi, double e_lo) {
+    const pdm1_problem &p = pl->p;
+    const bool used[3] = {true, p.scattering == PDM1_SCATTERING_WENTZEL, p.nuclear != 0};
+    for (int m = 0; m < p.n_materials; ++m) {
+        for (int q = 0; q < 3; ++q) {
+            if (!used[q]) continue;
+            double lo = pl->range[q][0][m], hi = pl->range[q][1][m];
+            if ((e_hi > hi && !is_close(e_hi, hi)) || (e_lo < lo && !is_close(e_lo, lo))) {
+                char buf[256];
+                snprintf(buf, sizeof buf, "Energy outside coefficient table range [%g, %g] MeV (march spans [%g, %g] MeV).",
+                         lo, hi, e_lo, e_hi);
+                return set_error(PDM1_ERR_RANGE, buf);
+            }
+        }
+    }
+    return PDM1_OK;
+}
+
+StageArgs make_args(pdm1_plan *pl, double *U, double *dose, double *edep, double *snap) {
+    StageArgs a{};
+    a.cf = pl->d_cf;
+    a.co = pl->d_co;
+    a.st = pl->d_st;
+    a.U = U;
+    a.U1 = pl->d_U1;
+    a.U2 = pl->d_U2;
+    a.V = pl->d_V;
+    a.qpart = pl->d_q;
+    a.dose = dose;
+    a.edep = edep;
+    a.snap = snap;
+    return a;
+}
+
+int n_tiles(const pdm1_problem &p) {
+    return ((p.nx + TX - 1) / TX) * ((p.ny + TY - 1) / TY) * ((p.nz + TZ - 1) / TZ);
+}
+
+int cell_blocks(const pdm1_problem &p) {
+    size_t n = (size_t)p.nx * p.ny * p.nz;
+    size_t b = (n + NT - 1) / NT;
+    return (int)std::min<size_t>(b, 148 * 8);
+}
+
+// Launch one energy step (prologue + stages) on `stream`; returns launches.
+int launch_step(pdm1_plan *pl, const StageArgs &a, cudaStream_t stream) {
+    const pdm1_problem &p = pl->p;
+    int tiles = n_tiles(p);
+    prologue_kernel<<<1, 256, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, nullptr);
+    if (p.energy_scheme == PDM1_SCHEME_FORWARD_EULER) {
+        stage_kernel<MODE_EULER><<<tiles, NT, kStageSmem, stream>>>(a);
+        euler_finish_kernel<<<cell_blocks(p), NT, 0, stream>>>(a);
+        return 3;
+    }
+    stage_kernel<MODE_A><<<tiles, NT, kStageSmem, stream>>>(a);
+    stage_kernel<MODE_B><<<tiles, NT, kStageSmem, stream>>>(a);
+    stage_kernel<MODE_C><<<tiles, NT, kStageSmem, stream>>>(a);
+    return 4;
+}
+
+int launch_step_with_energies(pdm1_plan *pl, const StageArgs &a, double *energies, cudaStream_t stream,
+                              int slot) {
+    const pdm1_problem &p = pl->p;
+    int tiles = n_tiles(p);
+    prologue_kernel<<<1, 256, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, energies);
+    cudaEventRecord(pl->ev[2 * slot], stream);
+    int n;
+    if (p.energy_scheme == PDM1_SCHEME_FORWARD_EULER) {
+        stage_kernel<MODE_EULER><<<tiles, NT, kStageSmem, stream>>>(a);
+        n = 1;
+    } else {
+        stage_kernel<MODE_A><<<tiles, NT, kStageSmem, stream>>>(a);
+        stage_kernel<MODE_B><<<tiles, NT, kStageSmem, stream>>>(a);
+        stage_kernel<MODE_C><<<tiles, NT, kStageSmem, stream>>>(a);
+        n = 3;
+    }
+    cudaEventRecord(pl->ev[2 * slot + 1], stream);
+    if (p.energy_scheme == PDM1_SCHEME_FORWARD_EULER) {
+        euler_finish_kernel<<<cell_blocks(p), NT, 0, stream>>>(a);
+        return 3;
+    }
+    return n + 1;
+}
+
+int set_smem_attributes() {
+    static bool done = false;
+    if (done) return PDM1_OK;
+    CUDA_TRY(cudaFuncSetAttribute(stage_kernel<MODE_A>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageSmem));
+    CUDA_TRY(cudaFuncSetAttribute(stage_kernel<MODE_B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageSmem));
+    CUDA_TRY(cudaFuncSetAttribute(stage_kernel<MODE_C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageSmem));
+    CUDA_TRY(cudaFuncSetAttribute(stage_kernel<MODE_EULER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageSmem));
+    CUDA_TRY(cudaFuncSetAttribute(stage_kernel<MODE_RHS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageSmem));
+    done = true;
+    return PDM1_OK;
+}
+
+int device_error_status(const MarchState &st) {
+    if (st.error & ERR_DEV_RANGE) return set_error(PDM1_ERR_RANGE, "energy outside a coefficient table during the march");
+    if (st.error & ERR_DEV_MAXSTEPS) return set_error(PDM1_ERR_MAX_STEPS, "energies buffer shorter than the march");
+    if (st.error & ERR_DEV_NONFINITE) return set_error(PDM1_ERR_NONFINITE, "non-finite or non-positive energy step");
+    return PDM1_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *pdm1_last_error(void) { return g_error.c_str(); }
+const char *pdm1_version(void) { return "pdm1 0.1 sm_100a"; }
+
+void pdm1_plan_destroy(pdm1_plan *pl) {
+    if (!pl) return;
+    cudaFree(pl->d_cf);
+    cudaFree(pl->d_co);
+    cudaFree(pl->d_st);
+    cudaFreeHost(pl->h_st);
+    cudaFree(pl->d_tables);
+    cudaFree(pl->d_ids);
+    cudaFree(pl->d_spatial);
+    cudaFree(pl->d_targets);
+    cudaFree(pl->d_U1);
+    cudaFree(pl->d_U2);
+    cudaFree(pl->d_V);
+    cudaFree(pl->d_q);
+    if (pl->ready) cudaEventDestroy(pl->ready);
+    for (cudaEvent_t e : pl->ev)
+        if (e) cudaEventDestroy(e);
+    if (pl->own_stream) cudaStreamDestroy(pl->own_stream);
+    delete pl;
+}
+
+int pdm1_plan_create(const pdm1_problem *problem, pdm1_plan **out) {
+    if (!out) return set_error(PDM1_ERR_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    int rc = validate_problem(problem);
+    if (rc) return rc;
+    rc = set_smem_attributes();
+    if (rc) return rc;
+    pdm1_plan *pl = new pdm1_plan();
+    pl->p = *problem;
+    const pdm1_problem &p = pl->p;
+    size_t N = (size_t)p.nx * p.ny * p.nz;
+    pl->h_ids.assign(problem->ids, problem->ids + N);
+    pl->h_spatial.assign(problem->inflow_spatial, problem->inflow_spatial + (size_t)p.nx * p.ny);
+    pl->p.ids = pl->h_ids.data();
+    pl->p.inflow_spatial = pl->h_spatial.data();
+    pl->p.materials = nullptr;   // tables are copied below; host pointers are not kept
+
+    std::vector<double> blob;
+    std::vector<std::pair<size_t, int>> fix;
+    ConfigDev &cf = pl->cf;
+    cf.nx = p.nx; cf.ny = p.ny; cf.nz = p.nz;
+    cf.dx = p.dx; cf.dy = p.dy; cf.dz = p.dz;
+    cf.nm = p.n_materials;
+    cf.scattering = p.scattering;
+    cf.nuclear = p.nuclear ? 1 : 0;
+    cf.interp = p.interpolation;
+    cf.scheme = p.energy_scheme;
+    cf.unit_speeds = p.wave_speeds == PDM1_SPEEDS_UNIT;
+    bool sources = p.scattering != PDM1_SCATTERING_OFF || p.nuclear;
+    cf.use_if = (p.energy_scheme == PDM1_SCHEME_IF_SSPRK3 && sources) ? 1 : 0;
+    cf.strang = (p.energy_scheme != PDM1_SCHEME_IF_SSPRK3 && sources) ? 1 : 0;
+    cf.cfl = p.cfl;
+    cf.max_dE = p.max_energy_step;
+    cf.Emin = p.energy_min;
+    cf.E_beam = p.beam_energy;
+    cf.sigma_E = p.energy_spread;
+    cf.rf = dd_exp(-(p.angular_spread * p.angular_spread));
+    for (int m = 0; m < p.n_materials; ++m) {
+        const pdm1_material &mt = problem->materials[m];
+        cf.mats[m].sp = add_table(blob, fix, mt.stopping_power);
+        cf.mats[m].tr = add_table(blob, fix, mt.transport);
+        cf.mats[m].nuc = add_table(blob, fix, mt.nuclear);
+        cf.mats[m].density = mt.density;
+        cf.mats[m].X0 = mt.radiation_length;
+        const pdm1_table *tabs[3] = {&mt.stopping_power, &mt.transport, &mt.nuclear};
+        for (int q = 0; q < 3; ++q) {
+            pl->range[q][0].push_back(tabs[q]->energy[0]);
+            pl->range[q][1].push_back(tabs[q]->energy[tabs[q]->n_nodes - 1]);
+        }
+    }
+    auto fail = [&](int code) { pdm1_plan_destroy(pl); return code; };
+    cudaError_t e;
+#define ALLOC(ptr, bytes)                                                      \
+    e = cudaMalloc((void **)&(ptr), (bytes));                                  \
+    if (e != cudaSuccess) {                                                    \
+        set_error(PDM1_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e)); \
+        return fail(PDM1_ERR_CUDA);                                            \
+    }
+    ALLOC(pl->d_tables, blob.size() * sizeof(double));
+    ALLOC(pl->d_cf, sizeof(ConfigDev));
+    ALLOC(pl->d_co, sizeof(Coeffs));
+    ALLOC(pl->d_st, sizeof(MarchState));
+    ALLOC(pl->d_ids, N * sizeof(int32_t));
+    ALLOC(pl->d_spatial, (size_t)p.nx * p.ny * sizeof(double));
+    ALLOC(pl->d_targets, 64 * sizeof(double));
+    ALLOC(pl->d_U1, 4 * N * sizeof(double));
+    ALLOC(pl->d_U2, 4 * N * sizeof(double));
+    ALLOC(pl->d_V, 4 * N * sizeof(double));
+    ALLOC(pl->d_q, N * sizeof(double));
+#undef ALLOC
+    pl->workspace = (13 * N) * sizeof(double);
+    if (cudaMallocHost((void **)&pl->h_st, sizeof(MarchState)) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&pl->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&pl->ready, cudaEventDisableTiming) != cudaSuccess)
+        return fail(set_error(PDM1_ERR_CUDA, "cudaMallocHost/stream/event creation failed"));
+    for (cudaEvent_t &ev : pl->ev)
+        if (cudaEventCreate(&ev) != cudaSuccess) return fail(set_error(PDM1_ERR_CUDA, "cudaEventCreate failed"));
+    // patch table pointers to device addresses
+    int ti = 0;
+    for (int m = 0; m < p.n_materials; ++m) {
+        TableView *views[3] = {&cf.mats[m].sp, &cf.mats[m].tr, &cf.mats[m].nuc};
+        for (TableView *v : views) {
+            size_t base = fix[ti++].first;
+            v->E = pl->d_tables + base;
+            v->v = pl->d_tables + base + v->n;
+            v->slope = pl->d_tables + base + 2 * v->n;
+        }
+    }
+    cf.ids = pl->d_ids;
+    cf.spatial = pl->d_spatial;
+    cf.targets = pl->d_targets;
+    if (cudaMemcpy(pl->d_tables, blob.data(), blob.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(pl->d_ids, pl->h_ids.data(), N * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(pl->d_spatial, pl->h_spatial.data(), (size_t)p.nx * p.ny * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(pl->d_cf, &cf, sizeof(ConfigDev), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(pl->d_co, 0, sizeof(Coeffs)) != cudaSuccess)
+        return fail(set_error(PDM1_ERR_CUDA, "plan upload failed"));
+    *out = pl;
+    return PDM1_OK;
+}
+
+size_t pdm1_plan_workspace_bytes(const pdm1_plan *pl) { return pl ? pl->workspace : 0; }
+
+static int march_impl(pdm1_plan *pl, double *U, double *dose, double *energies, int max_steps,
+                      const double *snap_targets, int n_snap, double *snap_out, double *snap_E_out,
+                      pdm1_march_info *info, pdm1_stream_t stream_, int step_limit) {
+    if (!pl || !U || !dose || !energies || max_steps < 1)
+        return set_error(PDM1_ERR_ARGUMENT, "pdm1_march: NULL buffer or max_steps < 1");
+    cudaStream_t stream = (cudaStream_t)stream_;
+    if (stream == nullptr) {
+        // the legacy default stream cannot be captured into a graph: order the
+        // plan's own stream after it and march there
+        CUDA_TRY(cudaEventRecord(pl->ready, nullptr));
+        CUDA_TRY(cudaStreamWaitEvent(pl->own_stream, pl->ready, 0));
+        stream = pl->own_stream;
+    }
+    const pdm1_problem &p = pl->p;
+    double E0 = p.beam_energy + p.energy_window_sigma * p.energy_spread;
+    int rc = check_energy_range(pl, E0, p.energy_min);
+    if (rc) return rc;
+    // sorted unique targets in [energy_min, E0], descending (energy.py:1531-1538)
+    std::vector<double> tg;
+    for (int i = 0; i < n_snap; ++i) {
+        double t = snap_targets[i];
+        if (p.energy_min <= t && t <= E0 && std::find(tg.begin(), tg.end(), t) == tg.end()) tg.push_back(t);
+    }
+    std::sort(tg.begin(), tg.end(), [](double a, double b) { return a > b; });
+    if (tg.size() > 64) return set_error(PDM1_ERR_ARGUMENT, "at most 64 snapshot energies");
+    if (!tg.empty() && !snap_out) return set_error(PDM1_ERR_ARGUMENT, "snap_out is NULL");
+    pl->cf.n_targets = (int)tg.size();
+    pl->cf.max_steps = max_steps;
+    pl->cf.step_limit = step_limit;
+    CUDA_TRY(cudaMemcpyAsync(pl->d_cf, &pl->cf, sizeof(ConfigDev), cudaMemcpyHostToDevice, stream));
+    if (!tg.empty())
+        CUDA_TRY(cudaMemcpyAsync(pl->d_targets, tg.data(), tg.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+    size_t N = (size_t)p.nx * p.ny * p.nz;
+    CUDA_TRY(cudaMemsetAsync(dose, 0, N * sizeof(double), stream));
+    init_kernel<<<1, 32, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, energies, E0, 1);
+    cfl_kernel<<<cell_blocks(p), NT, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, U);
+    CUDA_TRY(cudaGetLastError());
+    int launches = 2;
+    StageArgs a = make_args(pl, U, dose, nullptr, snap_out);
+    // capture a chunk of steps into a graph; replay until the device says done
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int per_step = 0;
+    bool use_graph = true;
+    if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        for (int s = 0; s < kStepsPerGraph; ++s) per_step = launch_step_with_energies(pl, a, energies, stream, s);
+        if (cudaStreamEndCapture(stream, &graph) != cudaSuccess ||
+            cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+            use_graph = false;
+        }
+    } else {
+        use_graph = false;
+    }
+    cudaGetLastError();
+    int replays = 0, prev_step = 0, stage_launches = 0;
+    double stage_ms = 0.0;
+    const int stages_per_step = p.energy_scheme == PDM1_SCHEME_FORWARD_EULER ? 1 : 3;
+    for (;;) {
+        if (use_graph) {
+            CUDA_TRY(cudaGraphLaunch(exec, stream));
+            replays++;
+        } else {
+            for (int s = 0; s < kStepsPerGraph; ++s) per_step = launch_step_with_energies(pl, a, energies, stream, s);
+        }
+        CUDA_TRY(cudaMemcpyAsync(pl->h_st, pl->d_st, sizeof(MarchState), cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        int ran = pl->h_st->step - prev_step;   // steps of this chunk that did work
+        prev_step = pl->h_st->step;
+        launches += ran * per_step + (kStepsPerGraph - ran) * per_step;
+        for (int s = 0; s < ran && s < kStepsPerGraph; ++s) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, pl->ev[2 * s], pl->ev[2 * s + 1]) == cudaSuccess) stage_ms += ms;
+        }
+        stage_launches += ran * stages_per_step;
+        if (pl->h_st->done || pl->h_st->error) break;
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    rc = device_error_status(*pl->h_st);
+    if (info) {
+        info->n_steps = pl->h_st->step;
+        info->n_snapshots = pl->h_st->taken;
+        info->final_state_valid = 1;
+        info->graph_replays = replays;
+        info->kernel_launches = launches;
+        info->stage_launches = stage_launches;
+        info->stage_ms = stage_ms;
+    }
+    if (snap_E_out)
+        for (int i = 0; i < pl->h_st->taken; ++i) snap_E_out[i] = tg[i];
+    return rc;
+}
+
+int pdm1_march(pdm1_plan *pl, double *U, double *dose, double *energies, int max_steps,
+               const double *snap_targets, int n_snap, double *snap_out, double *snap_E_out,
+               pdm1_march_info *info, pdm1_stream_t stream) {
+    return march_impl(pl, U, dose, energies, max_steps, snap_targets, n_snap, snap_out, snap_E_out,
+                      info, stream, -1);
+}
+
+int pdm1_march_steps(pdm1_plan *pl, double *U, double *dose, double *energies, int max_steps,
+                     int step_limit, pdm1_march_info *info, pdm1_stream_t stream) {
+    if (step_limit < 0) return set_error(PDM1_ERR_ARGUMENT, "step_limit must be >= 0");
+    return march_impl(pl, U, dose, energies, max_steps, nullptr, 0, nullptr, nullptr, info, stream,
+                      step_limit);
+}
+
+int pdm1_spatial_operator(pdm1_plan *pl, const double *U, double energy, const double *bc, double *rhs,
+                          pdm1_stream_t stream_) {
+    if (!pl || !U || !rhs) return set_error(PDM1_ERR_ARGUMENT, "NULL argument");
+    cudaStream_t stream = (cudaStream_t)stream_;
+    StageArgs a = make_args(pl, const_cast<double *>(U), nullptr, nullptr, nullptr);
+    a.rhs_out = rhs;
+    a.bc_plane = bc;
+    double de = energy - pl->p.beam_energy, s = pl->p.energy_spread;
+    a.rhs_energy_density = dd_exp(-(de * de) / (2.0 * (s * s))) / (std::sqrt(2.0 * 3.141592653589793) * s);
+    stage_kernel<MODE_RHS><<<n_tiles(pl->p), NT, kStageSmem, stream>>>(a);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(stream));
+    return PDM1_OK;
+}
+
+int pdm1_energy_step(pdm1_plan *pl, const double *U, double energy, double *dE_out, pdm1_stream_t stream_) {
+    if (!pl || !U || !dE_out) return set_error(PDM1_ERR_ARGUMENT, "NULL argument");
+    cudaStream_t stream = (cudaStream_t)stream_;
+    int rc = check_energy_range(pl, energy, energy);
+    if (rc) return rc;
+    init_kernel<<<1, 32, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, nullptr, energy, 1);
+    cfl_kernel<<<cell_blocks(pl->p), NT, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, U);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(pl->h_st, pl->d_st, sizeof(MarchState), cudaMemcpyDeviceToHost, stream));
+    CUDA_TRY(cudaStreamSynchronize(stream));
+    rc = device_error_status(*pl->h_st);
+    if (rc) return rc;
+    double inv = 0.0;
+    unsigned long long bits = pl->h_st->inv_bits;
+    std::memcpy(&inv, &bits, sizeof inv);
+    double dE = pl->p.cfl / inv;
+    *dE_out = pl->p.max_energy_step < dE ? pl->p.max_energy_step : dE;
+    return PDM1_OK;
+}
+
+int pdm1_advance(pdm1_plan *pl, double *U, double energy, double dE, double *edep, pdm1_stream_t stream_) {
+    if (!pl || !U || !edep || !(dE > 0.0)) return set_error(PDM1_ERR_ARGUMENT, "dE must be positive.");
+    cudaStream_t stream = (cudaStream_t)stream_;
+    int rc = check_energy_range(pl, energy, energy - dE);
+    if (rc) return rc;
+    pl->cf.n_targets = 0;
+    pl->cf.max_steps = 1;
+    pl->cf.step_limit = -1;
+    CUDA_TRY(cudaMemcpyAsync(pl->d_cf, &pl->cf, sizeof(ConfigDev), cudaMemcpyHostToDevice, stream));
+    init_kernel<<<1, 32, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, nullptr, energy, 1);
+    MarchState st{};
+    st.E = energy;
+    st.forced_dE = dE;
+    CUDA_TRY(cudaMemcpyAsync(pl->d_st, &st, sizeof st, cudaMemcpyHostToDevice, stream));
+    StageArgs a = make_args(pl, U, nullptr, edep, nullptr);
+    launch_step(pl, a, stream);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(pl->h_st, pl->d_st, sizeof(MarchState), cudaMemcpyDeviceToHost, stream));
+    CUDA_TRY(cudaStreamSynchronize(stream));
+    return device_error_status(*pl->h_st);
+}
+
+int pdm1_coefficients(pdm1_plan *pl, const double *E, int n, double *out) {
+    if (!pl || !E || !out || n <= 0) return set_error(PDM1_ERR_ARGUMENT, "NULL argument");
+    double *dE_ = nullptr, *dout = nullptr;
+    int *derr = nullptr;
+    int nm = pl->p.n_materials;
+    CUDA_TRY(cudaMalloc(&dE_, n * sizeof(double)));
+    CUDA_TRY(cudaMalloc(&dout, (size_t)n * nm * 3 * sizeof(double)));
+    CUDA_TRY(cudaMalloc(&derr, sizeof(int)));
+    CUDA_TRY(cudaMemcpy(dE_, E, n * sizeof(double), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemset(derr, 0, sizeof(int)));
+    int total = n * nm;
+    coeff_eval_kernel<<<(total + 127) / 128, 128>>>(pl->d_cf, dE_, n, dout, derr);
+    CUDA_TRY(cudaGetLastError());
+    int herr = 0;
+    CUDA_TRY(cudaMemcpy(out, dout, (size_t)total * 3 * sizeof(double), cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost));
+    cudaFree(dE_);
+    cudaFree(dout);
+    cudaFree(derr);
+    if (herr) return set_error(PDM1_ERR_RANGE, "energy outside coefficient table range");
+    return PDM1_OK;
+}
+
+#define BATCH(kernel, ...)                                                 \
+    if (n <= 0) return PDM1_OK;                                            \
+    kernel<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(__VA_ARGS__); \
+    CUDA_TRY(cudaGetLastError());                                          \
+    CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));                 \
+    return PDM1_OK;
+
+int pdm1_weno_batch(const double *v5, double *out, int n, pdm1_stream_t stream) { BATCH(weno_batch_kernel, v5, out, n) }
+int pdm1_project_batch(double *u4, int n, pdm1_stream_t stream) { BATCH(project_batch_kernel, u4, n) }
+int pdm1_eigen_batch(const double *u4, int axis, double *lo_hi, int n, pdm1_stream_t stream) {
+    BATCH(eigen_batch_kernel, u4, axis, lo_hi, n)
+}
+int pdm1_hll_batch(const double *l, const double *r, int axis, int ws, double *f, int n, pdm1_stream_t stream) {
+    BATCH(hll_batch_kernel, l, r, axis, ws, f, n)
+}
+int pdm1_exp_batch(const double *x, double *y, int n, pdm1_stream_t stream) { BATCH(exp_batch_kernel, x, y, n) }
+
+}  // extern "C"

@@ -1,0 +1,305 @@
+// pdm1_math.cuh -- scalar M1 building blocks shared by the march kernels.
+//
+// Every expression keeps the evaluation order of the reference's FP64 path
+// (cited per function, paths relative to the proton_solver project).  The
+// double-precision translation unit is compiled with --fmad=false, so each
+// product and sum is rounded separately, as NumPy does.
+#pragma once
+
+#include <cmath>
+#include <cstdint>
+
+#define PDM1_HD __host__ __device__ __forceinline__
+
+namespace pdm1 {
+
+constexpr double kEigEps = 1.0e-10;          // numerics/wave_speeds.py:10
+constexpr double kWenoEps = 1.0e-12;         // reconstruction_methods/weno_z.py:8
+constexpr double kRealEps = 1.0e-10;         // weno_z.py:10, realizability.py:110
+constexpr double kMevToJoule = 1.602176634e-13;   // numerics/energy.py:37
+constexpr double kExpClamp = 700.0;          // numerics/energy.py:296-304
+constexpr double kProtonRestMev = 938.27208816;   // physics/scattering.py:21
+constexpr double kRossiEsMev = 15.0;              // physics/scattering.py:22
+
+// ---------------------------------------------------------------------------
+// exp in double-double arithmetic: Cody-Waite reduction with ln 2 held as a
+// double-double, exp(r / 2^10) by a degree-9 Taylor series (Dekker/Knuth
+// error-free sums, FMA products), ten squarings, scaling by 2^k.  Good to
+// about 1e-29 relative before the final rounding, i.e. correctly rounded but
+// for rare ties; the same routine runs on the host and the device.
+// ---------------------------------------------------------------------------
+struct dd { double hi, lo; };
+
+PDM1_HD dd dd_quick(double a, double b) { dd r; r.hi = a + b; r.lo = b - (r.hi - a); return r; }
+
+PDM1_HD dd dd_add(dd a, dd b) {
+    double s = a.hi + b.hi;
+    double bb = s - a.hi;
+    double e = (a.hi - (s - bb)) + (b.hi - bb);
+    e += a.lo + b.lo;
+    return dd_quick(s, e);
+}
+
+PDM1_HD dd dd_mul(dd a, dd b) {
+    double p = a.hi * b.hi;
+    double e = fma(a.hi, b.hi, -p);
+    e += a.hi * b.lo + a.lo * b.hi;
+    return dd_quick(p, e);
+}
+
+PDM1_HD dd dd_div_d(double a, double b) {
+    double q1 = a / b;
+    double p = q1 * b;
+    double e = fma(q1, b, -p);
+    double rem = (a - p) - e;
+    return dd_quick(q1, rem / b);
+}
+
+PDM1_HD double dd_exp(double x) {
+    if (x != x) return x;
+    if (x > 709.782712893384) return INFINITY;
+    if (x < -745.2) return 0.0;
+    const double ln2_hi = 0.6931471805599453094;
+    const double ln2_lo = 2.3190468138462996e-17;
+    double k = rint(x * 1.4426950408889634);
+    double p = k * ln2_hi;
+    double pe = fma(k, ln2_hi, -p);
+    double s = x - p;
+    double t = -pe - k * ln2_lo;
+    dd r = dd_quick(s, t);
+    r.hi *= 0x1p-10;
+    r.lo *= 0x1p-10;
+    const double fact[10] = {1.0, 1.0, 2.0, 6.0, 24.0, 120.0, 720.0, 5040.0, 40320.0, 362880.0};
+    dd acc = dd_div_d(1.0, fact[9]);
+    for (int n = 8; n >= 0; --n) acc = dd_add(dd_mul(acc, r), dd_div_d(1.0, fact[n]));
+    for (int q = 0; q < 10; ++q) acc = dd_mul(acc, acc);
+    return ldexp(acc.hi + acc.lo, (int)k);
+}
+
+// ---------------------------------------------------------------------------
+// WENO-Z5 left reconstruction, reconstruction_methods/weno_z.py:12-87
+// ---------------------------------------------------------------------------
+template <typename T>
+PDM1_HD T weno_left(T v0, T v1, T v2, T v3, T v4) {
+    const T c3 = T(3), c6 = T(6);
+    T p0 = v0 / c3 - T(7) * v1 / c6 + T(11) * v2 / c6;
+    T p1 = -v1 / c6 + T(5) * v2 / c6 + v3 / c3;
+    T p2 = v2 / c3 + T(5) * v3 / c6 - v4 / c6;
+    const T k1312 = T(13.0 / 12.0);
+    T a, b;
+    a = v0 - T(2) * v1 + v2; b = v0 - T(4) * v1 + T(3) * v2;
+    T beta0 = k1312 * (a * a) + T(0.25) * (b * b);
+    a = v1 - T(2) * v2 + v3; b = v1 - v3;
+    T beta1 = k1312 * (a * a) + T(0.25) * (b * b);
+    a = v2 - T(2) * v3 + v4; b = T(3) * v2 - T(4) * v3 + v4;
+    T beta2 = k1312 * (a * a) + T(0.25) * (b * b);
+    T tau5 = fabs(beta2 - beta0);
+    T r0 = tau5 / (beta0 + T(kWenoEps));
+    T r1 = tau5 / (beta1 + T(kWenoEps));
+    T r2 = tau5 / (beta2 + T(kWenoEps));
+    T al0 = T(0.1) * (T(1) + r0 * r0);
+    T al1 = T(0.6) * (T(1) + r1 * r1);
+    T al2 = T(0.3) * (T(1) + r2 * r2);
+    T s = al0 + al1 + al2;
+    T w0 = al0 / s, w1 = al1 / s, w2 = al2 / s;
+    return w0 * p0 + w1 * p1 + w2 * p2;
+}
+
+// ---------------------------------------------------------------------------
+// Realizability projection, numerics/realizability.py:132-176
+// ---------------------------------------------------------------------------
+template <typename T>
+PDM1_HD void project(T &phi, T &jx, T &jy, T &jz) {
+    if (phi < T(0)) phi = T(0);
+    T jn = sqrt(jx * jx + jy * jy + jz * jz);
+    T jmax = T(1.0 - kRealEps) * phi;
+    if (jn > jmax) {
+        T s = jmax / jn;
+        jx *= s; jy *= s; jz *= s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Exact M1 eigenvalues along an axis: numerics/flux.py:63-135
+// (== numerics/wave_speeds.py:36-103)
+// ---------------------------------------------------------------------------
+template <typename T>
+PDM1_HD void eigen(T phi, T jx, T jy, T jz, T jn, int axis, T &lmin, T &lmax) {
+    const T iso = T(1) / sqrt(T(3));
+    if (phi < T(kEigEps)) phi = T(kEigEps);
+    if (jn < T(kEigEps)) { lmin = -iso; lmax = iso; return; }
+    T f = jn / phi;
+    if (f < T(0)) f = T(0);
+    else if (f > T(1.0 - kEigEps)) f = T(1.0 - kEigEps);
+    T jnormal = axis == 0 ? jx : (axis == 1 ? jy : jz);
+    T mu = jnormal / jn;
+    T chi = (T(5) - T(2) * sqrt(T(4) - T(3) * f * f)) / T(3);
+    T den = T(5) - T(3) * chi;
+    T disc = T(4) * f * f * mu * mu - den * (mu * mu * (T(3) * chi - T(1)) - T(2) * (T(1) - chi));
+    if (disc < T(0)) disc = T(0);
+    T root = sqrt(disc);
+    lmin = (T(2) * f * mu - root) / den;
+    lmax = (T(2) * f * mu + root) / den;
+}
+
+template <typename T>
+PDM1_HD T max_abs_speed(T phi, T jx, T jy, T jz, int axis) {
+    T jn = sqrt(jx * jx + jy * jy + jz * jz);
+    T lo, hi;
+    eigen(phi, jx, jy, jz, jn, axis, lo, hi);
+    T alo = fabs(lo), ahi = fabs(hi);
+    return alo > ahi ? alo : ahi;
+}
+
+// ---------------------------------------------------------------------------
+// M1 closure and HLL flux, numerics/flux.py:10-61 and 137-386
+// ---------------------------------------------------------------------------
+template <typename T>
+struct Closure { T jn, nx, ny, nz, iso, dir; };
+
+template <typename T>
+PDM1_HD Closure<T> closure(T phi, T jx, T jy, T jz) {
+    Closure<T> c;
+    c.jn = sqrt(jx * jx + jy * jy + jz * jz);
+    T f;
+    if (phi > T(0)) {
+        f = c.jn / phi;
+        if (f < T(0)) f = T(0);
+        else if (f > T(1)) f = T(1);
+    } else {
+        f = T(0);
+    }
+    T chi = (T(5) - T(2) * sqrt(T(4) - T(3) * f * f)) / T(3);
+    if (c.jn > T(0)) {
+        c.nx = jx / c.jn; c.ny = jy / c.jn; c.nz = jz / c.jn;
+    } else {
+        c.nx = c.ny = c.nz = T(0);
+    }
+    c.iso = T(0.5) * (T(1) - chi);
+    c.dir = T(0.5) * (T(3) * chi - T(1));
+    return c;
+}
+
+template <typename T>
+PDM1_HD void physical_flux(const T u[4], const Closure<T> &c, int axis, T F[4]) {
+    T phi = u[0];
+    if (axis == 0) {
+        F[0] = u[1];
+        F[1] = phi * (c.iso + c.dir * c.nx * c.nx);
+        F[2] = phi * c.dir * c.nx * c.ny;
+        F[3] = phi * c.dir * c.nx * c.nz;
+    } else if (axis == 1) {
+        F[0] = u[2];
+        F[1] = phi * c.dir * c.nx * c.ny;
+        F[2] = phi * (c.iso + c.dir * c.ny * c.ny);
+        F[3] = phi * c.dir * c.ny * c.nz;
+    } else {
+        F[0] = u[3];
+        F[1] = phi * c.dir * c.nx * c.nz;
+        F[2] = phi * c.dir * c.ny * c.nz;
+        F[3] = phi * (c.iso + c.dir * c.nz * c.nz);
+    }
+}
+
+template <typename T>
+PDM1_HD void hll_flux(const T L[4], const T R[4], int axis, bool unit_speeds, T F[4]) {
+    Closure<T> cl = closure(L[0], L[1], L[2], L[3]);
+    Closure<T> cr = closure(R[0], R[1], R[2], R[3]);
+    T FL[4], FR[4];
+    physical_flux(L, cl, axis, FL);
+    physical_flux(R, cr, axis, FR);
+    T sl, sr;
+    if (!unit_speeds) {
+        T lminl, lmaxl, lminr, lmaxr;
+        eigen(L[0], L[1], L[2], L[3], cl.jn, axis, lminl, lmaxl);
+        eigen(R[0], R[1], R[2], R[3], cr.jn, axis, lminr, lmaxr);
+        sl = lminr < lminl ? lminr : lminl;
+        sr = lmaxr > lmaxl ? lmaxr : lmaxl;
+        if (sl > T(0)) sl = T(0);
+        if (sr < T(0)) sr = T(0);
+    } else {
+        sl = T(-1);
+        sr = T(1);
+    }
+    T den = sr - sl;
+    T sp = sl * sr;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) F[c] = (sr * FL[c] - sl * FR[c] + sp * (R[c] - L[c])) / den;
+}
+
+// ---------------------------------------------------------------------------
+// Coefficient tables (physics/stopping_power.py, coefficient_interpolation.py,
+// numpy.interp).  A table is n nodes of (energy, value, PCHIP slope); the
+// energies are log-spaced, which gives a first guess of the interval that
+// is then corrected by comparisons, so the index is exactly
+// numpy.searchsorted(energy, x, side="right") - 1.
+// ---------------------------------------------------------------------------
+struct TableView {
+    const double *E, *v, *slope;
+    int n;
+    double log_e0, inv_log_step;   // inv_log_step == 0: no log guess
+};
+
+PDM1_HD int search_right(const TableView &t, double x) {
+    int g;
+    if (t.inv_log_step > 0.0 && x > 0.0) {
+        double gf = (log(x) - t.log_e0) * t.inv_log_step;
+        g = gf < 0.0 ? 0 : (gf > (double)(t.n - 1) ? t.n - 1 : (int)gf);
+    } else {
+        int lo = 0, hi = t.n;
+        while (lo < hi) {
+            int mid = (lo + hi) >> 1;
+            if (t.E[mid] <= x) lo = mid + 1; else hi = mid;
+        }
+        return lo - 1;
+    }
+    while (g >= 0 && t.E[g] > x) --g;
+    while (g + 1 < t.n && t.E[g + 1] <= x) ++g;
+    return g;
+}
+
+PDM1_HD double pchip_eval(const TableView &t, double x) {
+    int n = t.n;
+    if (x >= t.E[n - 1]) return t.v[n - 1];
+    int i = search_right(t, x);
+    if (i < 0) i = 0;
+    if (i > n - 2) i = n - 2;
+    double h = t.E[i + 1] - t.E[i];
+    double s = (x - t.E[i]) / h;
+    double s2 = s * s;
+    double s3 = s2 * s;
+    double h00 = 2.0 * s3 - 3.0 * s2 + 1.0;
+    double h10 = s3 - 2.0 * s2 + s;
+    double h01 = -2.0 * s3 + 3.0 * s2;
+    double h11 = s3 - s2;
+    return h00 * t.v[i] + h10 * h * t.slope[i] + h01 * t.v[i + 1] + h11 * h * t.slope[i + 1];
+}
+
+PDM1_HD double linear_eval(const TableView &t, double x) {
+    int n = t.n;
+    if (x < t.E[0]) return t.v[0];
+    if (x > t.E[n - 1]) return t.v[n - 1];
+    int j = search_right(t, x);
+    if (j >= n - 1) return t.v[n - 1];
+    if (t.E[j] == x) return t.v[j];
+    double slope = (t.v[j + 1] - t.v[j]) / (t.E[j + 1] - t.E[j]);
+    double r = slope * (x - t.E[j]) + t.v[j];
+    if (r != r) {
+        r = slope * (x - t.E[j + 1]) + t.v[j + 1];
+        if (r != r && t.v[j] == t.v[j + 1]) r = t.v[j];
+    }
+    return r;
+}
+
+// numpy.isclose(a, b) with rtol 1e-5, atol 1e-8; clip of stopping_power.py:151-170
+PDM1_HD bool clip_energy(const TableView &t, double &x) {
+    double lo = t.E[0], hi = t.E[t.n - 1];
+    bool close_lo = fabs(x - lo) <= 1e-8 + 1e-5 * fabs(lo);
+    bool close_hi = fabs(x - hi) <= 1e-8 + 1e-5 * fabs(hi);
+    if ((x < lo && !close_lo) || (x > hi && !close_hi)) return false;
+    if (x < lo) x = lo;
+    if (x > hi) x = hi;
+    return true;
+}
+
+}  // namespace pdm1

@@ -1,0 +1,246 @@
+"""The energy march: drop-in for proton_solver/numerics/energy.py:energy_march.
+
+``energy_march(U, material_map, grid, inflow, config, xp, snapshot_energies)``
+keeps the reference signature, argument meaning, exceptions and return
+contract ``(U | None, dose, energies, snapshots)``.  The work runs in
+libpdm1.so on the current CUDA device; PyTorch only provides device memory
+and the stream.  NumPy inputs give NumPy outputs, CUDA tensors give CUDA
+tensors, as the reference returns arrays of its ``xp``.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import math
+from typing import Any
+
+import numpy as np
+
+from .. import _native
+from ..physics.tables import material_tables
+
+MEV_TO_JOULE = 1.602176634e-13
+
+_SCATTER = {"OFF": 0, "ROSSI": 1, "WENTZEL": 2}
+_INTERP = {"LINEAR": 0, "PCHIP": 1}
+_SCHEME = {"FORWARD_EULER": 0, "SSPRK3": 1, "IF_SSPRK3": 2}
+_SPEEDS = {"EXACT": 0, "UNIT": 1}
+_PRECISION = {"FP64": 0, "FP32_FP64": 1}
+
+
+def _to_numpy(a):
+    if hasattr(a, "detach"):
+        return a.detach().cpu().numpy()
+    if hasattr(a, "get"):
+        return a.get()
+    return np.asarray(a)
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("the M1 march runs on a CUDA device; none is available")
+    return torch
+
+
+def _check_supported(config) -> None:
+    num, phys = config.numerics, config.physics
+    if num.spatial_scheme.name != "WENO_Z":
+        raise NotImplementedError(
+            f"spatial scheme {num.spatial_scheme.name} has no GPU kernel; only WENO_Z is built")
+    if getattr(num, "active_domain", False):
+        raise NotImplementedError("the legacy per-operator active_domain crop has no GPU kernel")
+    if num.energy_scheme.name not in _SCHEME:
+        raise NotImplementedError(f"Energy scheme {num.energy_scheme} has not been migrated yet.")
+    if config.beam.energy_spread == 0:
+        raise ValueError("Zero energy spread is not supported by the Gaussian inflow.")
+
+
+class M1Plan:
+    """One beam on one phantom, resident on the GPU (a ``pdm1_plan``)."""
+
+    def __init__(self, config, material_map, grid, inflow, precision: str | None = None):
+        _check_supported(config)
+        num, phys, beam = config.numerics, config.physics, config.beam
+        self.shape = tuple(int(n) for n in grid.shape)
+        self.config = config
+        ids = np.ascontiguousarray(_to_numpy(material_map.ids), dtype=np.int32)
+        if ids.shape != self.shape:
+            raise ValueError(f"material ids have shape {ids.shape}, expected {self.shape}")
+        spatial = np.ascontiguousarray(_to_numpy(inflow.spatial), dtype=np.float64)
+        materials = tuple(material_map.materials)
+        keep = [ids, spatial]
+        mats = (_native.Material * len(materials))()
+        for k, m in enumerate(materials):
+            t = material_tables(m.value)
+            arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in
+                    (t.sp_energy, t.sp_value, t.tr_energy, t.tr_value, t.nuc_energy, t.nuc_value)]
+            keep += arrs
+            ptr = [a.ctypes.data_as(C.POINTER(C.c_double)) for a in arrs]
+            mats[k] = _native.Material(_native.Table(len(arrs[0]), ptr[0], ptr[1]),
+                                       _native.Table(len(arrs[2]), ptr[2], ptr[3]),
+                                       _native.Table(len(arrs[4]), ptr[4], ptr[5]),
+                                       t.density, t.radiation_length)
+        if precision is None:
+            accel = getattr(config, "accel", None)
+            precision = accel.precision.name if accel is not None else "FP64"
+        p = _native.Problem()
+        p.nx, p.ny, p.nz = self.shape
+        p.dx, p.dy, p.dz = float(grid.dx), float(grid.dy), float(grid.dz)
+        p.n_materials = len(materials)
+        p.materials = mats
+        p.ids = ids.ctypes.data_as(C.POINTER(C.c_int32))
+        p.inflow_spatial = spatial.ctypes.data_as(C.POINTER(C.c_double))
+        p.beam_energy, p.energy_spread = beam.energy, beam.energy_spread
+        p.angular_spread = beam.angular_spread
+        p.scattering = _SCATTER[phys.scattering.name]
+        p.nuclear = int(bool(phys.nuclear))
+        p.interpolation = _INTERP[phys.coefficient_interpolation.name]
+        p.energy_scheme = _SCHEME[num.energy_scheme.name]
+        p.wave_speeds = _SPEEDS[num.wave_speeds.name]
+        p.max_energy_step, p.cfl = num.max_energy_step, num.cfl
+        p.energy_min, p.energy_window_sigma = num.energy_min, num.energy_window_sigma
+        p.moving_active_domain = int(bool(num.moving_active_domain))
+        p.vacuum_aware_cfl = int(bool(num.vacuum_aware_cfl))
+        p.active_guard_cells = int(num.active_guard_cells)
+        p.active_relative_tolerance = math.exp(-0.5 * num.active_truncation_sigma ** 2)
+        p.precision = _PRECISION[precision]
+        self.materials = materials
+        self.start_energy = beam.energy + num.energy_window_sigma * beam.energy_spread
+        h = C.c_void_p()
+        _native.check(_native.lib().pdm1_plan_create(C.byref(p), C.byref(h)))
+        self._h = h
+        self._keep = keep
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _native.lib().pdm1_plan_destroy(h)
+            self._h = None
+
+    __del__ = close
+
+    @property
+    def workspace_bytes(self) -> int:
+        return int(_native.lib().pdm1_plan_workspace_bytes(self._h))
+
+    @staticmethod
+    def _stream():
+        torch = _torch()
+        return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def max_steps_bound(self) -> int:
+        """A generous bound on the step count: dE >= cfl*S_min*d/(3*sqrt(3)) ... capped."""
+        return 2_000_000
+
+    def march_device(self, U, dose, energies, snapshot_energies=(), snap_out=None):
+        """Run the march on device tensors; return (n_steps, snapshot energies)."""
+        targets = np.ascontiguousarray(sorted({float(t) for t in snapshot_energies}), dtype=np.float64)
+        ns = len(targets)
+        snap_E = np.zeros(max(ns, 1))
+        info = _native.MarchInfo()
+        rc = _native.lib().pdm1_march(
+            self._h, C.c_void_p(U.data_ptr()), C.c_void_p(dose.data_ptr()),
+            C.c_void_p(energies.data_ptr()), int(energies.numel() - 1),
+            targets.ctypes.data_as(C.POINTER(C.c_double)) if ns else None, ns,
+            C.c_void_p(snap_out.data_ptr()) if snap_out is not None else None,
+            snap_E.ctypes.data_as(C.POINTER(C.c_double)), C.byref(info), self._stream())
+        _native.check(rc)
+        self.last_info = info
+        return info.n_steps, [float(snap_E[i]) for i in range(info.n_snapshots)]
+
+    def march(self, U=None, snapshot_energies=(), max_steps=200_000):
+        """(U, dose, energies, snapshots) with CUDA tensors for U/dose/snapshots."""
+        torch = _torch()
+        dev = torch.device("cuda", torch.cuda.current_device())
+        if U is None:
+            Ud = torch.zeros((4, *self.shape), dtype=torch.float64, device=dev)
+        else:
+            Ud = torch.as_tensor(U, dtype=torch.float64).to(dev).contiguous().clone()
+        dose = torch.empty(self.shape, dtype=torch.float64, device=dev)
+        energies = torch.empty(max_steps + 1, dtype=torch.float64, device=dev)
+        targets = sorted({float(t) for t in snapshot_energies})
+        snap = (torch.empty((len(targets), 4, *self.shape), dtype=torch.float64, device=dev)
+                if targets else None)
+        n, snap_E = self.march_device(Ud, dose, energies, targets, snap)
+        E = energies[: n + 1].cpu().numpy()
+        snapshots = {e: snap[i].clone() for i, e in enumerate(snap_E)}
+        return Ud, dose, E, snapshots
+
+    def march_steps(self, steps, U=None, max_steps=200_000):
+        """Run the first ``steps`` energy steps; return (U, dose, energies)."""
+        torch = _torch()
+        dev = torch.device("cuda", torch.cuda.current_device())
+        Ud = (torch.zeros((4, *self.shape), dtype=torch.float64, device=dev) if U is None else
+              torch.as_tensor(U, dtype=torch.float64).to(dev).contiguous().clone())
+        dose = torch.empty(self.shape, dtype=torch.float64, device=dev)
+        energies = torch.empty(max_steps + 1, dtype=torch.float64, device=dev)
+        info = _native.MarchInfo()
+        _native.check(_native.lib().pdm1_march_steps(
+            self._h, C.c_void_p(Ud.data_ptr()), C.c_void_p(dose.data_ptr()),
+            C.c_void_p(energies.data_ptr()), int(max_steps), int(steps), C.byref(info),
+            self._stream()))
+        self.last_info = info
+        return Ud, dose, energies[: info.n_steps + 1].cpu().numpy()
+
+    # -- building blocks (operator-level parity) --------------------------------
+    def spatial_operator(self, U, energy, boundary_state=None):
+        torch = _torch()
+        Ud = torch.as_tensor(U, dtype=torch.float64).cuda().contiguous()
+        bc = None if boundary_state is None else torch.as_tensor(
+            boundary_state, dtype=torch.float64).cuda().contiguous()
+        rhs = torch.empty_like(Ud)
+        _native.check(_native.lib().pdm1_spatial_operator(
+            self._h, C.c_void_p(Ud.data_ptr()), float(energy),
+            C.c_void_p(bc.data_ptr()) if bc is not None else None,
+            C.c_void_p(rhs.data_ptr()), self._stream()))
+        return rhs
+
+    def energy_step(self, U, energy):
+        torch = _torch()
+        Ud = torch.as_tensor(U, dtype=torch.float64).cuda().contiguous()
+        out = C.c_double()
+        _native.check(_native.lib().pdm1_energy_step(
+            self._h, C.c_void_p(Ud.data_ptr()), float(energy), C.byref(out), self._stream()))
+        return out.value
+
+    def advance(self, U, energy, dE):
+        torch = _torch()
+        Ud = torch.as_tensor(U, dtype=torch.float64).cuda().contiguous().clone()
+        edep = torch.empty(self.shape, dtype=torch.float64, device=Ud.device)
+        _native.check(_native.lib().pdm1_advance(
+            self._h, C.c_void_p(Ud.data_ptr()), float(energy), float(dE),
+            C.c_void_p(edep.data_ptr()), self._stream()))
+        return Ud, edep
+
+    def coefficients(self, energies):
+        E = np.ascontiguousarray(energies, dtype=np.float64)
+        out = np.empty((len(E), len(self.materials), 3))
+        _native.check(_native.lib().pdm1_coefficients(
+            self._h, E.ctypes.data_as(C.POINTER(C.c_double)), len(E),
+            out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+
+def energy_march(U: Any, material_map, grid, inflow, config, xp=None,
+                 snapshot_energies: tuple[float, ...] = ()):
+    """March the M1 system from high to low kinetic energy on the GPU.
+
+    Same contract as proton_solver/numerics/energy.py:1497-1643.
+    """
+    if not config.numerics.moving_active_domain and U is None:
+        raise ValueError("A full-grid initial state is required when moving_active_domain "
+                         "is disabled.")
+    host = U is None or not hasattr(U, "is_cuda") or not U.is_cuda
+    plan = M1Plan(config, material_map, grid, inflow)
+    try:
+        Ud, dose, energies, snaps = plan.march(U, snapshot_energies)
+    finally:
+        plan.close()
+    store = getattr(getattr(config, "output", None), "store_final_state", True)
+    if config.numerics.moving_active_domain and not store:
+        Ud = None
+    if host:
+        conv = lambda t: None if t is None else t.cpu().numpy()
+        return conv(Ud), conv(dose), energies, {e: conv(s) for e, s in snaps.items()}
+    return Ud, dose, energies, snaps
