@@ -944,7 +944,8 @@ int launch_step_with_energies(pdm1_plan *pl, const StageArgs &a, double *energie
     const pdm1_problem &p = pl->p;
     int tiles = n_tiles(p);
     prologue_kernel<<<1, 256, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, energies);
-    cudaEventRecord(pl->ev[2 * slot], stream);
+    // external event nodes: real timestamps when the step is replayed from a graph
+    cudaEventRecordWithFlags(pl->ev[2 * slot], stream, cudaEventRecordExternal);
     int n;
     if (p.energy_scheme == PDM1_SCHEME_FORWARD_EULER) {
         stage_kernel<MODE_EULER><<<tiles, NT, kStageSmem, stream>>>(a);
@@ -955,7 +956,7 @@ int launch_step_with_energies(pdm1_plan *pl, const StageArgs &a, double *energie
         stage_kernel<MODE_C><<<tiles, NT, kStageSmem, stream>>>(a);
         n = 3;
     }
-    cudaEventRecord(pl->ev[2 * slot + 1], stream);
+    cudaEventRecordWithFlags(pl->ev[2 * slot + 1], stream, cudaEventRecordExternal);
     if (p.energy_scheme == PDM1_SCHEME_FORWARD_EULER) {
         euler_finish_kernel<<<cell_blocks(p), NT, 0, stream>>>(a);
         return 3;
@@ -1147,6 +1148,7 @@ static int march_impl(pdm1_plan *pl, double *U, double *dose, double *energies, 
         CUDA_TRY(cudaMemcpyAsync(pl->d_targets, tg.data(), tg.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
     size_t N = (size_t)p.nx * p.ny * p.nz;
     CUDA_TRY(cudaMemsetAsync(dose, 0, N * sizeof(double), stream));
+    (void)cudaGetLastError();   // start from a clean launch-error state
     init_kernel<<<1, 32, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, energies, E0, 1);
     cfl_kernel<<<cell_blocks(p), NT, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, U);
     CUDA_TRY(cudaGetLastError());
@@ -1166,7 +1168,7 @@ static int march_impl(pdm1_plan *pl, double *U, double *dose, double *energies, 
     } else {
         use_graph = false;
     }
-    cudaGetLastError();
+    (void)cudaGetLastError();   // a refused capture falls back to direct launches
     int replays = 0, prev_step = 0, stage_launches = 0;
     double stage_ms = 0.0;
     const int stages_per_step = p.energy_scheme == PDM1_SCHEME_FORWARD_EULER ? 1 : 3;
@@ -1176,6 +1178,7 @@ static int march_impl(pdm1_plan *pl, double *U, double *dose, double *energies, 
             replays++;
         } else {
             for (int s = 0; s < kStepsPerGraph; ++s) per_step = launch_step_with_energies(pl, a, energies, stream, s);
+            CUDA_TRY(cudaGetLastError());
         }
         CUDA_TRY(cudaMemcpyAsync(pl->h_st, pl->d_st, sizeof(MarchState), cudaMemcpyDeviceToHost, stream));
         CUDA_TRY(cudaStreamSynchronize(stream));
@@ -1184,7 +1187,8 @@ static int march_impl(pdm1_plan *pl, double *U, double *dose, double *energies, 
         launches += ran * per_step + (kStepsPerGraph - ran) * per_step;
         for (int s = 0; s < ran && s < kStepsPerGraph; ++s) {
             float ms = 0.f;
-            if (cudaEventElapsedTime(&ms, pl->ev[2 * s], pl->ev[2 * s + 1]) == cudaSuccess) stage_ms += ms;
+            CUDA_TRY(cudaEventElapsedTime(&ms, pl->ev[2 * s], pl->ev[2 * s + 1]));
+            stage_ms += ms;
         }
         stage_launches += ran * stages_per_step;
         if (pl->h_st->done || pl->h_st->error) break;
@@ -1222,6 +1226,7 @@ int pdm1_march_steps(pdm1_plan *pl, double *U, double *dose, double *energies, i
 
 int pdm1_spatial_operator(pdm1_plan *pl, const double *U, double energy, const double *bc, double *rhs,
                           pdm1_stream_t stream_) {
+    (void)cudaGetLastError();
     if (!pl || !U || !rhs) return set_error(PDM1_ERR_ARGUMENT, "NULL argument");
     cudaStream_t stream = (cudaStream_t)stream_;
     StageArgs a = make_args(pl, const_cast<double *>(U), nullptr, nullptr, nullptr);
@@ -1236,6 +1241,7 @@ int pdm1_spatial_operator(pdm1_plan *pl, const double *U, double energy, const d
 }
 
 int pdm1_energy_step(pdm1_plan *pl, const double *U, double energy, double *dE_out, pdm1_stream_t stream_) {
+    (void)cudaGetLastError();
     if (!pl || !U || !dE_out) return set_error(PDM1_ERR_ARGUMENT, "NULL argument");
     cudaStream_t stream = (cudaStream_t)stream_;
     int rc = check_energy_range(pl, energy, energy);
@@ -1256,6 +1262,7 @@ int pdm1_energy_step(pdm1_plan *pl, const double *U, double energy, double *dE_o
 }
 
 int pdm1_advance(pdm1_plan *pl, double *U, double energy, double dE, double *edep, pdm1_stream_t stream_) {
+    (void)cudaGetLastError();
     if (!pl || !U || !edep || !(dE > 0.0)) return set_error(PDM1_ERR_ARGUMENT, "dE must be positive.");
     cudaStream_t stream = (cudaStream_t)stream_;
     int rc = check_energy_range(pl, energy, energy - dE);
@@ -1278,6 +1285,7 @@ int pdm1_advance(pdm1_plan *pl, double *U, double energy, double dE, double *ede
 }
 
 int pdm1_coefficients(pdm1_plan *pl, const double *E, int n, double *out) {
+    (void)cudaGetLastError();
     if (!pl || !E || !out || n <= 0) return set_error(PDM1_ERR_ARGUMENT, "NULL argument");
     double *dE_ = nullptr, *dout = nullptr;
     int *derr = nullptr;
@@ -1302,6 +1310,7 @@ int pdm1_coefficients(pdm1_plan *pl, const double *E, int n, double *out) {
 
 #define BATCH(kernel, ...)                                                 \
     if (n <= 0) return PDM1_OK;                                            \
+    (void)cudaGetLastError();                                              \
     kernel<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(__VA_ARGS__); \
     CUDA_TRY(cudaGetLastError());                                          \
     CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));                 \
