@@ -306,6 +306,8 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", default="slab80")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-steps", type=int, default=0,
+                    help="only run the first K energy steps of one spot (for ncu captures) and exit")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -313,6 +315,16 @@ def main():
     cfg, desc = workload(args.workload)
     if args.impl == "reference":
         run_reference(args, cfg, desc, rank, world)
+        return
+    if args.profile_steps > 0:
+        from proton_dose_m1_b200.numerics.energy import M1Plan
+        import torch
+        plan = M1Plan(cfg, *problem(cfg))
+        U, dose, E = plan.march_steps(args.profile_steps)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_steps": len(E) - 1, "energy": float(E[-1]),
+                          "stage_launches": plan.last_info.stage_launches,
+                          "stage_ms": plan.last_info.stage_ms}))
         return
     import torch
     import torch.distributed as dist
