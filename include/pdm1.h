@@ -117,6 +117,25 @@ int pdm1_march(pdm1_plan *plan, double *U, double *dose, double *energies, int m
 int pdm1_march_steps(pdm1_plan *plan, double *U, double *dose, double *energies, int max_steps,
                      int step_limit, pdm1_march_info *info, pdm1_stream_t stream);
 
+/* The march without any allocation by the library (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc: applications that hand
+ * the whole device to their own memory pool, plugins whose host forbids device
+ * allocation, and paths that must not take an allocation's implicit device
+ * synchronisation.  Instead of a plan's workspace, the configuration, tables and
+ * stage scratch live in one file-scope __device__ array of 16 MiB that every GPU
+ * loading libpdm1.so holds until the process exits; problems that do not fit
+ * (roughly more than 130000 cells) are rejected with PDM1_ERR_ARGUMENT.  The
+ * caller passes the problem (host), U (device, in/out), dose and energies
+ * (device, out) exactly as for pdm1_plan_create + pdm1_march, without snapshots.
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) and sets kernel attributes, so make it before any
+ * stream capture.  All calls on a device share the one array and it keeps the
+ * last call's contents (the march state is cleared at the start of every
+ * call): calls that overlap on the GPU race.  Launches directly on `stream`
+ * (no graph, no events) and synchronises it before returning. */
+int pdm1_march_noalloc(const pdm1_problem *problem, double *U, double *dose, double *energies,
+                       int max_steps, pdm1_march_info *info, pdm1_stream_t stream);
+
 /* Building blocks on the full grid, for operator-level parity checks. */
 
 /* numerics/spatial.py:104-252: rhs = -div F(U), boundary_state (4,nx,ny)

@@ -34,12 +34,15 @@ namespace {
 constexpr int kMaxMat = 16;
 constexpr int kStepsPerGraph = 32;
 
-thread_local std::string g_error;
+// fixed-size message buffer: reporting an error allocates nothing
+thread_local char g_error[512];
 
-int set_error(int code, const std::string &msg) {
-    g_error = msg;
+int set_error(int code, const char *msg) {
+    snprintf(g_error, sizeof g_error, "%s", msg);
     return code;
 }
+
+int set_error(int code, const std::string &msg) { return set_error(code, msg.c_str()); }
 
 #define CUDA_TRY(expr)                                                                    \
     do {                                                                                  \
@@ -987,7 +990,7 @@ int device_error_status(const MarchState &st) {
 
 extern "C" {
 
-const char *pdm1_last_error(void) { return g_error.c_str(); }
+const char *pdm1_last_error(void) { return g_error; }
 const char *pdm1_version(void) { return "pdm1 0.1 sm_100a"; }
 
 void pdm1_plan_destroy(pdm1_plan *pl) {
@@ -1327,3 +1330,255 @@ int pdm1_hll_batch(const double *l, const double *r, int axis, int ws, double *f
 int pdm1_exp_batch(const double *x, double *y, int n, pdm1_stream_t stream) { BATCH(exp_batch_kernel, x, y, n) }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free march.
+//
+// For callers that must not allocate GPU memory themselves: code running under
+// a host application that owns the whole device memory through its own pool,
+// plugins whose host forbids cudaMalloc/cudaFree (both synchronise the device
+// and can fail once a pool has reserved the memory), and latency-critical
+// paths where an allocation's implicit synchronisation is not allowed.  The
+// plan data and the stage scratch live in one file-scope __device__ array of
+// kNoAllocScratchBytes that every GPU loading this library holds until exit.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;   // 16 MiB per GPU
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+// Device address of g_noalloc_scratch per device: in host code the symbol is
+// only a host-side stand-in, so the address comes from cudaGetSymbolAddress.
+void *g_noalloc_base[kNoAllocMaxDevices];
+
+// PCHIP nodal slopes on the device, the same expressions as pchip_slopes()
+// (physics/stopping_power.py:94-138), one thread per node.
+__global__ void pchip_slopes_kernel(const double *E, const double *v, double *slope, int n) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    auto h = [&](int i) { return E[i + 1] - E[i]; };
+    auto d = [&](int i) { return (v[i + 1] - v[i]) / (E[i + 1] - E[i]); };
+    if (n == 2) {
+        slope[k] = d(0);
+        return;
+    }
+    auto endpoint = [](double h0, double h1, double d0, double d1) {
+        double sl = ((2.0 * h0 + h1) * d0 - h0 * d1) / (h0 + h1);
+        double s_sl = (double)((sl > 0.0) - (sl < 0.0)), s_d0 = (double)((d0 > 0.0) - (d0 < 0.0));
+        double s_d1 = (double)((d1 > 0.0) - (d1 < 0.0));
+        if (s_sl != s_d0) return 0.0;
+        if (s_d0 != s_d1 && fabs(sl) > 3.0 * fabs(d0)) return 3.0 * d0;
+        return sl;
+    };
+    if (k == 0) {
+        slope[0] = endpoint(h(0), h(1), d(0), d(1));
+    } else if (k == n - 1) {
+        slope[n - 1] = endpoint(h(n - 2), h(n - 3), d(n - 2), d(n - 3));
+    } else {
+        double dm = d(k - 1), dk = d(k);
+        double out = 0.0;
+        if (dm * dk > 0.0) {
+            double w1 = 2.0 * h(k) + h(k - 1);
+            double w2 = h(k) + 2.0 * h(k - 1);
+            out = (w1 + w2) / (w1 / dm + w2 / dk);
+        }
+        slope[k] = out;
+    }
+}
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Table metadata without touching the heap: node count and the log-spacing guess.
+TableView table_meta(const pdm1_table &t) {
+    TableView v{};
+    v.n = t.n_nodes;
+    double l0 = std::log(t.energy[0]), l1 = std::log(t.energy[t.n_nodes - 1]);
+    double step = (l1 - l0) / (t.n_nodes - 1);
+    bool uniform = t.energy[0] > 0.0 && step > 0.0;
+    for (int i = 0; uniform && i < t.n_nodes; i += 97)
+        if (std::fabs(std::log(t.energy[i]) - (l0 + step * i)) > 1e-6 * step) uniform = false;
+    v.log_e0 = l0;
+    v.inv_log_step = uniform ? 1.0 / step : 0.0;
+    return v;
+}
+
+void launch_step_plain(const pdm1_problem &p, ConfigDev *d_cf, Coeffs *d_co, MarchState *d_st,
+                       const StageArgs &a, double *energies, cudaStream_t stream) {
+    int tiles = n_tiles(p);
+    prologue_kernel<<<1, 256, 0, stream>>>(d_cf, d_co, d_st, energies);
+    if (p.energy_scheme == PDM1_SCHEME_FORWARD_EULER) {
+        stage_kernel<MODE_EULER><<<tiles, NT, kStageSmem, stream>>>(a);
+        euler_finish_kernel<<<cell_blocks(p), NT, 0, stream>>>(a);
+        return;
+    }
+    stage_kernel<MODE_A><<<tiles, NT, kStageSmem, stream>>>(a);
+    stage_kernel<MODE_B><<<tiles, NT, kStageSmem, stream>>>(a);
+    stage_kernel<MODE_C><<<tiles, NT, kStageSmem, stream>>>(a);
+}
+
+}  // namespace
+
+extern "C" int pdm1_march_noalloc(const pdm1_problem *problem, double *U, double *dose,
+                                  double *energies, int max_steps, pdm1_march_info *info,
+                                  pdm1_stream_t stream_) {
+    if (!U || !dose || !energies || max_steps < 1)
+        return set_error(PDM1_ERR_ARGUMENT, "pdm1_march_noalloc: NULL buffer or max_steps < 1");
+    int rc = validate_problem(problem);
+    if (rc) return rc;
+    const pdm1_problem &p = *problem;
+    const size_t N = (size_t)p.nx * p.ny * p.nz;
+
+    // layout of the scratch array
+    size_t off = 0;
+    const size_t o_cf = off; off = align256(off + sizeof(ConfigDev));
+    const size_t o_co = off; off = align256(off + sizeof(Coeffs));
+    const size_t o_st = off; off = align256(off + sizeof(MarchState));
+    size_t o_tab[kMaxMat][3];
+    for (int m = 0; m < p.n_materials; ++m) {
+        const pdm1_table *tabs[3] = {&p.materials[m].stopping_power, &p.materials[m].transport,
+                                     &p.materials[m].nuclear};
+        for (int q = 0; q < 3; ++q) {
+            o_tab[m][q] = off;
+            off = align256(off + 3 * (size_t)tabs[q]->n_nodes * sizeof(double));
+        }
+    }
+    const size_t o_ids = off; off = align256(off + N * sizeof(int32_t));
+    const size_t o_sp = off; off = align256(off + (size_t)p.nx * p.ny * sizeof(double));
+    const size_t o_U1 = off; off = align256(off + 4 * N * sizeof(double));
+    const size_t o_U2 = off; off = align256(off + 4 * N * sizeof(double));
+    const size_t o_V = off; off = align256(off + 4 * N * sizeof(double));
+    const size_t o_q = off; off = align256(off + N * sizeof(double));
+    if (off > kNoAllocScratchBytes) {
+        char msg[256];
+        snprintf(msg, sizeof msg,
+                 "pdm1_march_noalloc: the problem needs %zu bytes of scratch (%zu cells, %d materials); "
+                 "the allocation-free march holds at most %zu bytes (about 130000 cells)",
+                 off, N, p.n_materials, kNoAllocScratchBytes);
+        return set_error(PDM1_ERR_ARGUMENT, msg);
+    }
+    double E0 = p.beam_energy + p.energy_window_sigma * p.energy_spread;
+    {
+        // energy range of the march against the tables (check_energy_range without a plan)
+        const bool used[3] = {true, p.scattering == PDM1_SCATTERING_WENTZEL, p.nuclear != 0};
+        for (int m = 0; m < p.n_materials; ++m) {
+            const pdm1_table *tabs[3] = {&p.materials[m].stopping_power, &p.materials[m].transport,
+                                         &p.materials[m].nuclear};
+            for (int q = 0; q < 3; ++q) {
+                if (!used[q]) continue;
+                double lo = tabs[q]->energy[0], hi = tabs[q]->energy[tabs[q]->n_nodes - 1];
+                if ((E0 > hi && !is_close(E0, hi)) || (p.energy_min < lo && !is_close(p.energy_min, lo)))
+                    return set_error(PDM1_ERR_RANGE, "Energy outside coefficient table range.");
+            }
+        }
+    }
+
+    // once per device, with that device current: the scratch array's device address
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return set_error(PDM1_ERR_ARGUMENT, "device ordinal too large");
+    if (!g_noalloc_base[dev]) {
+        void *ptr = nullptr;
+        CUDA_TRY(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+        CUDA_TRY(cudaFuncSetAttribute(stage_kernel<MODE_A>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageSmem));
+        CUDA_TRY(cudaFuncSetAttribute(stage_kernel<MODE_B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageSmem));
+        CUDA_TRY(cudaFuncSetAttribute(stage_kernel<MODE_C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageSmem));
+        CUDA_TRY(cudaFuncSetAttribute(stage_kernel<MODE_EULER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageSmem));
+        g_noalloc_base[dev] = ptr;
+    }
+    unsigned char *base = static_cast<unsigned char *>(g_noalloc_base[dev]);
+    cudaStream_t stream = (cudaStream_t)stream_;
+    ConfigDev *d_cf = reinterpret_cast<ConfigDev *>(base + o_cf);
+    Coeffs *d_co = reinterpret_cast<Coeffs *>(base + o_co);
+    MarchState *d_st = reinterpret_cast<MarchState *>(base + o_st);
+
+    // the configuration, tables, ids and inflow profile go into the scratch array
+    ConfigDev cf{};
+    cf.nx = p.nx; cf.ny = p.ny; cf.nz = p.nz;
+    cf.dx = p.dx; cf.dy = p.dy; cf.dz = p.dz;
+    cf.nm = p.n_materials;
+    cf.scattering = p.scattering;
+    cf.nuclear = p.nuclear ? 1 : 0;
+    cf.interp = p.interpolation;
+    cf.scheme = p.energy_scheme;
+    cf.unit_speeds = p.wave_speeds == PDM1_SPEEDS_UNIT;
+    bool sources = p.scattering != PDM1_SCATTERING_OFF || p.nuclear;
+    cf.use_if = (p.energy_scheme == PDM1_SCHEME_IF_SSPRK3 && sources) ? 1 : 0;
+    cf.strang = (p.energy_scheme != PDM1_SCHEME_IF_SSPRK3 && sources) ? 1 : 0;
+    cf.cfl = p.cfl;
+    cf.max_dE = p.max_energy_step;
+    cf.Emin = p.energy_min;
+    cf.E_beam = p.beam_energy;
+    cf.sigma_E = p.energy_spread;
+    cf.rf = dd_exp(-(p.angular_spread * p.angular_spread));
+    cf.max_steps = max_steps;
+    cf.step_limit = -1;
+    cf.n_targets = 0;
+    cf.targets = nullptr;
+    cf.ids = reinterpret_cast<const int32_t *>(base + o_ids);
+    cf.spatial = reinterpret_cast<const double *>(base + o_sp);
+    for (int m = 0; m < p.n_materials; ++m) {
+        const pdm1_material &mt = p.materials[m];
+        const pdm1_table *tabs[3] = {&mt.stopping_power, &mt.transport, &mt.nuclear};
+        TableView *views[3] = {&cf.mats[m].sp, &cf.mats[m].tr, &cf.mats[m].nuc};
+        for (int q = 0; q < 3; ++q) {
+            const pdm1_table &t = *tabs[q];
+            double *dE_ = reinterpret_cast<double *>(base + o_tab[m][q]);
+            *views[q] = table_meta(t);
+            views[q]->E = dE_;
+            views[q]->v = dE_ + t.n_nodes;
+            views[q]->slope = dE_ + 2 * t.n_nodes;
+            CUDA_TRY(cudaMemcpyAsync(dE_, t.energy, t.n_nodes * sizeof(double), cudaMemcpyHostToDevice, stream));
+            CUDA_TRY(cudaMemcpyAsync(dE_ + t.n_nodes, t.value, t.n_nodes * sizeof(double), cudaMemcpyHostToDevice, stream));
+            pchip_slopes_kernel<<<(t.n_nodes + 255) / 256, 256, 0, stream>>>(dE_, dE_ + t.n_nodes, dE_ + 2 * t.n_nodes, t.n_nodes);
+        }
+        cf.mats[m].density = mt.density;
+        cf.mats[m].X0 = mt.radiation_length;
+    }
+    CUDA_TRY(cudaMemcpyAsync(base + o_ids, p.ids, N * sizeof(int32_t), cudaMemcpyHostToDevice, stream));
+    CUDA_TRY(cudaMemcpyAsync(base + o_sp, p.inflow_spatial, (size_t)p.nx * p.ny * sizeof(double), cudaMemcpyHostToDevice, stream));
+    CUDA_TRY(cudaMemcpyAsync(d_cf, &cf, sizeof cf, cudaMemcpyHostToDevice, stream));
+    // the array keeps the previous call's contents: clear what must start at zero
+    CUDA_TRY(cudaMemsetAsync(d_co, 0, sizeof(Coeffs), stream));
+    CUDA_TRY(cudaMemsetAsync(d_st, 0, sizeof(MarchState), stream));
+    CUDA_TRY(cudaMemsetAsync(dose, 0, N * sizeof(double), stream));
+
+    StageArgs a{};
+    a.cf = d_cf;
+    a.co = d_co;
+    a.st = d_st;
+    a.U = U;
+    a.U1 = reinterpret_cast<double *>(base + o_U1);
+    a.U2 = reinterpret_cast<double *>(base + o_U2);
+    a.V = reinterpret_cast<double *>(base + o_V);
+    a.qpart = reinterpret_cast<double *>(base + o_q);
+    a.dose = dose;
+
+    (void)cudaGetLastError();
+    init_kernel<<<1, 32, 0, stream>>>(d_cf, d_co, d_st, energies, E0, 1);
+    cfl_kernel<<<cell_blocks(p), NT, 0, stream>>>(d_cf, d_co, d_st, U);
+    CUDA_TRY(cudaGetLastError());
+    int launches = 2 + 3 * p.n_materials, chunks = 0;
+    const int per_step = p.energy_scheme == PDM1_SCHEME_FORWARD_EULER ? 3 : 4;
+    MarchState hs{};
+    for (;;) {
+        for (int s = 0; s < kStepsPerGraph; ++s) launch_step_plain(p, d_cf, d_co, d_st, a, energies, stream);
+        CUDA_TRY(cudaGetLastError());
+        launches += kStepsPerGraph * per_step;
+        ++chunks;
+        CUDA_TRY(cudaMemcpyAsync(&hs, d_st, sizeof hs, cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        if (hs.done || hs.error) break;
+    }
+    if (info) {
+        info->n_steps = hs.step;
+        info->n_snapshots = 0;
+        info->final_state_valid = 1;
+        info->graph_replays = 0;
+        info->kernel_launches = launches;
+        info->stage_launches = 0;
+        info->stage_ms = 0.0;
+    }
+    (void)chunks;
+    return device_error_status(hs);
+}
