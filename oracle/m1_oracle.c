@@ -1417,7 +1417,7 @@ static int march_impl(const orc_problem *p, double *U, double *dose, double *ene
     int moving = d->moving_active_domain;
     box_t box = {0, d->nx, 0, d->ny, 0, d->nz};
     double *Ua = U;
-    double tol = exp(-0.5 * d->active_truncation_sigma * d->active_truncation_sigma);
+    double tol = exp(-0.5 * (d->active_truncation_sigma * d->active_truncation_sigma));   /* energy.py:1305-1307 */
     int guard = d->active_guard_cells;
     if (moving) {
         if ((rc = initial_box(p, guard, &box))) goto out;

@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -59,6 +60,15 @@ struct MatDev {
     double density, X0;
 };
 
+// A rectangular domain of the full grid: the whole grid, or the moving active box
+// (numerics/moving_active_domain.py), with its tile decomposition.
+struct DomainDev {
+    int i0, j0, k0;          // origin in the full grid
+    int nx, ny, nz;          // extent
+    int tiles_y, tiles_z, ntiles;
+    int inflow;              // the domain's z-min face is the beam entrance (k0 == 0)
+};
+
 struct ConfigDev {
     int nx, ny, nz;
     double dx, dy, dz;
@@ -73,6 +83,14 @@ struct ConfigDev {
     const int32_t *ids;
     const double *spatial;
     const double *targets;      // descending
+    // moving active box
+    int moving, vacuum_aware, guard;
+    double tol;                 // exp(-sigma_trunc^2 / 2)
+    DomainDev init_box;         // moving_active_domain.py:35-60
+    double *bufA, *bufB;        // compact-state ping-pong
+    unsigned long long *slab;   // max phi per x | y | z slab of the current box (double bits)
+    unsigned char *active;      // vacuum-aware activity mask on the current box
+    int grid_ctas;              // persistent grid of the stage kernels
     MatDev mats[kMaxMat];
 };
 
@@ -88,6 +106,8 @@ struct Coeffs {
     double ed[4];                           // spectrum at those energies
     double ed_next;                         // spectrum at E_next (CFL inflow)
     double hn[kMaxMat], hs[kMaxMat];        // Strang half-step factors
+    double S_cfl[kMaxMat];                  // moving box: S at the step's start energy
+    double ed_cfl;                          // moving box: spectrum at that energy
 };
 
 struct MarchState {
@@ -95,7 +115,16 @@ struct MarchState {
     unsigned long long inv_bits;   // CFL max (non-negative double bits)
     double forced_dE;              // > 0: one step with this dE (pdm1_advance)
     int step, done, ti, taken, error;
+    DomainDev dom;                 // the domain the stage kernels work on
+    DomainDev prev;                // moving box before this step's rebox
+    double *Ua;                    // state on `dom`
+    double *Uprev;                 // state on `prev`
+    int reboxed;
+    unsigned long long newmax_bits;   // max phi over the new box (vacuum-aware CFL)
+    double pin_max;                // max inflow phi over the new box
 };
+
+__host__ __device__ inline DomainDev make_domain(int i0, int j0, int k0, int nx, int ny, int nz, int inflow);
 
 enum { ERR_DEV_RANGE = 1, ERR_DEV_MAXSTEPS = 2, ERR_DEV_NONFINITE = 4 };
 
@@ -150,7 +179,7 @@ __device__ __forceinline__ void source_factor(double ts, double tn, bool inverse
 // init: state at the start energy, S and spectrum for the first CFL
 // ---------------------------------------------------------------------------
 __global__ void init_kernel(const ConfigDev *cfp, Coeffs *co, MarchState *st, double *energies,
-                            double E0, int reset) {
+                            double E0, double *U, int full_domain) {
     const ConfigDev &cf = *cfp;
     int t = threadIdx.x;
     if (t < cf.nm) {
@@ -161,17 +190,23 @@ __global__ void init_kernel(const ConfigDev *cfp, Coeffs *co, MarchState *st, do
     if (t == 0) {
         co->ed_next = energy_density(cf, E0);
         co->E_next = E0;
-        if (reset) {
-            st->E = E0;
-            st->inv_bits = 0ull;
-            st->forced_dE = 0.0;
-            st->step = 0;
-            st->done = 0;
-            st->ti = 0;
-            st->taken = 0;
-            st->error = 0;
-            if (energies) energies[0] = E0;
-        }
+        st->E = E0;
+        st->inv_bits = 0ull;
+        st->forced_dE = 0.0;
+        st->step = 0;
+        st->done = 0;
+        st->ti = 0;
+        st->taken = 0;
+        st->error = 0;
+        st->reboxed = 0;
+        st->newmax_bits = 0ull;
+        st->pin_max = 0.0;
+        const bool moving = cf.moving && !full_domain;
+        st->dom = moving ? cf.init_box : make_domain(0, 0, 0, cf.nx, cf.ny, cf.nz, 1);
+        st->prev = st->dom;
+        st->Ua = moving ? cf.bufA : U;
+        st->Uprev = st->Ua;
+        if (energies) energies[0] = E0;
     }
 }
 
@@ -334,20 +369,30 @@ constexpr int SY = TX * 6 * TZ;          // y halo
 constexpr int SZ = TX * TY * 6;          // z halo
 constexpr size_t kStageSmem = sizeof(double) * 4 * (SX + SY + SZ + NF);
 
+__host__ __device__ inline DomainDev make_domain(int i0, int j0, int k0, int nx, int ny, int nz, int inflow) {
+    DomainDev d;
+    d.i0 = i0; d.j0 = j0; d.k0 = k0;
+    d.nx = nx; d.ny = ny; d.nz = nz;
+    d.tiles_y = (ny + TY - 1) / TY;
+    d.tiles_z = (nz + TZ - 1) / TZ;
+    d.ntiles = ((nx + TX - 1) / TX) * d.tiles_y * d.tiles_z;
+    d.inflow = inflow;
+    return d;
+}
+
 enum StageMode { MODE_A = 0, MODE_B = 1, MODE_C = 2, MODE_EULER = 3, MODE_RHS = 4 };
 
 struct StageArgs {
     const ConfigDev *cf;
     const Coeffs *co;
     MarchState *st;
-    double *U;          // accepted state (in/out)
-    double *U1;         // stage states
+    double *U1;         // stage states (on the current domain)
     double *U2;
     double *V;          // marched variable of stage 1 / 2
     double *qpart;      // (q0 + q1)/6 quadrature part
-    double *dose;       // accumulated dose (MODE_C / MODE_EULER), or NULL
+    double *dose;       // accumulated dose (full grid), or NULL
     double *edep;       // when non-NULL: energy deposition written instead of dose
-    double *snap;       // snapshot buffer base (slot * 4N)
+    double *snap;       // snapshot buffer base (slot * 4N, full grid)
     double *rhs_out;    // MODE_RHS output
     const double *bc_plane;   // MODE_RHS: explicit z-min boundary state (4,nx,ny)
     double rhs_energy_density;
@@ -365,19 +410,25 @@ __device__ __forceinline__ double sval(const Smem &s, int c, int i, int j, int k
     return s.X[((c * (TX + 6) + (i + 3)) * TY + j) * TZ + k];
 }
 
+__device__ __forceinline__ size_t global_cell(const ConfigDev &cf, const DomainDev &d, int li, int lj, int lk) {
+    return ((size_t)(d.i0 + li) * cf.ny + (d.j0 + lj)) * cf.nz + (d.k0 + lk);
+}
+
+// Stencil source value at a domain cell; indices outside the domain are
+// clamped (zero-gradient ghosts, numerics/boundary.py:327-397).
 template <int MODE>
-__device__ __forceinline__ void load_cell(const StageArgs &a, const ConfigDev &cf, const Coeffs &co,
-                                          const double *src, size_t N, int gi, int gj, int gk,
-                                          double out[4]) {
-    int nx = cf.nx, ny = cf.ny, nz = cf.nz;
-    gi = gi < 0 ? 0 : (gi >= nx ? nx - 1 : gi);
-    gj = gj < 0 ? 0 : (gj >= ny ? ny - 1 : gj);
-    gk = gk >= nz ? nz - 1 : gk;
-    size_t o = ((size_t)gi * ny + gj) * nz + gk;
+__device__ __forceinline__ void load_cell(const ConfigDev &cf, const Coeffs &co, const DomainDev &d,
+                                          const double *src, int li, int lj, int lk, double out[4]) {
+    const int nx = d.nx, ny = d.ny, nz = d.nz;
+    const size_t N = (size_t)nx * ny * nz;
+    li = li < 0 ? 0 : (li >= nx ? nx - 1 : li);
+    lj = lj < 0 ? 0 : (lj >= ny ? ny - 1 : lj);
+    lk = lk >= nz ? nz - 1 : lk;
+    size_t o = ((size_t)li * ny + lj) * nz + lk;
 #pragma unroll
     for (int c = 0; c < 4; ++c) out[c] = src[c * N + o];
     if ((MODE == MODE_A || MODE == MODE_EULER) && cf.strang) {
-        int m = cf.ids[o];
+        int m = cf.ids[global_cell(cf, d, li, lj, lk)];
         double hn = co.hn[m], hs = co.hs[m];
         if (cf.nuclear)
 #pragma unroll
@@ -388,13 +439,15 @@ __device__ __forceinline__ void load_cell(const StageArgs &a, const ConfigDev &c
     }
 }
 
-// z-min boundary value of component c at column (gi, gj) for this stage
+// z-min boundary value of component c at domain column (li, lj) for this stage.
+// A moving box away from the entrance has zero inflow (moving_active_domain.py:85-95).
 template <int MODE>
-__device__ __forceinline__ double boundary_value(const StageArgs &a, const ConfigDev &cf,
-                                                 const Coeffs &co, int c, int gi, int gj) {
+__device__ __forceinline__ double boundary_value(const StageArgs &a, const ConfigDev &cf, const Coeffs &co,
+                                                 const DomainDev &d, int c, int li, int lj) {
     if (MODE == MODE_RHS && a.bc_plane)
-        return a.bc_plane[((size_t)c * cf.nx + gi) * cf.ny + gj];
-    if (c == 1 || c == 2) return 0.0;
+        return a.bc_plane[((size_t)c * d.nx + li) * d.ny + lj];
+    if (!d.inflow || c == 1 || c == 2) return 0.0;
+    const int gi = d.i0 + li, gj = d.j0 + lj;
     double sp = cf.spatial[(size_t)gi * cf.ny + gj];
     if (MODE == MODE_A || MODE == MODE_EULER || MODE == MODE_RHS) {
         double ed = MODE == MODE_RHS ? a.rhs_energy_density : co.ed[0];
@@ -422,8 +475,11 @@ __device__ __forceinline__ double boundary_value(const StageArgs &a, const Confi
     return vs2 / co.S2[m];
 }
 
-__device__ __forceinline__ void cfl_contrib(const ConfigDev &cf, const Coeffs &co, const double u[4],
-                                            int m, int gi, int gj, int gk, double &inv) {
+// One cell's CFL term (numerics/energy.py:539-660): sum over axes of a/(S d).
+// `entrance`: the cell is on the domain's z-min layer, where the inflow state
+// (zero for a box away from the entrance) joins the z speeds.
+__device__ __forceinline__ double cfl_term(const ConfigDev &cf, const double u[4], double s, bool entrance,
+                                           double phi_in, const bool use[3]) {
     double a0, a1, a2;
     if (cf.unit_speeds) {
         a0 = a1 = a2 = 1.0;
@@ -431,15 +487,16 @@ __device__ __forceinline__ void cfl_contrib(const ConfigDev &cf, const Coeffs &c
         a0 = max_abs_speed(u[0], u[1], u[2], u[3], 0);
         a1 = max_abs_speed(u[0], u[1], u[2], u[3], 1);
         a2 = max_abs_speed(u[0], u[1], u[2], u[3], 2);
-        if (gk == 0) {
-            double phi = cf.spatial[(size_t)gi * cf.ny + gj] * co.ed_next;
-            double jz = cf.rf * phi;
-            double ain = max_abs_speed(phi, 0.0, 0.0, jz, 2);
+        if (entrance) {
+            double jz = cf.rf * phi_in;
+            double ain = max_abs_speed(phi_in, 0.0, 0.0, jz, 2);
             if (ain > a2) a2 = ain;
         }
     }
-    double s = co.S1[m];
-    inv = a0 / (s * cf.dx) + a1 / (s * cf.dy) + a2 / (s * cf.dz);
+    if (!use[0]) a0 = 0.0;
+    if (!use[1]) a1 = 0.0;
+    if (!use[2]) a2 = 0.0;
+    return a0 / (s * cf.dx) + a1 / (s * cf.dy) + a2 / (s * cf.dz);
 }
 
 __device__ __forceinline__ void block_max_atomic(double v, unsigned long long *target) {
@@ -447,12 +504,42 @@ __device__ __forceinline__ void block_max_atomic(double v, unsigned long long *t
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
     __shared__ double wmax[NT / 32];
     int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
     if (l == 0) wmax[w] = v;
     __syncthreads();
     if (w == 0) {
         v = l < NT / 32 ? wmax[l] : 0.0;
         for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
         if (l == 0 && v > 0.0) atomicMax(target, (unsigned long long)__double_as_longlong(v));
+    }
+}
+
+__device__ __forceinline__ void atomic_max_double(unsigned long long *target, double v) {
+    if (v > 0.0) atomicMax(target, (unsigned long long)__double_as_longlong(v));
+}
+
+// Per-slab maxima of phi over one tile (moving box): cell values in `buf`
+// (TX*TY*TZ doubles, -1 for cells outside the box).
+__device__ __forceinline__ void tile_slab_max(const ConfigDev &cf, const DomainDev &d, const double *buf,
+                                              int i0, int j0, int k0) {
+    int t = threadIdx.x;
+    unsigned long long *sx = cf.slab, *sy = cf.slab + cf.nx, *sz = cf.slab + cf.nx + cf.ny;
+    if (t < TX) {
+        double m = 0.0;
+        for (int e = 0; e < TY * TZ; ++e) m = fmax(m, buf[t * TY * TZ + e]);
+        if (i0 + t < d.nx) atomic_max_double(&sx[i0 + t], m);
+    } else if (t < TX + TY) {
+        int j = t - TX;
+        double m = 0.0;
+        for (int i = 0; i < TX; ++i)
+            for (int k = 0; k < TZ; ++k) m = fmax(m, buf[(i * TY + j) * TZ + k]);
+        if (j0 + j < d.ny) atomic_max_double(&sy[j0 + j], m);
+    } else if (t < TX + TY + TZ) {
+        int k = t - TX - TY;
+        double m = 0.0;
+        for (int i = 0; i < TX; ++i)
+            for (int j = 0; j < TY; ++j) m = fmax(m, buf[(i * TY + j) * TZ + k]);
+        if (k0 + k < d.nz) atomic_max_double(&sz[k0 + k], m);
     }
 }
 
@@ -467,252 +554,511 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(StageArgs a) {
     s.Y = s.X + 4 * SX;
     s.Z = s.Y + 4 * SY;
     s.F = s.Z + 4 * SZ;
-    const int nx = cf.nx, ny = cf.ny, nz = cf.nz;
+    const DomainDev d = a.st->dom;
+    double *const Ua = a.st->Ua;
+    const int nx = d.nx, ny = d.ny, nz = d.nz;
     const size_t N = (size_t)nx * ny * nz;
-    const int tiles_y = (ny + TY - 1) / TY, tiles_z = (nz + TZ - 1) / TZ;
     const int tid = threadIdx.x;
-    const double *src = (MODE == MODE_B) ? a.U1 : (MODE == MODE_C ? a.U2 : a.U);
+    const double *src = (MODE == MODE_B) ? a.U1 : (MODE == MODE_C ? a.U2 : Ua);
+    const bool unit = cf.unit_speeds != 0;
+    const bool all_axes[3] = {true, true, true};
     double cta_inv = 0.0;
 
-    int tile = blockIdx.x;
-    const int tz = tile % tiles_z, ty = (tile / tiles_z) % tiles_y, tx = tile / (tiles_z * tiles_y);
-    const int i0 = tx * TX, j0 = ty * TY, k0 = tz * TZ;
+    for (int tile = blockIdx.x; tile < d.ntiles; tile += gridDim.x) {
+        const int tz = tile % d.tiles_z, ty = (tile / d.tiles_z) % d.tiles_y, tx = tile / (d.tiles_z * d.tiles_y);
+        const int i0 = tx * TX, j0 = ty * TY, k0 = tz * TZ;
 
-    // ---- 1. stage the stencil source + halo ----
-    for (int e = tid; e < SX; e += NT) {
-        int k = e % TZ, j = (e / TZ) % TY, ii = e / (TZ * TY);
-        double u[4];
-        load_cell<MODE>(a, cf, co, src, N, i0 + ii - 3, j0 + j, k0 + k, u);
+        // ---- 1. stage the stencil source + halo ----
+        for (int e = tid; e < SX; e += NT) {
+            int k = e % TZ, j = (e / TZ) % TY, ii = e / (TZ * TY);
+            double u[4];
+            load_cell<MODE>(cf, co, d, src, i0 + ii - 3, j0 + j, k0 + k, u);
 #pragma unroll
-        for (int c = 0; c < 4; ++c) s.X[((c * (TX + 6) + ii) * TY + j) * TZ + k] = u[c];
-    }
-    for (int e = tid; e < SY; e += NT) {
-        int k = e % TZ, jj = (e / TZ) % 6, i = e / (TZ * 6);
-        int gj = jj < 3 ? j0 + jj - 3 : j0 + TY + jj - 3;
-        double u[4];
-        load_cell<MODE>(a, cf, co, src, N, i0 + i, gj, k0 + k, u);
+            for (int c = 0; c < 4; ++c) s.X[((c * (TX + 6) + ii) * TY + j) * TZ + k] = u[c];
+        }
+        for (int e = tid; e < SY; e += NT) {
+            int k = e % TZ, jj = (e / TZ) % 6, i = e / (TZ * 6);
+            int gj = jj < 3 ? j0 + jj - 3 : j0 + TY + jj - 3;
+            double u[4];
+            load_cell<MODE>(cf, co, d, src, i0 + i, gj, k0 + k, u);
 #pragma unroll
-        for (int c = 0; c < 4; ++c) s.Y[((c * TX + i) * 6 + jj) * TZ + k] = u[c];
-    }
-    for (int e = tid; e < SZ; e += NT) {
-        int kk = e % 6, j = (e / 6) % TY, i = e / (6 * TY);
-        int gk = kk < 3 ? k0 + kk - 3 : k0 + TZ + kk - 3;
-        if (gk < 0) continue;   // z-min ghost, filled below
-        double u[4];
-        load_cell<MODE>(a, cf, co, src, N, i0 + i, j0 + j, gk, u);
+            for (int c = 0; c < 4; ++c) s.Y[((c * TX + i) * 6 + jj) * TZ + k] = u[c];
+        }
+        for (int e = tid; e < SZ; e += NT) {
+            int kk = e % 6, j = (e / 6) % TY, i = e / (6 * TY);
+            int gk = kk < 3 ? k0 + kk - 3 : k0 + TZ + kk - 3;
+            if (gk < 0) continue;   // z-min ghost, filled below
+            double u[4];
+            load_cell<MODE>(cf, co, d, src, i0 + i, j0 + j, gk, u);
 #pragma unroll
-        for (int c = 0; c < 4; ++c) s.Z[((c * TX + i) * TY + j) * 6 + kk] = u[c];
-    }
-    __syncthreads();
-    // ---- 2. z-min ghost cells: quartic extrapolation through the inflow ----
-    if (k0 == 0) {
-        for (int e = tid; e < 4 * TX * TY; e += NT) {
-            int j = e % TY, i = (e / TY) % TX, c = e / (TX * TY);
-            int gi = i0 + i, gj = j0 + j;
-            if (gi >= nx || gj >= ny) continue;
-            double ui = boundary_value<MODE>(a, cf, co, c, gi, gj);
-            const double *col = &s.X[((c * (TX + 6) + (i + 3)) * TY + j) * TZ];
-            double u0 = col[0], u1 = col[1], u2 = col[2], u3 = col[3];
-            double *z = &s.Z[((c * TX + i) * TY + j) * 6];
-            z[2] = 5.0 * ui - (77.0 / 12.0) * u0 + (43.0 / 12.0) * u1 - (17.0 / 12.0) * u2 + 0.25 * u3;
-            z[1] = 25.0 * ui - (505.0 / 12.0) * u0 + (335.0 / 12.0) * u1 - (145.0 / 12.0) * u2 + (9.0 / 4.0) * u3;
-            z[0] = 75.0 * ui - (545.0 / 4.0) * u0 + (395.0 / 4.0) * u1 - (181.0 / 4.0) * u2 + (35.0 / 4.0) * u3;
+            for (int c = 0; c < 4; ++c) s.Z[((c * TX + i) * TY + j) * 6 + kk] = u[c];
         }
         __syncthreads();
-    }
-    // ---- 3. every face of the tile: WENO-Z, projection, HLL ----
-    const bool unit = cf.unit_speeds != 0;
-    for (int f = tid; f < NF; f += NT) {
-        int axis, i, j, k;
-        if (f < NFX) {
-            axis = 0; k = f % TZ; j = (f / TZ) % TY; i = f / (TZ * TY);          // face left of cell i
-        } else if (f < NFX + NFY) {
-            int u = f - NFX;
-            axis = 1; k = u % TZ; j = (u / TZ) % (TY + 1); i = u / (TZ * (TY + 1));
-        } else {
-            int u = f - NFX - NFY;
-            axis = 2; k = u % (TZ + 1); j = (u / (TZ + 1)) % TY; i = u / ((TZ + 1) * TY);
-        }
-        double L[4], R[4];
-        const int di = axis == 0, dj = axis == 1, dk = axis == 2;
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            double w[6];
-#pragma unroll
-            for (int q = 0; q < 6; ++q) {
-                int o = q - 3;
-                w[q] = sval(s, c, i + o * di, j + o * dj, k + o * dk);
+        // ---- 2. z-min ghost cells: quartic extrapolation through the inflow ----
+        if (k0 == 0) {
+            for (int e = tid; e < 4 * TX * TY; e += NT) {
+                int j = e % TY, i = (e / TY) % TX, c = e / (TX * TY);
+                int li = i0 + i, lj = j0 + j;
+                if (li >= nx || lj >= ny) continue;
+                double ui = boundary_value<MODE>(a, cf, co, d, c, li, lj);
+                const double *col = &s.X[((c * (TX + 6) + (i + 3)) * TY + j) * TZ];
+                double u0 = col[0], u1 = col[1], u2 = col[2], u3 = col[3];
+                double *z = &s.Z[((c * TX + i) * TY + j) * 6];
+                z[2] = 5.0 * ui - (77.0 / 12.0) * u0 + (43.0 / 12.0) * u1 - (17.0 / 12.0) * u2 + 0.25 * u3;
+                z[1] = 25.0 * ui - (505.0 / 12.0) * u0 + (335.0 / 12.0) * u1 - (145.0 / 12.0) * u2 + (9.0 / 4.0) * u3;
+                z[0] = 75.0 * ui - (545.0 / 4.0) * u0 + (395.0 / 4.0) * u1 - (181.0 / 4.0) * u2 + (35.0 / 4.0) * u3;
             }
-            L[c] = weno_left(w[0], w[1], w[2], w[3], w[4]);
-            R[c] = weno_left(w[5], w[4], w[3], w[2], w[1]);
+            __syncthreads();
         }
-        project(L[0], L[1], L[2], L[3]);
-        project(R[0], R[1], R[2], R[3]);
-        double F[4];
-        hll_flux(L, R, axis, unit, F);
-#pragma unroll
-        for (int c = 0; c < 4; ++c) s.F[c * NF + f] = F[c];
-    }
-    __syncthreads();
-    // ---- 4. divergence and the stage update, one cell per thread ----
-    const int k = tid % TZ, j = (tid / TZ) % TY, i = tid / (TZ * TY);
-    const int gi = i0 + i, gj = j0 + j, gk = k0 + k;
-    const bool valid = gi < nx && gj < ny && gk < nz;
-    if (valid) {
-        const int fx0 = (i * TY + j) * TZ + k, fx1 = ((i + 1) * TY + j) * TZ + k;
-        const int fy0 = NFX + (i * (TY + 1) + j) * TZ + k, fy1 = NFX + (i * (TY + 1) + j + 1) * TZ + k;
-        const int fz0 = NFX + NFY + (i * TY + j) * (TZ + 1) + k, fz1 = fz0 + 1;
-        double L[4];
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const double *F = s.F + c * NF;
-            double gx = (F[fx1] - F[fx0]) / cf.dx;
-            double gy = (F[fy1] - F[fy0]) / cf.dy;
-            double gz = (F[fz1] - F[fz0]) / cf.dz;
-            L[c] = -(gx + gy + gz);
-        }
-        const size_t o = ((size_t)gi * ny + gj) * nz + gk;
-        if (MODE == MODE_RHS) {
-#pragma unroll
-            for (int c = 0; c < 4; ++c) a.rhs_out[c * N + o] = L[c];
-        } else {
-            const int m = cf.ids[o];
-            const double dE = co.dE;
-            // the accepted state at this cell (with the Strang half step applied)
-            double un[4];
-            if (MODE == MODE_A || MODE == MODE_EULER) {
-#pragma unroll
-                for (int c = 0; c < 4; ++c) un[c] = s.X[((c * (TX + 6) + (i + 3)) * TY + j) * TZ + k];
+        // ---- 3. every face of the tile: WENO-Z, projection, HLL ----
+        for (int f = tid; f < NF; f += NT) {
+            int axis, i, j, k;
+            if (f < NFX) {
+                axis = 0; k = f % TZ; j = (f / TZ) % TY; i = f / (TZ * TY);
+            } else if (f < NFX + NFY) {
+                int u = f - NFX;
+                axis = 1; k = u % TZ; j = (u / TZ) % (TY + 1); i = u / (TZ * (TY + 1));
             } else {
-                load_cell<MODE_A>(a, cf, co, a.U, N, gi, gj, gk, un);
+                int u = f - NFX - NFY;
+                axis = 2; k = u % (TZ + 1); j = (u / (TZ + 1)) % TY; i = u / ((TZ + 1) * TY);
             }
-            const double s0 = co.S0[m];
-            if (MODE == MODE_A) {
-                double u1[4], v1[4];
+            double L[4], R[4];
+            const int di = axis == 0, dj = axis == 1, dk = axis == 2;
 #pragma unroll
-                for (int c = 0; c < 4; ++c) {
-                    double v0 = s0 * un[c];
-                    double v = L[c] * dE + v0;
-                    v1[c] = v;
-                    double w = v * (c == 0 ? co.c1p[m] : co.c1c[m]);
-                    u1[c] = w / co.S1[m];
+            for (int c = 0; c < 4; ++c) {
+                double w[6];
+#pragma unroll
+                for (int q = 0; q < 6; ++q) {
+                    int o = q - 3;
+                    w[q] = sval(s, c, i + o * di, j + o * dj, k + o * dk);
                 }
-                project(u1[0], u1[1], u1[2], u1[3]);
+                L[c] = weno_left(w[0], w[1], w[2], w[3], w[4]);
+                R[c] = weno_left(w[5], w[4], w[3], w[2], w[1]);
+            }
+            project(L[0], L[1], L[2], L[3]);
+            project(R[0], R[1], R[2], R[3]);
+            double F[4];
+            hll_flux(L, R, axis, unit, F);
 #pragma unroll
-                for (int c = 0; c < 4; ++c) {
-                    a.U1[c * N + o] = u1[c];
-                    a.V[c * N + o] = v1[c];
-                }
-                double q0 = un[0] * s0, q1 = u1[0] * co.S1[m];
-                a.qpart[o] = 1.0 / 6.0 * q0 + 1.0 / 6.0 * q1;
-            } else if (MODE == MODE_B) {
-                double u2[4];
+            for (int c = 0; c < 4; ++c) s.F[c * NF + f] = F[c];
+        }
+        __syncthreads();
+        // ---- 4. divergence and the stage update, one cell per thread ----
+        const int k = tid % TZ, j = (tid / TZ) % TY, i = tid / (TZ * TY);
+        const int li = i0 + i, lj = j0 + j, lk = k0 + k;
+        const bool valid = li < nx && lj < ny && lk < nz;
+        double phi_new = -1.0;   // for the moving box's slab maxima
+        if (valid) {
+            const int fx0 = (i * TY + j) * TZ + k, fx1 = ((i + 1) * TY + j) * TZ + k;
+            const int fy0 = NFX + (i * (TY + 1) + j) * TZ + k, fy1 = NFX + (i * (TY + 1) + j + 1) * TZ + k;
+            const int fz0 = NFX + NFY + (i * TY + j) * (TZ + 1) + k, fz1 = fz0 + 1;
+            double L[4];
 #pragma unroll
-                for (int c = 0; c < 4; ++c) {
-                    double r = L[c] * (c == 0 ? co.c1ip[m] : co.c1ic[m]);
-                    r = (r * dE + a.V[c * N + o]) * 0.25;
-                    double v = 0.75 * (s0 * un[c]) + r;
-                    a.V[c * N + o] = v;
-                    double w = v * (c == 0 ? co.c2p[m] : co.c2c[m]);
-                    u2[c] = w / co.S2[m];
-                }
-                project(u2[0], u2[1], u2[2], u2[3]);
+            for (int c = 0; c < 4; ++c) {
+                const double *F = s.F + c * NF;
+                double gx = (F[fx1] - F[fx0]) / cf.dx;
+                double gy = (F[fy1] - F[fy0]) / cf.dy;
+                double gz = (F[fz1] - F[fz0]) / cf.dz;
+                L[c] = -(gx + gy + gz);
+            }
+            const size_t o = ((size_t)li * ny + lj) * nz + lk;
+            if (MODE == MODE_RHS) {
 #pragma unroll
-                for (int c = 0; c < 4; ++c) a.U2[c * N + o] = u2[c];
+                for (int c = 0; c < 4; ++c) a.rhs_out[c * N + o] = L[c];
             } else {
-                double unew[4];
-                double ed;
-                if (MODE == MODE_C) {
+                const size_t go = global_cell(cf, d, li, lj, lk);
+                const int m = cf.ids[go];
+                const double dE = co.dE;
+                // the accepted state at this cell (with the Strang half step applied)
+                double un[4];
+                if (MODE == MODE_A || MODE == MODE_EULER) {
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) un[c] = s.X[((c * (TX + 6) + (i + 3)) * TY + j) * TZ + k];
+                } else {
+                    load_cell<MODE_A>(cf, co, d, Ua, li, lj, lk, un);
+                }
+                const double s0 = co.S0[m];
+                if (MODE == MODE_A) {
+                    double u1[4], v1[4];
 #pragma unroll
                     for (int c = 0; c < 4; ++c) {
-                        double r = L[c] * (c == 0 ? co.c2ip[m] : co.c2ic[m]);
-                        r = (r * dE + a.V[c * N + o]) * (2.0 / 3.0);
-                        double v = 1.0 / 3.0 * (s0 * un[c]) + r;
+                        double v0 = s0 * un[c];
+                        double v = L[c] * dE + v0;
+                        v1[c] = v;
                         double w = v * (c == 0 ? co.c1p[m] : co.c1c[m]);
-                        unew[c] = w / co.S1[m];
+                        u1[c] = w / co.S1[m];
                     }
-                    project(unew[0], unew[1], unew[2], unew[3]);
-                    double q2 = s.X[((0 * (TX + 6) + (i + 3)) * TY + j) * TZ + k] * co.S2[m];
-                    ed = dE * (a.qpart[o] + 2.0 / 3.0 * q2);
-                } else {   // forward Euler, numerics/energy.py:663-722
+                    project(u1[0], u1[1], u1[2], u1[3]);
 #pragma unroll
                     for (int c = 0; c < 4; ++c) {
-                        double w = L[c] * dE + s0 * un[c];
-                        unew[c] = w / co.S1[m];
+                        a.U1[c * N + o] = u1[c];
+                        a.V[c * N + o] = v1[c];
                     }
-                    project(unew[0], unew[1], unew[2], unew[3]);
-                    ed = dE * un[0] * s0;
-                }
-                if (cf.strang) {
-                    if (cf.nuclear)
+                    double q0 = un[0] * s0, q1 = u1[0] * co.S1[m];
+                    a.qpart[o] = 1.0 / 6.0 * q0 + 1.0 / 6.0 * q1;
+                } else if (MODE == MODE_B) {
+                    double u2[4];
 #pragma unroll
-                        for (int c = 0; c < 4; ++c) unew[c] *= co.hn[m];
-                    if (cf.scattering != PDM1_SCATTERING_OFF)
-#pragma unroll
-                        for (int c = 1; c < 4; ++c) unew[c] *= co.hs[m];
-                }
-                double *dst = MODE == MODE_C ? a.U : a.U1;
-#pragma unroll
-                for (int c = 0; c < 4; ++c) dst[c * N + o] = unew[c];
-                if (a.edep) a.edep[o] = ed;
-                else a.dose[o] += ed * kMevToJoule / cf.mats[m].density;
-                if (MODE == MODE_C) {
-                    if (co.snap_slot >= 0 && a.snap) {
-                        double *sn = a.snap + (size_t)co.snap_slot * 4 * N;
-#pragma unroll
-                        for (int c = 0; c < 4; ++c) sn[c * N + o] = unew[c];
+                    for (int c = 0; c < 4; ++c) {
+                        double r = L[c] * (c == 0 ? co.c1ip[m] : co.c1ic[m]);
+                        r = (r * dE + a.V[c * N + o]) * 0.25;
+                        double v = 0.75 * (s0 * un[c]) + r;
+                        a.V[c * N + o] = v;
+                        double w = v * (c == 0 ? co.c2p[m] : co.c2c[m]);
+                        u2[c] = w / co.S2[m];
                     }
-                    cfl_contrib(cf, co, unew, m, gi, gj, gk, cta_inv);
+                    project(u2[0], u2[1], u2[2], u2[3]);
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) a.U2[c * N + o] = u2[c];
+                } else {
+                    double unew[4];
+                    double ed;
+                    if (MODE == MODE_C) {
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) {
+                            double r = L[c] * (c == 0 ? co.c2ip[m] : co.c2ic[m]);
+                            r = (r * dE + a.V[c * N + o]) * (2.0 / 3.0);
+                            double v = 1.0 / 3.0 * (s0 * un[c]) + r;
+                            double w = v * (c == 0 ? co.c1p[m] : co.c1c[m]);
+                            unew[c] = w / co.S1[m];
+                        }
+                        project(unew[0], unew[1], unew[2], unew[3]);
+                        double q2 = s.X[((0 * (TX + 6) + (i + 3)) * TY + j) * TZ + k] * co.S2[m];
+                        ed = dE * (a.qpart[o] + 2.0 / 3.0 * q2);
+                    } else {   // forward Euler, numerics/energy.py:663-722
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) {
+                            double w = L[c] * dE + s0 * un[c];
+                            unew[c] = w / co.S1[m];
+                        }
+                        project(unew[0], unew[1], unew[2], unew[3]);
+                        ed = dE * un[0] * s0;
+                    }
+                    if (cf.strang) {
+                        if (cf.nuclear)
+#pragma unroll
+                            for (int c = 0; c < 4; ++c) unew[c] *= co.hn[m];
+                        if (cf.scattering != PDM1_SCATTERING_OFF)
+#pragma unroll
+                            for (int c = 1; c < 4; ++c) unew[c] *= co.hs[m];
+                    }
+                    double *dst = MODE == MODE_C ? Ua : a.U1;
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) dst[c * N + o] = unew[c];
+                    if (a.edep) a.edep[o] = ed;
+                    else a.dose[go] += ed * kMevToJoule / cf.mats[m].density;
+                    if (MODE == MODE_C) {
+                        if (co.snap_slot >= 0 && a.snap) {
+                            const size_t NG = (size_t)cf.nx * cf.ny * cf.nz;
+                            double *sn = a.snap + (size_t)co.snap_slot * 4 * NG;
+#pragma unroll
+                            for (int c = 0; c < 4; ++c) sn[c * NG + go] = unew[c];
+                        }
+                        if (!cf.moving) {
+                            double phi_in = 0.0;
+                            if (lk == 0 && d.inflow)
+                                phi_in = cf.spatial[(size_t)(d.i0 + li) * cf.ny + (d.j0 + lj)] * co.ed_next;
+                            double v = cfl_term(cf, unew, co.S1[m], lk == 0, phi_in, all_axes);
+                            cta_inv = fmax(cta_inv, v);
+                        }
+                        phi_new = unew[0];
+                    }
                 }
             }
         }
+        if (MODE == MODE_C && cf.moving) {
+            __syncthreads();
+            s.F[tid] = phi_new;   // the flux buffer is free after the divergence
+            __syncthreads();
+            tile_slab_max(cf, d, s.F, i0, j0, k0);
+        }
+        __syncthreads();   // shared memory is reused by the next tile
     }
-    if (MODE == MODE_C) block_max_atomic(cta_inv, &a.st->inv_bits);
+    if (MODE == MODE_C && !cf.moving) block_max_atomic(cta_inv, &a.st->inv_bits);
 }
 
-// Forward Euler writes U1; this copies it back, snapshots and reduces the CFL.
+// Forward Euler writes U1; this copies it back, snapshots, and either reduces
+// the CFL bound (static domain) or the slab maxima (moving box).
 __global__ void __launch_bounds__(NT) euler_finish_kernel(StageArgs a) {
     const ConfigDev &cf = *a.cf;
     const Coeffs &co = *a.co;
     if (!co.active) return;
-    const size_t N = (size_t)cf.nx * cf.ny * cf.nz;
+    const DomainDev d = a.st->dom;
+    double *Ua = a.st->Ua;
+    const size_t N = (size_t)d.nx * d.ny * d.nz, NG = (size_t)cf.nx * cf.ny * cf.nz;
+    const bool all_axes[3] = {true, true, true};
     double inv = 0.0;
     for (size_t o = (size_t)blockIdx.x * NT + threadIdx.x; o < N; o += (size_t)gridDim.x * NT) {
         double u[4];
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             u[c] = a.U1[c * N + o];
-            a.U[c * N + o] = u[c];
+            Ua[c * N + o] = u[c];
         }
+        int lk = (int)(o % d.nz), lj = (int)((o / d.nz) % d.ny), li = (int)(o / ((size_t)d.nz * d.ny));
+        size_t go = global_cell(cf, d, li, lj, lk);
         if (co.snap_slot >= 0 && a.snap) {
-            double *sn = a.snap + (size_t)co.snap_slot * 4 * N;
+            double *sn = a.snap + (size_t)co.snap_slot * 4 * NG;
 #pragma unroll
-            for (int c = 0; c < 4; ++c) sn[c * N + o] = u[c];
+            for (int c = 0; c < 4; ++c) sn[c * NG + go] = u[c];
         }
-        int gk = (int)(o % cf.nz), gj = (int)((o / cf.nz) % cf.ny), gi = (int)(o / ((size_t)cf.nz * cf.ny));
-        double v;
-        cfl_contrib(cf, co, u, cf.ids[o], gi, gj, gk, v);
-        inv = fmax(inv, v);
+        if (cf.moving) {
+            atomic_max_double(&cf.slab[li], u[0]);
+            atomic_max_double(&cf.slab[cf.nx + lj], u[0]);
+            atomic_max_double(&cf.slab[cf.nx + cf.ny + lk], u[0]);
+        } else {
+            double phi_in = 0.0;
+            if (lk == 0 && d.inflow) phi_in = cf.spatial[(size_t)(d.i0 + li) * cf.ny + (d.j0 + lj)] * co.ed_next;
+            inv = fmax(inv, cfl_term(cf, u, co.S1[cf.ids[go]], lk == 0, phi_in, all_axes));
+        }
     }
-    block_max_atomic(inv, &a.st->inv_bits);
+    if (!cf.moving) block_max_atomic(inv, &a.st->inv_bits);
 }
 
-// CFL bound of a state (energy.py:539-660) with S and spectrum of co->S1 / ed_next.
-__global__ void __launch_bounds__(NT) cfl_kernel(const ConfigDev *cfp, const Coeffs *co,
-                                                 MarchState *st, const double *U) {
+// CFL bound of the state on the current domain (energy.py:539-660), with S and
+// the spectrum at the state's energy: co->S1 / ed_next (static domain, first
+// step) or co->S_cfl / ed_cfl (moving box, every step).  With vacuum-aware
+// masks (energy.py:459-537) a direction counts only within 3 cells, along that
+// axis, of an active cell.
+__global__ void __launch_bounds__(NT) cfl_kernel(const ConfigDev *cfp, const Coeffs *co, MarchState *st,
+                                                 int use_box_coeffs) {
     const ConfigDev &cf = *cfp;
-    const size_t N = (size_t)cf.nx * cf.ny * cf.nz;
+    if (st->done) return;
+    const DomainDev d = st->dom;
+    const double *U = st->Ua;
+    const size_t N = (size_t)d.nx * d.ny * d.nz;
+    const double *S = use_box_coeffs ? co->S_cfl : co->S1;
+    const double ed = use_box_coeffs ? co->ed_cfl : co->ed_next;
+    bool masks = false;
+    if (cf.moving && cf.vacuum_aware && use_box_coeffs) {
+        double sc = fmax(__longlong_as_double((long long)st->newmax_bits), st->pin_max);
+        masks = sc != 0.0;   // energy.py:518-523: no transported state and no beam -> all directions
+    }
     double inv = 0.0;
     for (size_t o = (size_t)blockIdx.x * NT + threadIdx.x; o < N; o += (size_t)gridDim.x * NT) {
         double u[4];
 #pragma unroll
         for (int c = 0; c < 4; ++c) u[c] = U[c * N + o];
-        int gk = (int)(o % cf.nz), gj = (int)((o / cf.nz) % cf.ny), gi = (int)(o / ((size_t)cf.nz * cf.ny));
-        double v;
-        cfl_contrib(cf, *co, u, cf.ids[o], gi, gj, gk, v);
-        inv = fmax(inv, v);
+        int lk = (int)(o % d.nz), lj = (int)((o / d.nz) % d.ny), li = (int)(o / ((size_t)d.nz * d.ny));
+        bool use[3] = {true, true, true};
+        if (masks) {
+            const unsigned char *act = cf.active;
+            for (int ax = 0; ax < 3; ++ax) {
+                int lo, hi, pos;
+                size_t stride;
+                if (ax == 0) { pos = li; lo = max(0, li - 3); hi = min(d.nx - 1, li + 3); stride = (size_t)d.ny * d.nz; }
+                else if (ax == 1) { pos = lj; lo = max(0, lj - 3); hi = min(d.ny - 1, lj + 3); stride = d.nz; }
+                else { pos = lk; lo = max(0, lk - 3); hi = min(d.nz - 1, lk + 3); stride = 1; }
+                bool any = false;
+                for (int q = lo; q <= hi && !any; ++q) any = act[o + (long long)(q - pos) * (long long)stride] != 0;
+                use[ax] = any;
+            }
+        }
+        double phi_in = 0.0;
+        if (lk == 0 && d.inflow) phi_in = cf.spatial[(size_t)(d.i0 + li) * cf.ny + (d.j0 + lj)] * ed;
+        inv = fmax(inv, cfl_term(cf, u, S[cf.ids[global_cell(cf, d, li, lj, lk)]], lk == 0, phi_in, use));
     }
     block_max_atomic(inv, &st->inv_bits);
+}
+
+// ---------------------------------------------------------------------------
+// Moving active box (numerics/moving_active_domain.py, energy.py:1262-1494)
+// ---------------------------------------------------------------------------
+
+// Start of the march: the initial box, the compact state copied from the
+// caller's full-grid U, and the slab maxima of that state.
+__global__ void __launch_bounds__(NT) box_init_kernel(const ConfigDev *cfp, MarchState *st, const double *Ufull) {
+    const ConfigDev &cf = *cfp;
+    const DomainDev d = cf.init_box;
+    const size_t N = (size_t)d.nx * d.ny * d.nz, NG = (size_t)cf.nx * cf.ny * cf.nz;
+    for (size_t o = (size_t)blockIdx.x * NT + threadIdx.x; o < N; o += (size_t)gridDim.x * NT) {
+        int lk = (int)(o % d.nz), lj = (int)((o / d.nz) % d.ny), li = (int)(o / ((size_t)d.nz * d.ny));
+        size_t go = global_cell(cf, d, li, lj, lk);
+        double u0 = 0.0;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            double v = Ufull[c * NG + go];
+            cf.bufA[c * N + o] = v;
+            if (c == 0) u0 = v;
+        }
+        atomic_max_double(&cf.slab[li], u0);
+        atomic_max_double(&cf.slab[cf.nx + lj], u0);
+        atomic_max_double(&cf.slab[cf.nx + cf.ny + lk], u0);
+    }
+}
+
+// One CTA at the start of every step: desired_box (moving_active_domain.py:
+// 107-193) from the slab maxima of the current state and the inflow at the
+// step's energy; the switch to the new box; S and spectrum for the CFL.
+__global__ void __launch_bounds__(256) box_kernel(const ConfigDev *cfp, Coeffs *co, MarchState *st) {
+    const ConfigDev &cf = *cfp;
+    __shared__ double red[256];
+    __shared__ double s_ed, s_scale;
+    __shared__ int s_lo[3], s_hi[3];
+    __shared__ int s_done;
+    const int t = threadIdx.x;
+    if (t == 0) s_done = st->done || st->error;
+    __syncthreads();
+    if (s_done) return;
+    const DomainDev d = st->dom;
+    const double E = st->E;
+    if (t == 0) s_ed = energy_density(cf, E);
+    if (t < cf.nm) {
+        double sv = 1.0;
+        if (!stopping_power_dev(cf.mats[t], E, sv)) atomicOr(&st->error, ERR_DEV_RANGE);
+        co->S_cfl[t] = sv;
+    }
+    __syncthreads();
+    const double ed = s_ed;
+    const unsigned long long *sx = cf.slab, *sy = cf.slab + cf.nx, *sz = cf.slab + cf.nx + cf.ny;
+    auto as_d = [](unsigned long long b) { return __longlong_as_double((long long)b); };
+    // scale = max(max phi, max phi_in)   (phi_in only while the box touches z = 0)
+    double m = 0.0;
+    for (int i = t; i < d.nx; i += 256) m = fmax(m, as_d(sx[i]));
+    if (d.inflow)
+        for (int e = t; e < d.nx * d.ny; e += 256) {
+            int i = e / d.ny, j = e % d.ny;
+            m = fmax(m, cf.spatial[(size_t)(d.i0 + i) * cf.ny + (d.j0 + j)] * ed);
+        }
+    red[t] = m;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (t < w) red[t] = fmax(red[t], red[t + w]);
+        __syncthreads();
+    }
+    if (t == 0) {
+        s_scale = red[0];
+        for (int q = 0; q < 3; ++q) { s_lo[q] = INT_MAX; s_hi[q] = -1; }
+    }
+    __syncthreads();
+    const double scale = s_scale;
+    const double thr = cf.tol * scale;
+    if (scale != 0.0) {
+        // active x / y indices: slab max above the threshold, or an inflow cell
+        // of that row above it (the inflow joins the k = 0 layer)
+        for (int i = t; i < d.nx; i += 256) {
+            bool act = as_d(sx[i]) > thr;
+            if (!act && d.inflow)
+                for (int j = 0; j < d.ny && !act; ++j)
+                    act = cf.spatial[(size_t)(d.i0 + i) * cf.ny + (d.j0 + j)] * ed > thr;
+            if (act) { atomicMin(&s_lo[0], i); atomicMax(&s_hi[0], i); }
+        }
+        for (int j = t; j < d.ny; j += 256) {
+            bool act = as_d(sy[j]) > thr;
+            if (!act && d.inflow)
+                for (int i = 0; i < d.nx && !act; ++i)
+                    act = cf.spatial[(size_t)(d.i0 + i) * cf.ny + (d.j0 + j)] * ed > thr;
+            if (act) { atomicMin(&s_lo[1], j); atomicMax(&s_hi[1], j); }
+        }
+        for (int k = t; k < d.nz; k += 256) {
+            bool act = as_d(sz[k]) > thr;
+            if (!act && k == 0 && d.inflow)
+                for (int e = 0; e < d.nx * d.ny && !act; ++e)
+                    act = cf.spatial[(size_t)(d.i0 + e / d.ny) * cf.ny + (d.j0 + e % d.ny)] * ed > thr;
+            if (act) { atomicMin(&s_lo[2], k); atomicMax(&s_hi[2], k); }
+        }
+    }
+    __syncthreads();
+    // reset the slab maxima for this step's stage C
+    for (int e = t; e < cf.nx + cf.ny + cf.nz; e += 256) cf.slab[e] = 0ull;
+    if (t == 0) {
+        DomainDev nb;
+        if (scale == 0.0 || s_hi[0] < 0 || s_hi[1] < 0 || s_hi[2] < 0) {
+            nb = cf.init_box;
+        } else {
+            const int g = cf.guard;
+            int ai0 = d.i0 + s_lo[0], ai1 = d.i0 + s_hi[0] + 1;
+            int aj0 = d.j0 + s_lo[1], aj1 = d.j0 + s_hi[1] + 1;
+            int ak0 = d.k0 + s_lo[2], ak1 = d.k0 + s_hi[2] + 1;
+            int bi0 = ai0 - g > 0 ? ai0 - g : 0, bi1 = ai1 + g < cf.nx ? ai1 + g : cf.nx;
+            int bj0 = aj0 - g > 0 ? aj0 - g : 0, bj1 = aj1 + g < cf.ny ? aj1 + g : cf.ny;
+            int bk0 = ak0 - g > 0 ? ak0 - g : 0, bk1 = ak1 + g < cf.nz ? ak1 + g : cf.nz;
+            nb = make_domain(bi0, bj0, bk0, bi1 - bi0, bj1 - bj0, bk1 - bk0, bk0 == 0);
+        }
+        bool same = nb.i0 == d.i0 && nb.j0 == d.j0 && nb.k0 == d.k0 && nb.nx == d.nx && nb.ny == d.ny && nb.nz == d.nz;
+        st->reboxed = same ? 0 : 1;
+        if (!same) {
+            st->prev = d;
+            st->Uprev = st->Ua;
+            st->Ua = st->Ua == cf.bufA ? cf.bufB : cf.bufA;
+            st->dom = nb;
+        }
+        st->inv_bits = 0ull;
+        co->ed_cfl = ed;
+        // vacuum-aware masks (energy.py:496-537) use the inflow of the new box
+        st->newmax_bits = 0ull;
+        double pin = 0.0;
+        if (cf.vacuum_aware && nb.inflow)
+            for (int e = 0; e < nb.nx * nb.ny; ++e)
+                pin = fmax(pin, cf.spatial[(size_t)(nb.i0 + e / nb.ny) * cf.ny + (nb.j0 + e % nb.ny)] * ed);
+        st->pin_max = pin;
+    }
+}
+
+// Copy the overlap of the previous box into the new one (zeros elsewhere,
+// moving_active_domain.py:196-232); for the vacuum-aware CFL also the max phi
+// of the new box.
+__global__ void __launch_bounds__(NT) rebox_kernel(const ConfigDev *cfp, MarchState *st) {
+    const ConfigDev &cf = *cfp;
+    if (st->done) return;
+    const DomainDev d = st->dom;
+    const bool moved = st->reboxed != 0;
+    if (!moved && !cf.vacuum_aware) return;
+    const DomainDev p = st->prev;
+    const double *Up = st->Uprev;
+    double *Ua = st->Ua;
+    const size_t N = (size_t)d.nx * d.ny * d.nz, NP = (size_t)p.nx * p.ny * p.nz;
+    double m = 0.0;
+    for (size_t o = (size_t)blockIdx.x * NT + threadIdx.x; o < N; o += (size_t)gridDim.x * NT) {
+        if (moved) {
+            int lk = (int)(o % d.nz), lj = (int)((o / d.nz) % d.ny), li = (int)(o / ((size_t)d.nz * d.ny));
+            int pi = d.i0 + li - p.i0, pj = d.j0 + lj - p.j0, pk = d.k0 + lk - p.k0;
+            bool in = pi >= 0 && pi < p.nx && pj >= 0 && pj < p.ny && pk >= 0 && pk < p.nz;
+            size_t po = in ? ((size_t)pi * p.ny + pj) * p.nz + pk : 0;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) Ua[c * N + o] = in ? Up[c * NP + po] : 0.0;
+        }
+        m = fmax(m, Ua[o]);
+    }
+    if (cf.vacuum_aware) block_max_atomic(m, &st->newmax_bits);
+}
+
+// Activity mask of the vacuum-aware CFL: phi above tol * max(phi, phi_in),
+// plus the inflow at the entrance layer (numerics/energy.py:496-537).
+__global__ void __launch_bounds__(NT) mask_kernel(const ConfigDev *cfp, const Coeffs *co, const MarchState *st) {
+    const ConfigDev &cf = *cfp;
+    if (st->done) return;
+    const DomainDev d = st->dom;
+    const double *Ua = st->Ua;
+    const double scale = fmax(__longlong_as_double((long long)st->newmax_bits), st->pin_max);
+    if (scale == 0.0) return;
+    const double thr = cf.tol * scale;
+    const double ed = co->ed_cfl;
+    const size_t N = (size_t)d.nx * d.ny * d.nz;
+    for (size_t o = (size_t)blockIdx.x * NT + threadIdx.x; o < N; o += (size_t)gridDim.x * NT) {
+        int lk = (int)(o % d.nz), lj = (int)((o / d.nz) % d.ny), li = (int)(o / ((size_t)d.nz * d.ny));
+        bool act = Ua[o] > thr;
+        if (lk == 0 && d.inflow)
+            act = act || cf.spatial[(size_t)(d.i0 + li) * cf.ny + (d.j0 + lj)] * ed > thr;
+        cf.active[o] = act ? 1 : 0;
+    }
+}
+
+// Scatter the compact state into a full-grid array (zeros elsewhere),
+// moving_active_domain.py:235-244.
+__global__ void __launch_bounds__(NT) embed_kernel(const ConfigDev *cfp, const MarchState *st, double *Ufull) {
+    const ConfigDev &cf = *cfp;
+    const DomainDev d = st->dom;
+    const double *Ua = st->Ua;
+    const size_t N = (size_t)d.nx * d.ny * d.nz, NG = (size_t)cf.nx * cf.ny * cf.nz;
+    for (size_t go = (size_t)blockIdx.x * NT + threadIdx.x; go < NG; go += (size_t)gridDim.x * NT) {
+        int gk = (int)(go % cf.nz), gj = (int)((go / cf.nz) % cf.ny), gi = (int)(go / ((size_t)cf.nz * cf.ny));
+        int li = gi - d.i0, lj = gj - d.j0, lk = gk - d.k0;
+        bool in = li >= 0 && li < d.nx && lj >= 0 && lj < d.ny && lk >= 0 && lk < d.nz;
+        size_t o = ((size_t)li * d.ny + lj) * d.nz + lk;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) Ufull[c * NG + go] = in ? Ua[c * N + o] : 0.0;
+    }
 }
 
 // Scalar batches for unit parity checks
@@ -812,6 +1158,9 @@ struct pdm1_plan {
     double *d_spatial = nullptr;
     double *d_targets = nullptr;
     double *d_U1 = nullptr, *d_U2 = nullptr, *d_V = nullptr, *d_q = nullptr;
+    double *d_bufA = nullptr, *d_bufB = nullptr;   // moving box: compact-state ping-pong
+    unsigned long long *d_slab = nullptr;
+    unsigned char *d_active = nullptr;
     size_t workspace = 0;
     std::vector<int32_t> h_ids;
     std::vector<double> h_spatial;
@@ -866,7 +1215,10 @@ int validate_problem(const pdm1_problem *p) {
     if (!(p->max_energy_step > 0.0)) return set_error(PDM1_ERR_ARGUMENT, "max_energy_step must be positive.");
     if (p->energy_scheme < 0 || p->energy_scheme > 2) return set_error(PDM1_ERR_UNSUPPORTED, "unknown energy scheme");
     if (p->precision != PDM1_FP64 && p->precision != PDM1_FP32_FP64) return set_error(PDM1_ERR_ARGUMENT, "unknown precision");
-    if (p->moving_active_domain) return set_error(PDM1_ERR_UNSUPPORTED, "moving_active_domain is not built in this library version");
+    if (p->moving_active_domain && p->active_guard_cells < 0)
+        return set_error(PDM1_ERR_ARGUMENT, "active_guard_cells must be non-negative");
+    if (p->moving_active_domain && !(p->active_relative_tolerance >= 0.0))
+        return set_error(PDM1_ERR_ARGUMENT, "active_relative_tolerance must be non-negative");
     for (int m = 0; m < p->n_materials; ++m) {
         const pdm1_material &mt = p->materials[m];
         if (!table_ok(mt.stopping_power) || !table_ok(mt.transport) || !table_ok(mt.nuclear))
@@ -900,12 +1252,11 @@ int check_energy_range(const pdm1_plan *pl, double e_hi, double e_lo) {
     return PDM1_OK;
 }
 
-StageArgs make_args(pdm1_plan *pl, double *U, double *dose, double *edep, double *snap) {
+StageArgs make_args(pdm1_plan *pl, double *dose, double *edep, double *snap) {
     StageArgs a{};
     a.cf = pl->d_cf;
     a.co = pl->d_co;
     a.st = pl->d_st;
-    a.U = U;
     a.U1 = pl->d_U1;
     a.U2 = pl->d_U2;
     a.V = pl->d_V;
@@ -927,44 +1278,62 @@ int cell_blocks(const pdm1_problem &p) {
 }
 
 // Launch one energy step (prologue + stages) on `stream`; returns launches.
+// The moving box's per-step work ahead of the prologue: desired box, rebox,
+// activity mask, CFL bound over the new box.
+int launch_box_step(pdm1_plan *pl, cudaStream_t stream) {
+    const pdm1_problem &p = pl->p;
+    box_kernel<<<1, 256, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st);
+    rebox_kernel<<<cell_blocks(p), NT, 0, stream>>>(pl->d_cf, pl->d_st);
+    int n = 3;
+    if (p.vacuum_aware_cfl) {
+        mask_kernel<<<cell_blocks(p), NT, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st);
+        ++n;
+    }
+    cfl_kernel<<<cell_blocks(p), NT, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, 1);
+    return n;
+}
+
 int launch_step(pdm1_plan *pl, const StageArgs &a, cudaStream_t stream) {
     const pdm1_problem &p = pl->p;
-    int tiles = n_tiles(p);
+    const int grid = pl->cf.grid_ctas;
     prologue_kernel<<<1, 256, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, nullptr);
     if (p.energy_scheme == PDM1_SCHEME_FORWARD_EULER) {
-        stage_kernel<MODE_EULER><<<tiles, NT, kStageSmem, stream>>>(a);
+        stage_kernel<MODE_EULER><<<grid, NT, kStageSmem, stream>>>(a);
         euler_finish_kernel<<<cell_blocks(p), NT, 0, stream>>>(a);
         return 3;
     }
-    stage_kernel<MODE_A><<<tiles, NT, kStageSmem, stream>>>(a);
-    stage_kernel<MODE_B><<<tiles, NT, kStageSmem, stream>>>(a);
-    stage_kernel<MODE_C><<<tiles, NT, kStageSmem, stream>>>(a);
+    stage_kernel<MODE_A><<<grid, NT, kStageSmem, stream>>>(a);
+    stage_kernel<MODE_B><<<grid, NT, kStageSmem, stream>>>(a);
+    stage_kernel<MODE_C><<<grid, NT, kStageSmem, stream>>>(a);
     return 4;
 }
 
 int launch_step_with_energies(pdm1_plan *pl, const StageArgs &a, double *energies, cudaStream_t stream,
                               int slot) {
     const pdm1_problem &p = pl->p;
-    int tiles = n_tiles(p);
+    const int grid = pl->cf.grid_ctas;
+    int launched = 0;
+    if (p.moving_active_domain) launched += launch_box_step(pl, stream);
     prologue_kernel<<<1, 256, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, energies);
     // external event nodes: real timestamps when the step is replayed from a graph
     cudaEventRecordWithFlags(pl->ev[2 * slot], stream, cudaEventRecordExternal);
     int n;
     if (p.energy_scheme == PDM1_SCHEME_FORWARD_EULER) {
-        stage_kernel<MODE_EULER><<<tiles, NT, kStageSmem, stream>>>(a);
+        stage_kernel<MODE_EULER><<<grid, NT, kStageSmem, stream>>>(a);
         n = 1;
     } else {
-        stage_kernel<MODE_A><<<tiles, NT, kStageSmem, stream>>>(a);
-        stage_kernel<MODE_B><<<tiles, NT, kStageSmem, stream>>>(a);
-        stage_kernel<MODE_C><<<tiles, NT, kStageSmem, stream>>>(a);
+        stage_kernel<MODE_A><<<grid, NT, kStageSmem, stream>>>(a);
+        stage_kernel<MODE_B><<<grid, NT, kStageSmem, stream>>>(a);
+        stage_kernel<MODE_C><<<grid, NT, kStageSmem, stream>>>(a);
         n = 3;
     }
     cudaEventRecordWithFlags(pl->ev[2 * slot + 1], stream, cudaEventRecordExternal);
+    launched += n + 1;
     if (p.energy_scheme == PDM1_SCHEME_FORWARD_EULER) {
         euler_finish_kernel<<<cell_blocks(p), NT, 0, stream>>>(a);
-        return 3;
+        ++launched;
     }
-    return n + 1;
+    return launched;
 }
 
 int set_smem_attributes() {
@@ -1007,6 +1376,10 @@ void pdm1_plan_destroy(pdm1_plan *pl) {
     cudaFree(pl->d_U2);
     cudaFree(pl->d_V);
     cudaFree(pl->d_q);
+    cudaFree(pl->d_bufA);
+    cudaFree(pl->d_bufB);
+    cudaFree(pl->d_slab);
+    cudaFree(pl->d_active);
     if (pl->ready) cudaEventDestroy(pl->ready);
     for (cudaEvent_t e : pl->ev)
         if (e) cudaEventDestroy(e);
@@ -1083,6 +1456,12 @@ int pdm1_plan_create(const pdm1_problem *problem, pdm1_plan **out) {
     ALLOC(pl->d_U2, 4 * N * sizeof(double));
     ALLOC(pl->d_V, 4 * N * sizeof(double));
     ALLOC(pl->d_q, N * sizeof(double));
+    if (p.moving_active_domain) {
+        ALLOC(pl->d_bufA, 4 * N * sizeof(double));
+        ALLOC(pl->d_bufB, 4 * N * sizeof(double));
+        ALLOC(pl->d_slab, (size_t)(p.nx + p.ny + p.nz) * sizeof(unsigned long long));
+        ALLOC(pl->d_active, N);
+    }
 #undef ALLOC
     pl->workspace = (13 * N) * sizeof(double);
     if (cudaMallocHost((void **)&pl->h_st, sizeof(MarchState)) != cudaSuccess ||
@@ -1105,6 +1484,40 @@ int pdm1_plan_create(const pdm1_problem *problem, pdm1_plan **out) {
     cf.ids = pl->d_ids;
     cf.spatial = pl->d_spatial;
     cf.targets = pl->d_targets;
+    // moving active box: initial box from the inflow support (moving_active_domain.py:35-60)
+    cf.moving = p.moving_active_domain ? 1 : 0;
+    cf.vacuum_aware = (p.moving_active_domain && p.vacuum_aware_cfl) ? 1 : 0;
+    cf.guard = p.active_guard_cells;
+    cf.tol = p.active_relative_tolerance;
+    cf.bufA = pl->d_bufA;
+    cf.bufB = pl->d_bufB;
+    cf.slab = pl->d_slab;
+    cf.active = pl->d_active;
+    if (p.moving_active_domain) {
+        int ilo = -1, ihi = -1, jlo = -1, jhi = -1;
+        for (int i = 0; i < p.nx; ++i)
+            for (int j = 0; j < p.ny; ++j)
+                if (pl->h_spatial[(size_t)i * p.ny + j] > 0.0) {
+                    if (ilo < 0 || i < ilo) ilo = i;
+                    if (i > ihi) ihi = i;
+                    if (jlo < 0 || j < jlo) jlo = j;
+                    if (j > jhi) jhi = j;
+                }
+        if (ilo < 0) return fail(set_error(PDM1_ERR_NO_BEAM, "Beam inflow has empty transverse support."));
+        const int g = p.active_guard_cells;
+        int i0 = std::max(0, ilo - g), i1 = std::min(p.nx, ihi + 1 + g);
+        int j0 = std::max(0, jlo - g), j1 = std::min(p.ny, jhi + 1 + g);
+        int k1 = std::min(p.nz, 1 + g);
+        cf.init_box = make_domain(i0, j0, 0, i1 - i0, j1 - j0, k1, 1);
+        if (k1 < 4)
+            return fail(set_error(PDM1_ERR_ARGUMENT, "WENO-Z inflow extrapolation requires at least four z cells."));
+    }
+    {
+        int dev = 0, sms = 148;
+        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        int tiles = make_domain(0, 0, 0, p.nx, p.ny, p.nz, 1).ntiles;
+        cf.grid_ctas = std::max(1, std::min(tiles, 2 * sms));
+    }
     if (cudaMemcpy(pl->d_tables, blob.data(), blob.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(pl->d_ids, pl->h_ids.data(), N * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(pl->d_spatial, pl->h_spatial.data(), (size_t)p.nx * p.ny * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
@@ -1151,12 +1564,19 @@ static int march_impl(pdm1_plan *pl, double *U, double *dose, double *energies, 
         CUDA_TRY(cudaMemcpyAsync(pl->d_targets, tg.data(), tg.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
     size_t N = (size_t)p.nx * p.ny * p.nz;
     CUDA_TRY(cudaMemsetAsync(dose, 0, N * sizeof(double), stream));
+    if (p.moving_active_domain && !tg.empty())
+        CUDA_TRY(cudaMemsetAsync(snap_out, 0, tg.size() * 4 * N * sizeof(double), stream));
     (void)cudaGetLastError();   // start from a clean launch-error state
-    init_kernel<<<1, 32, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, energies, E0, 1);
-    cfl_kernel<<<cell_blocks(p), NT, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, U);
+    init_kernel<<<1, 32, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, energies, E0, U, 0);
+    if (p.moving_active_domain) {
+        CUDA_TRY(cudaMemsetAsync(pl->d_slab, 0, (size_t)(p.nx + p.ny + p.nz) * sizeof(unsigned long long), stream));
+        box_init_kernel<<<cell_blocks(p), NT, 0, stream>>>(pl->d_cf, pl->d_st, U);
+    } else {
+        cfl_kernel<<<cell_blocks(p), NT, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, 0);
+    }
     CUDA_TRY(cudaGetLastError());
     int launches = 2;
-    StageArgs a = make_args(pl, U, dose, nullptr, snap_out);
+    StageArgs a = make_args(pl, dose, nullptr, snap_out);
     // capture a chunk of steps into a graph; replay until the device says done
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -1198,6 +1618,12 @@ static int march_impl(pdm1_plan *pl, double *U, double *dose, double *energies, 
     }
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
+    if (p.moving_active_domain) {
+        embed_kernel<<<cell_blocks(p), NT, 0, stream>>>(pl->d_cf, pl->d_st, U);
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        ++launches;
+    }
     rc = device_error_status(*pl->h_st);
     if (info) {
         info->n_steps = pl->h_st->step;
@@ -1232,12 +1658,20 @@ int pdm1_spatial_operator(pdm1_plan *pl, const double *U, double energy, const d
     (void)cudaGetLastError();
     if (!pl || !U || !rhs) return set_error(PDM1_ERR_ARGUMENT, "NULL argument");
     cudaStream_t stream = (cudaStream_t)stream_;
-    StageArgs a = make_args(pl, const_cast<double *>(U), nullptr, nullptr, nullptr);
+    {
+        MarchState st{};
+        st.dom = make_domain(0, 0, 0, pl->p.nx, pl->p.ny, pl->p.nz, 1);
+        st.prev = st.dom;
+        st.Ua = const_cast<double *>(U);
+        st.Uprev = st.Ua;
+        CUDA_TRY(cudaMemcpyAsync(pl->d_st, &st, sizeof st, cudaMemcpyHostToDevice, stream));
+    }
+    StageArgs a = make_args(pl, nullptr, nullptr, nullptr);
     a.rhs_out = rhs;
     a.bc_plane = bc;
     double de = energy - pl->p.beam_energy, s = pl->p.energy_spread;
     a.rhs_energy_density = dd_exp(-(de * de) / (2.0 * (s * s))) / (std::sqrt(2.0 * 3.141592653589793) * s);
-    stage_kernel<MODE_RHS><<<n_tiles(pl->p), NT, kStageSmem, stream>>>(a);
+    stage_kernel<MODE_RHS><<<pl->cf.grid_ctas, NT, kStageSmem, stream>>>(a);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(stream));
     return PDM1_OK;
@@ -1249,8 +1683,8 @@ int pdm1_energy_step(pdm1_plan *pl, const double *U, double energy, double *dE_o
     cudaStream_t stream = (cudaStream_t)stream_;
     int rc = check_energy_range(pl, energy, energy);
     if (rc) return rc;
-    init_kernel<<<1, 32, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, nullptr, energy, 1);
-    cfl_kernel<<<cell_blocks(pl->p), NT, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, U);
+    init_kernel<<<1, 32, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, nullptr, energy, const_cast<double *>(U), 1);
+    cfl_kernel<<<cell_blocks(pl->p), NT, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, 0);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(pl->h_st, pl->d_st, sizeof(MarchState), cudaMemcpyDeviceToHost, stream));
     CUDA_TRY(cudaStreamSynchronize(stream));
@@ -1274,12 +1708,16 @@ int pdm1_advance(pdm1_plan *pl, double *U, double energy, double dE, double *ede
     pl->cf.max_steps = 1;
     pl->cf.step_limit = -1;
     CUDA_TRY(cudaMemcpyAsync(pl->d_cf, &pl->cf, sizeof(ConfigDev), cudaMemcpyHostToDevice, stream));
-    init_kernel<<<1, 32, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, nullptr, energy, 1);
+    init_kernel<<<1, 32, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, nullptr, energy, U, 1);
     MarchState st{};
     st.E = energy;
     st.forced_dE = dE;
+    st.dom = make_domain(0, 0, 0, pl->p.nx, pl->p.ny, pl->p.nz, 1);
+    st.prev = st.dom;
+    st.Ua = U;
+    st.Uprev = U;
     CUDA_TRY(cudaMemcpyAsync(pl->d_st, &st, sizeof st, cudaMemcpyHostToDevice, stream));
-    StageArgs a = make_args(pl, U, nullptr, edep, nullptr);
+    StageArgs a = make_args(pl, nullptr, edep, nullptr);
     launch_step(pl, a, stream);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(pl->h_st, pl->d_st, sizeof(MarchState), cudaMemcpyDeviceToHost, stream));
@@ -1404,8 +1842,7 @@ TableView table_meta(const pdm1_table &t) {
 }
 
 void launch_step_plain(const pdm1_problem &p, ConfigDev *d_cf, Coeffs *d_co, MarchState *d_st,
-                       const StageArgs &a, double *energies, cudaStream_t stream) {
-    int tiles = n_tiles(p);
+                       const StageArgs &a, double *energies, int tiles, cudaStream_t stream) {
     prologue_kernel<<<1, 256, 0, stream>>>(d_cf, d_co, d_st, energies);
     if (p.energy_scheme == PDM1_SCHEME_FORWARD_EULER) {
         stage_kernel<MODE_EULER><<<tiles, NT, kStageSmem, stream>>>(a);
@@ -1427,6 +1864,8 @@ extern "C" int pdm1_march_noalloc(const pdm1_problem *problem, double *U, double
     int rc = validate_problem(problem);
     if (rc) return rc;
     const pdm1_problem &p = *problem;
+    if (p.moving_active_domain)
+        return set_error(PDM1_ERR_UNSUPPORTED, "pdm1_march_noalloc: the moving active box needs a plan");
     const size_t N = (size_t)p.nx * p.ny * p.nz;
 
     // layout of the scratch array
@@ -1515,6 +1954,11 @@ extern "C" int pdm1_march_noalloc(const pdm1_problem *problem, double *U, double
     cf.step_limit = -1;
     cf.n_targets = 0;
     cf.targets = nullptr;
+    {
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cf.grid_ctas = std::max(1, std::min(make_domain(0, 0, 0, p.nx, p.ny, p.nz, 1).ntiles, 2 * sms));
+    }
     cf.ids = reinterpret_cast<const int32_t *>(base + o_ids);
     cf.spatial = reinterpret_cast<const double *>(base + o_sp);
     for (int m = 0; m < p.n_materials; ++m) {
@@ -1547,7 +1991,6 @@ extern "C" int pdm1_march_noalloc(const pdm1_problem *problem, double *U, double
     a.cf = d_cf;
     a.co = d_co;
     a.st = d_st;
-    a.U = U;
     a.U1 = reinterpret_cast<double *>(base + o_U1);
     a.U2 = reinterpret_cast<double *>(base + o_U2);
     a.V = reinterpret_cast<double *>(base + o_V);
@@ -1555,14 +1998,14 @@ extern "C" int pdm1_march_noalloc(const pdm1_problem *problem, double *U, double
     a.dose = dose;
 
     (void)cudaGetLastError();
-    init_kernel<<<1, 32, 0, stream>>>(d_cf, d_co, d_st, energies, E0, 1);
-    cfl_kernel<<<cell_blocks(p), NT, 0, stream>>>(d_cf, d_co, d_st, U);
+    init_kernel<<<1, 32, 0, stream>>>(d_cf, d_co, d_st, energies, E0, U, 1);
+    cfl_kernel<<<cell_blocks(p), NT, 0, stream>>>(d_cf, d_co, d_st, 0);
     CUDA_TRY(cudaGetLastError());
     int launches = 2 + 3 * p.n_materials, chunks = 0;
     const int per_step = p.energy_scheme == PDM1_SCHEME_FORWARD_EULER ? 3 : 4;
     MarchState hs{};
     for (;;) {
-        for (int s = 0; s < kStepsPerGraph; ++s) launch_step_plain(p, d_cf, d_co, d_st, a, energies, stream);
+        for (int s = 0; s < kStepsPerGraph; ++s) launch_step_plain(p, d_cf, d_co, d_st, a, energies, cf.grid_ctas, stream);
         CUDA_TRY(cudaGetLastError());
         launches += kStepsPerGraph * per_step;
         ++chunks;
