@@ -204,25 +204,37 @@ def run_reference(args, cfg, desc, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def accelerated_config(cfg):
+    """The accelerated form: moving active box + FP32 stencil / FP64 dose."""
+    from dataclasses import replace
+    from proton_dose_m1_b200 import Accel, SolverConfig
+    from proton_dose_m1_b200.enums import Precision
+    return SolverConfig(geometry=cfg.geometry, beam=cfg.beam, physics=cfg.physics,
+                        numerics=replace(cfg.numerics, moving_active_domain=True),
+                        accel=Accel(precision=Precision.FP32_FP64))
+
+
 def run_ours(args, cfg, desc, rank, world, local_rank):
     import torch
     import torch.distributed as dist
+    from proton_dose_m1_b200 import metrics
     from proton_dose_m1_b200.numerics.energy import M1Plan, energy_march
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     mm, grid, inflow = problem(cfg)
-    plan = M1Plan(cfg, mm, grid, inflow)
+    run_cfg = accelerated_config(cfg) if args.method == "accelerated" else cfg
+    precision = run_cfg.accel.precision.name
+    plan = M1Plan(run_cfg, mm, grid, inflow)
     shape = grid.shape
-    N = int(np.prod(shape))
     stream = torch.cuda.Stream(device=dev)
     U = torch.zeros((4, *shape), dtype=torch.float64, device=dev)
     dose = torch.empty(shape, dtype=torch.float64, device=dev)
     energies = torch.empty(200_001, dtype=torch.float64, device=dev)
 
-    def one_spot():
+    def one_spot(p=plan, d=dose):
         U.zero_()
-        return plan.march_device(U, dose, energies)
+        return p.march_device(U, d, energies)
 
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
@@ -231,7 +243,7 @@ def run_ours(args, cfg, desc, rank, world, local_rank):
         if world > 1:
             dist.barrier()
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        stage_ms, stage_launches, launches, n_steps = 0.0, 0, 0, 0
+        stage_ms, stage_launches, launches, n_steps, cell_steps = 0.0, 0, 0, 0, 0.0
         with ClockSampler(local_rank) as clocks:
             start.record(stream)
             for _ in range(args.steps):
@@ -239,18 +251,44 @@ def run_ours(args, cfg, desc, rank, world, local_rank):
                 info = plan.last_info
                 stage_ms += info.stage_ms
                 stage_launches += info.stage_launches
+                cell_steps += info.cell_steps
                 launches += info.kernel_launches + 1   # + the zero fill
                 n_steps = n
             end.record(stream)
             torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
-    ms = start.elapsed_time(end)
-    if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * args.steps / (ms / 1e3)
+        ms = start.elapsed_time(end)
+        if world > 1:
+            t = torch.tensor([ms], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        value = world * args.steps / (ms / 1e3)
+
+        # gate: the same spot on the plain FP64 full-domain path (untimed here)
+        gate = None
+        plain_spots_per_s = None
+        if args.method == "accelerated" and rank == 0:
+            plain = M1Plan(cfg, mm, grid, inflow)
+            dose_plain = torch.empty_like(dose)
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s0.record(stream)
+            one_spot(plain, dose_plain)
+            s1.record(stream)
+            torch.cuda.synchronize()
+            plain_spots_per_s = 1e3 / s0.elapsed_time(s1)
+            one_spot()
+            torch.cuda.synchronize()
+            score = metrics.compare(dose, dose_plain, grid)
+            gate = {"vs": "plain FP64 GPU path (full domain)",
+                    "gamma_1pct_1mm_pass_percent": score["gamma_1pct_1mm_pass_percent"],
+                    "max_dose_relative_difference": score["maximum_dose_relative_difference"],
+                    "max_abs_difference_over_max": score["max_abs_difference_over_max"],
+                    "r80_difference_mm": score["range"]["r80_difference_mm"],
+                    "dfw_difference_mm": score["range"]["dfw_difference_mm"],
+                    "passed": bool(score["gamma_1pct_1mm_pass_percent"] >= 99.5
+                                   and abs(score["maximum_dose_relative_difference"]) <= 0.005)}
+            plain.close()
 
     # end to end through the public API with host buffers
     U_host = np.zeros((4, *shape))
@@ -258,36 +296,46 @@ def run_ours(args, cfg, desc, rank, world, local_rank):
     for _ in range(max(1, args.steps)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        Uo, doseo, Eo, _ = energy_march(U_host, mm, grid, inflow, cfg, np)
+        Uo, doseo, Eo, _ = energy_march(U_host, mm, grid, inflow, run_cfg, np)
         torch.cuda.synchronize()
         e2e_times.append(time.perf_counter() - t0)
     e2e_s = sum(e2e_times) / len(e2e_times)
     h2d = U_host.nbytes + mm.ids.nbytes + inflow.spatial.nbytes
-    d2h = Uo.nbytes + doseo.nbytes + Eo.nbytes
+    d2h = (Uo.nbytes if Uo is not None else 0) + doseo.nbytes + Eo.nbytes
 
     if rank != 0:
         return
     peak, peak_kind = measured_peaks()
     avg_launch_ms = stage_ms / max(stage_launches, 1)
-    precision = "FP64"
-    alg_bytes = N * ALG_BYTES_PER_CELL_STEP[precision] / 3.0
-    achieved = alg_bytes / (avg_launch_ms / 1e3) / 1e9
+    # algorithmic bytes of the stage launches: cells marched x bytes per cell-step,
+    # a third per stage launch (cell_steps already sums the domain over steps)
+    alg_total = cell_steps * ALG_BYTES_PER_CELL_STEP[precision]
+    achieved = alg_total / (stage_ms / 1e3) / 1e9 if stage_ms > 0 else 0.0
     traffic = None
     prof = ROOT / "profiles" / "stage_kernel_traffic.json"
     if prof.exists():
-        traffic = json.loads(prof.read_text()).get(args.workload)
+        traffic = json.loads(prof.read_text()).get(f"{args.workload}/{args.method}")
     line = {
         "metric": METRIC, "value": value, "unit": "spots/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded phantom, no dataset)",
-        "config": {"workload": args.workload, "description": desc, "method": "plain FP64, full domain",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 stencil / f64 dose" if precision == "FP32_FP64" else "f64",
+        "data": "synthetic (analytic phantom, no dataset)",
+        "config": {"workload": args.workload, "description": desc,
+                   "method": ("moving active box + FP32 stencil / FP64 dose" if args.method == "accelerated"
+                              else "plain FP64, full domain"),
                    "energy_steps_per_spot": n_steps,
-                   "l2": "working set (U, two stage states, V, dose: ~350 MB) exceeds the 126 MB L2"},
+                   "cells_marched_per_spot": cell_steps / max(args.steps, 1),
+                   "plain_fp64_spots_per_s": plain_spots_per_s,
+                   "l2": "working set (state, two stage states, V, dose: ~350 MB) exceeds the 126 MB L2"},
+        "gate": gate,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
-                     "kernel": "stage_kernel (A/B/C)", "avg_launch_ms": avg_launch_ms,
-                     "algorithmic_bytes_per_launch": alg_bytes, "peak_source": peak_kind},
+                     "kernel": f"stage_kernel<{'float' if precision == 'FP32_FP64' else 'double'}> (A/B/C)",
+                     "avg_launch_ms": avg_launch_ms,
+                     "algorithmic_bytes_per_launch": alg_total / max(stage_launches, 1),
+                     "algorithmic_bytes_per_cell_step": ALG_BYTES_PER_CELL_STEP[precision],
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"},
         "e2e": {"value": 1.0 / e2e_s, "unit": "spots/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": launches,
@@ -306,6 +354,8 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", default="slab80")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--method", choices=("accelerated", "plain"), default="accelerated",
+                    help="accelerated: moving box + FP32 stencil/FP64 dose; plain: FP64 full domain")
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="only run the first K energy steps of one spot (for ncu captures) and exit")
     args = ap.parse_args()
@@ -319,7 +369,8 @@ def main():
     if args.profile_steps > 0:
         from proton_dose_m1_b200.numerics.energy import M1Plan
         import torch
-        plan = M1Plan(cfg, *problem(cfg))
+        run_cfg = accelerated_config(cfg) if args.method == "accelerated" else cfg
+        plan = M1Plan(run_cfg, *problem(cfg))
         U, dose, E = plan.march_steps(args.profile_steps)
         torch.cuda.synchronize()
         print(json.dumps({"profile_steps": len(E) - 1, "energy": float(E[-1]),

@@ -94,6 +94,7 @@ typedef struct {
     int kernel_launches;      /* kernels this library launched for the march */
     int stage_launches;       /* launches of the fused stage kernels */
     double stage_ms;          /* their summed device time (CUDA events on the march stream) */
+    double cell_steps;        /* sum over energy steps of the cells marched */
 } pdm1_march_info;
 
 /* Plan: copies the problem to the device and allocates the workspace.
@@ -164,6 +165,19 @@ int pdm1_eigen_batch(const double *u4, int axis, double *lo_hi, int n, pdm1_stre
 int pdm1_hll_batch(const double *left4, const double *right4, int axis, int wave_speeds,
                    double *flux4, int n, pdm1_stream_t stream);
 int pdm1_exp_batch(const double *x, double *y, int n, pdm1_stream_t stream);
+
+/* Global 3-D gamma index of `dose_eval` against `dose_ref` (device, same
+ * (nx,ny,nz) grid, spacings in mm) as the reference scores doses
+ * (proton_solver/metrics.py:542-606, pymedphys.gamma with interp_fraction,
+ * max_gamma, global normalisation, lower dose cutoff in percent of it, and
+ * skip-once-passed).  gamma_out (device, nx*ny*nz) receives gamma, NaN below
+ * the cutoff; *pass_rate_out (host) the percentage of evaluated voxels with
+ * gamma <= 1.  Synchronises `stream`. */
+int pdm1_gamma(const double *dose_ref, const double *dose_eval, int nx, int ny, int nz,
+               double dx_mm, double dy_mm, double dz_mm, double dose_percent,
+               double distance_mm, double lower_cutoff_percent, int interp_fraction,
+               double max_gamma, double global_normalisation, double *gamma_out,
+               double *pass_rate_out, pdm1_stream_t stream);
 
 const char *pdm1_last_error(void);
 const char *pdm1_version(void);

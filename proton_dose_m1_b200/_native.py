@@ -47,7 +47,8 @@ class Problem(C.Structure):
 class MarchInfo(C.Structure):
     _fields_ = [("n_steps", C.c_int), ("n_snapshots", C.c_int), ("final_state_valid", C.c_int),
                 ("graph_replays", C.c_int), ("kernel_launches", C.c_int),
-                ("stage_launches", C.c_int), ("stage_ms", C.c_double)]
+                ("stage_launches", C.c_int), ("stage_ms", C.c_double),
+                ("cell_steps", C.c_double)]
 
 
 _lib = None
@@ -81,6 +82,9 @@ def lib():
         L.pdm1_eigen_batch.argtypes = [_vp, C.c_int, _vp, C.c_int, _vp]
         L.pdm1_hll_batch.argtypes = [_vp, _vp, C.c_int, C.c_int, _vp, C.c_int, _vp]
         L.pdm1_exp_batch.argtypes = [_vp, _vp, C.c_int, _vp]
+        L.pdm1_gamma.argtypes = [_vp, _vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                 C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
+                                 C.c_double, C.c_double, _vp, _dp, _vp]
         _lib = L
     return _lib
 
@@ -102,5 +106,5 @@ EXPORTED_SYMBOLS = (
     "pdm1_march_steps",
     "pdm1_spatial_operator", "pdm1_energy_step", "pdm1_advance", "pdm1_coefficients",
     "pdm1_weno_batch", "pdm1_project_batch", "pdm1_eigen_batch", "pdm1_hll_batch",
-    "pdm1_exp_batch", "pdm1_last_error", "pdm1_version",
+    "pdm1_exp_batch", "pdm1_gamma", "pdm1_last_error", "pdm1_version",
 )

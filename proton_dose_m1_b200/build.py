@@ -14,16 +14,22 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 LIB = PKG / "libpdm1.so"
-SOURCES = [PKG / "csrc" / "pdm1_march.cu"]
-HEADERS = [PKG / "csrc" / "pdm1_math.cuh", ROOT / "include" / "pdm1.h"]
-
-NVCC_FLAGS = [
-    "-gencode", "arch=compute_100a,code=sm_100a",
-    "-O3", "-lineinfo", "-std=c++17", "--fmad=false",
-    "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
-    "-shared",
-]
-
+CSRC = PKG / "csrc"
+BUILD = PKG / "_build"
+HEADERS = [CSRC / "pdm1_math.cuh", CSRC / "pdm1_device.cuh", CSRC / "pdm1_stage.cuh",
+           ROOT / "include" / "pdm1.h"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off"]
+# translation unit -> its own precision flags
+UNITS = {
+    # the FP64 march: every product and sum separately rounded, IEEE div/sqrt
+    CSRC / "pdm1_march.cu": ["--fmad=false"],
+    # the single-precision stencil: fast math, FMA contraction
+    CSRC / "pdm1_stage_fp32.cu": ["--use_fast_math"],
+    # dose scoring (gamma index)
+    CSRC / "pdm1_gamma.cu": [],
+}
+SOURCES = list(UNITS)
 
 def nvcc() -> str:
     for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
@@ -41,14 +47,24 @@ def stale() -> bool:
 
 def build(force: bool = False, verbose: bool = False) -> Path:
     if force or stale():
-        cmd = [nvcc(), *NVCC_FLAGS, "-o", str(LIB), *map(str, SOURCES)]
-        if verbose:
-            cmd.insert(1, "-Xptxas=-v")
-        r = subprocess.run(cmd, capture_output=True, text=True)
+        BUILD.mkdir(exist_ok=True)
+        objs = []
+        log = []
+        for src, flags in UNITS.items():
+            obj = BUILD / (src.stem + ".o")
+            cmd = [nvcc(), *ARCH, *COMMON, *flags, "-c", "-o", str(obj), str(src)]
+            if verbose:
+                cmd.insert(1, "-Xptxas=-v")
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"nvcc failed on {src.name}:\n{r.stdout}\n{r.stderr}")
+            log.append(r.stderr)
+            objs.append(str(obj))
+        r = subprocess.run([nvcc(), *ARCH, "-shared", "-o", str(LIB), *objs], capture_output=True, text=True)
         if r.returncode != 0:
-            raise RuntimeError(f"nvcc failed:\n{r.stdout}\n{r.stderr}")
+            raise RuntimeError(f"nvcc link failed:\n{r.stdout}\n{r.stderr}")
         if verbose:
-            print(r.stderr)
+            print("\n".join(log))
     return LIB
 
 

@@ -1,0 +1,334 @@
+// pdm1_device.cuh -- device-side data of a plan and helpers shared by the
+// double-precision march (pdm1_march.cu) and the single-precision stencil
+// kernels (pdm1_stage_fp32.cu).
+#pragma once
+
+#include "../../include/pdm1.h"
+#include "pdm1_math.cuh"
+
+#include <cuda_runtime.h>
+
+namespace pdm1 {
+
+constexpr int kMaxMat = 16;
+
+enum { ERR_DEV_RANGE = 1, ERR_DEV_MAXSTEPS = 2, ERR_DEV_NONFINITE = 4 };
+// ---------------------------------------------------------------------------
+// Device-side plan data
+// ---------------------------------------------------------------------------
+struct MatDev {
+    TableView sp, tr, nuc;
+    double density, X0;
+};
+
+// A rectangular domain of the full grid: the whole grid, or the moving active box
+// (numerics/moving_active_domain.py), with its tile decomposition.
+struct DomainDev {
+    int i0, j0, k0;          // origin in the full grid
+    int nx, ny, nz;          // extent
+    int tiles_y, tiles_z, ntiles;
+    int inflow;              // the domain's z-min face is the beam entrance (k0 == 0)
+};
+
+struct ConfigDev {
+    int nx, ny, nz;
+    double dx, dy, dz;
+    int nm;
+    int scattering, nuclear, interp, scheme, unit_speeds;
+    int use_if;          // integrating factors active (IF_SSPRK3 with sources)
+    int strang;          // Strang-split sources around an SSPRK3 / Euler step
+    double cfl, max_dE, Emin, E_beam, sigma_E, rf;
+    int max_steps;
+    int step_limit;      // >= 0: stop (without error) after this many steps
+    int n_targets;
+    const int32_t *ids;
+    const double *spatial;
+    const double *targets;      // descending
+    // moving active box
+    int moving, vacuum_aware, guard;
+    double tol;                 // exp(-sigma_trunc^2 / 2)
+    DomainDev init_box;         // moving_active_domain.py:35-60
+    double *bufA, *bufB;        // compact-state ping-pong
+    unsigned long long *slab;   // max phi per x | y | z slab of the current box (double bits)
+    unsigned char *active;      // vacuum-aware activity mask on the current box
+    int grid_ctas;              // persistent grid of the stage kernels
+    MatDev mats[kMaxMat];
+};
+
+struct Coeffs {
+    double E, dE, E_next;
+    int active;
+    int snap_slot;
+    double S0[kMaxMat], S1[kMaxMat], S2[kMaxMat];
+    double c1p[kMaxMat], c1c[kMaxMat], c1ip[kMaxMat], c1ic[kMaxMat];
+    double c2p[kMaxMat], c2c[kMaxMat], c2ip[kMaxMat], c2ic[kMaxMat];
+    double Sb[4][kMaxMat];                  // S at E, E-dE/3, E-2dE/3, E-dE
+    double fip[4][kMaxMat], fic[4][kMaxMat];   // inverse factors at those depths
+    double ed[4];                           // spectrum at those energies
+    double ed_next;                         // spectrum at E_next (CFL inflow)
+    double hn[kMaxMat], hs[kMaxMat];        // Strang half-step factors
+    double S_cfl[kMaxMat];                  // moving box: S at the step's start energy
+    double ed_cfl;                          // moving box: spectrum at that energy
+};
+
+struct MarchState {
+    double E;
+    unsigned long long inv_bits;   // CFL max (non-negative double bits)
+    double forced_dE;              // > 0: one step with this dE (pdm1_advance)
+    int step, done, ti, taken, error;
+    DomainDev dom;                 // the domain the stage kernels work on
+    DomainDev prev;                // moving box before this step's rebox
+    double *Ua;                    // state on `dom`
+    double *Uprev;                 // state on `prev`
+    int reboxed;
+    unsigned long long newmax_bits;   // max phi over the new box (vacuum-aware CFL)
+    double pin_max;                // max inflow phi over the new box
+    double cell_steps;             // sum over steps of the cells marched (domain volume)
+};
+
+__host__ __device__ inline DomainDev make_domain(int i0, int j0, int k0, int nx, int ny, int nz, int inflow);
+
+
+// ---------------------------------------------------------------------------
+// Material coefficients (device), mirroring physics/*.py
+// ---------------------------------------------------------------------------
+__device__ inline bool stopping_power_dev(const MatDev &m, double E, double &out) {
+    if (!clip_energy(m.sp, E)) return false;
+    if (E == m.sp.E[m.sp.n - 1]) { out = m.sp.v[m.sp.n - 1]; return true; }
+    out = pchip_eval(m.sp, E);
+    return true;
+}
+
+__device__ inline bool transport_dev(const ConfigDev &cf, const MatDev &m, double E, double &out) {
+    if (cf.scattering == PDM1_SCATTERING_OFF) { out = 0.0; return true; }
+    if (cf.scattering == PDM1_SCATTERING_ROSSI) {
+        double e = E > 1.0e-8 ? E : 1.0e-8;
+        double M = kProtonRestMev;
+        double pv = e * (e + 2.0 * M) / (e + M);
+        double r = kRossiEsMev / pv;
+        out = r * r / m.X0;
+        return true;
+    }
+    if (!clip_energy(m.tr, E)) return false;
+    out = cf.interp == PDM1_INTERP_LINEAR ? linear_eval(m.tr, E) : pchip_eval(m.tr, E);
+    return true;
+}
+
+__device__ inline bool nuclear_dev(const ConfigDev &cf, const MatDev &m, double E, double &out) {
+    if (!clip_energy(m.nuc, E)) return false;
+    out = cf.interp == PDM1_INTERP_LINEAR ? linear_eval(m.nuc, E) : pchip_eval(m.nuc, E);
+    return true;
+}
+
+// numerics/boundary.py:82-114 spectrum factor
+__device__ __forceinline__ double energy_density(const ConfigDev &cf, double E) {
+    double de = E - cf.E_beam;
+    double s = cf.sigma_E;
+    return dd_exp(-(de * de) / (2.0 * (s * s))) / (sqrt(2.0 * 3.141592653589793) * s);
+}
+
+__device__ __forceinline__ void source_factor(double ts, double tn, bool inverse, double &fp, double &fc) {
+    double sign = inverse ? 1.0 : -1.0;
+    double a = tn < kExpClamp ? tn : kExpClamp;
+    double tsum = tn + ts;
+    double b = tsum < kExpClamp ? tsum : kExpClamp;
+    fp = dd_exp(sign * a);
+    fc = dd_exp(sign * b);
+}
+
+// ---------------------------------------------------------------------------
+// The fused stage kernel
+// ---------------------------------------------------------------------------
+constexpr int TX = 4, TY = 8, TZ = 8;
+constexpr int NT = TX * TY * TZ;
+constexpr int NFX = (TX + 1) * TY * TZ;
+constexpr int NFY = TX * (TY + 1) * TZ;
+constexpr int NFZ = TX * TY * (TZ + 1);
+constexpr int NF = NFX + NFY + NFZ;
+constexpr int SX = (TX + 6) * TY * TZ;   // x-arm including the core
+constexpr int SY = TX * 6 * TZ;          // y halo
+constexpr int SZ = TX * TY * 6;          // z halo
+template <typename T>
+constexpr size_t stage_smem_bytes() { return sizeof(T) * 4 * (SX + SY + SZ + NF); }
+
+__host__ __device__ inline DomainDev make_domain(int i0, int j0, int k0, int nx, int ny, int nz, int inflow) {
+    DomainDev d;
+    d.i0 = i0; d.j0 = j0; d.k0 = k0;
+    d.nx = nx; d.ny = ny; d.nz = nz;
+    d.tiles_y = (ny + TY - 1) / TY;
+    d.tiles_z = (nz + TZ - 1) / TZ;
+    d.ntiles = ((nx + TX - 1) / TX) * d.tiles_y * d.tiles_z;
+    d.inflow = inflow;
+    return d;
+}
+
+enum StageMode { MODE_A = 0, MODE_B = 1, MODE_C = 2, MODE_EULER = 3, MODE_RHS = 4 };
+
+struct StageArgs {
+    const ConfigDev *cf;
+    const Coeffs *co;
+    MarchState *st;
+    double *U1;         // stage states (on the current domain)
+    double *U2;
+    double *V;          // marched variable of stage 1 / 2
+    double *qpart;      // (q0 + q1)/6 quadrature part
+    double *dose;       // accumulated dose (full grid), or NULL
+    double *edep;       // when non-NULL: energy deposition written instead of dose
+    double *snap;       // snapshot buffer base (slot * 4N, full grid)
+    double *rhs_out;    // MODE_RHS output
+    const double *bc_plane;   // MODE_RHS: explicit z-min boundary state (4,nx,ny)
+    double rhs_energy_density;
+};
+
+template <typename T>
+struct SmemT {
+    T *X, *Y, *Z, *F;
+};
+
+template <typename T>
+__device__ __forceinline__ T sval(const SmemT<T> &s, int c, int i, int j, int k) {
+    if (j < 0) return s.Y[((c * TX + i) * 6 + (j + 3)) * TZ + k];
+    if (j >= TY) return s.Y[((c * TX + i) * 6 + (j - TY + 3)) * TZ + k];
+    if (k < 0) return s.Z[((c * TX + i) * TY + j) * 6 + (k + 3)];
+    if (k >= TZ) return s.Z[((c * TX + i) * TY + j) * 6 + (k - TZ + 3)];
+    return s.X[((c * (TX + 6) + (i + 3)) * TY + j) * TZ + k];
+}
+
+__device__ __forceinline__ size_t global_cell(const ConfigDev &cf, const DomainDev &d, int li, int lj, int lk) {
+    return ((size_t)(d.i0 + li) * cf.ny + (d.j0 + lj)) * cf.nz + (d.k0 + lk);
+}
+
+// Stencil source value at a domain cell; indices outside the domain are
+// clamped (zero-gradient ghosts, numerics/boundary.py:327-397).
+template <int MODE>
+__device__ __forceinline__ void load_cell(const ConfigDev &cf, const Coeffs &co, const DomainDev &d,
+                                          const double *src, int li, int lj, int lk, double out[4]) {
+    const int nx = d.nx, ny = d.ny, nz = d.nz;
+    const size_t N = (size_t)nx * ny * nz;
+    li = li < 0 ? 0 : (li >= nx ? nx - 1 : li);
+    lj = lj < 0 ? 0 : (lj >= ny ? ny - 1 : lj);
+    lk = lk >= nz ? nz - 1 : lk;
+    size_t o = ((size_t)li * ny + lj) * nz + lk;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) out[c] = src[c * N + o];
+    if ((MODE == MODE_A || MODE == MODE_EULER) && cf.strang) {
+        int m = cf.ids[global_cell(cf, d, li, lj, lk)];
+        double hn = co.hn[m], hs = co.hs[m];
+        if (cf.nuclear)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) out[c] *= hn;
+        if (cf.scattering != PDM1_SCATTERING_OFF)
+#pragma unroll
+            for (int c = 1; c < 4; ++c) out[c] *= hs;
+    }
+}
+
+// z-min boundary value of component c at domain column (li, lj) for this stage.
+// A moving box away from the entrance has zero inflow (moving_active_domain.py:85-95).
+template <int MODE>
+__device__ __forceinline__ double boundary_value(const StageArgs &a, const ConfigDev &cf, const Coeffs &co,
+                                                 const DomainDev &d, int c, int li, int lj) {
+    if (MODE == MODE_RHS && a.bc_plane)
+        return a.bc_plane[((size_t)c * d.nx + li) * d.ny + lj];
+    if (!d.inflow || c == 1 || c == 2) return 0.0;
+    const int gi = d.i0 + li, gj = d.j0 + lj;
+    double sp = cf.spatial[(size_t)gi * cf.ny + gj];
+    if (MODE == MODE_A || MODE == MODE_EULER || MODE == MODE_RHS) {
+        double ed = MODE == MODE_RHS ? a.rhs_energy_density : co.ed[0];
+        double phi = sp * ed;
+        return c == 0 ? phi : cf.rf * phi;
+    }
+    // RK-consistent stage traces, numerics/energy.py:348-455 (107-231 without sources)
+    int m = cf.ids[((size_t)gi * cf.ny + gj) * cf.nz];
+    double V[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        double phi = sp * co.ed[q];
+        double x = c == 0 ? phi : cf.rf * phi;
+        double B = co.Sb[q][m] * x;
+        if (q > 0 && cf.use_if) B *= (c == 0 ? co.fip[q][m] : co.fic[q][m]);
+        V[q] = B;
+    }
+    if (MODE == MODE_B) {
+        double vs1 = 0.5 * (-9.0 * V[0] + 18.0 * V[1] - 9.0 * V[2] + 2.0 * V[3]);
+        if (cf.use_if) vs1 *= (c == 0 ? co.c1p[m] : co.c1c[m]);
+        return vs1 / co.S1[m];
+    }
+    double vs2 = 0.25 * (11.0 * V[0] - 27.0 * V[1] + 27.0 * V[2] - 7.0 * V[3]);
+    if (cf.use_if) vs2 *= (c == 0 ? co.c2p[m] : co.c2c[m]);
+    return vs2 / co.S2[m];
+}
+
+// One cell's CFL term (numerics/energy.py:539-660): sum over axes of a/(S d).
+// `entrance`: the cell is on the domain's z-min layer, where the inflow state
+// (zero for a box away from the entrance) joins the z speeds.
+__device__ __forceinline__ double cfl_term(const ConfigDev &cf, const double u[4], double s, bool entrance,
+                                           double phi_in, const bool use[3]) {
+    double a0, a1, a2;
+    if (cf.unit_speeds) {
+        a0 = a1 = a2 = 1.0;
+    } else {
+        a0 = max_abs_speed(u[0], u[1], u[2], u[3], 0);
+        a1 = max_abs_speed(u[0], u[1], u[2], u[3], 1);
+        a2 = max_abs_speed(u[0], u[1], u[2], u[3], 2);
+        if (entrance) {
+            double jz = cf.rf * phi_in;
+            double ain = max_abs_speed(phi_in, 0.0, 0.0, jz, 2);
+            if (ain > a2) a2 = ain;
+        }
+    }
+    if (!use[0]) a0 = 0.0;
+    if (!use[1]) a1 = 0.0;
+    if (!use[2]) a2 = 0.0;
+    return a0 / (s * cf.dx) + a1 / (s * cf.dy) + a2 / (s * cf.dz);
+}
+
+__device__ __forceinline__ void block_max_atomic(double v, unsigned long long *target) {
+    // v >= 0 or NaN; NaN never wins (fmax), like the oracle's comparison loop
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    __shared__ double wmax[NT / 32];
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) wmax[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        v = l < NT / 32 ? wmax[l] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (l == 0 && v > 0.0) atomicMax(target, (unsigned long long)__double_as_longlong(v));
+    }
+}
+
+__device__ __forceinline__ void atomic_max_double(unsigned long long *target, double v) {
+    if (v > 0.0) atomicMax(target, (unsigned long long)__double_as_longlong(v));
+}
+
+// Per-slab maxima of phi over one tile (moving box): cell values in `buf`
+// (TX*TY*TZ doubles, -1 for cells outside the box).
+__device__ __forceinline__ void tile_slab_max(const ConfigDev &cf, const DomainDev &d, const double *buf,
+                                              int i0, int j0, int k0) {
+    int t = threadIdx.x;
+    unsigned long long *sx = cf.slab, *sy = cf.slab + cf.nx, *sz = cf.slab + cf.nx + cf.ny;
+    if (t < TX) {
+        double m = 0.0;
+        for (int e = 0; e < TY * TZ; ++e) m = fmax(m, buf[t * TY * TZ + e]);
+        if (i0 + t < d.nx) atomic_max_double(&sx[i0 + t], m);
+    } else if (t < TX + TY) {
+        int j = t - TX;
+        double m = 0.0;
+        for (int i = 0; i < TX; ++i)
+            for (int k = 0; k < TZ; ++k) m = fmax(m, buf[(i * TY + j) * TZ + k]);
+        if (j0 + j < d.ny) atomic_max_double(&sy[j0 + j], m);
+    } else if (t < TX + TY + TZ) {
+        int k = t - TX - TY;
+        double m = 0.0;
+        for (int i = 0; i < TX; ++i)
+            for (int j = 0; j < TY; ++j) m = fmax(m, buf[(i * TY + j) * TZ + k]);
+        if (k0 + k < d.nz) atomic_max_double(&sz[k0 + k], m);
+    }
+}
+
+// Single-precision stencil kernels (pdm1_stage_fp32.cu, compiled with fast math).
+int stage_fp32_set_attributes();
+void launch_stage_fp32(int mode, int grid, const StageArgs &a, cudaStream_t stream);
+
+}  // namespace pdm1

@@ -17,6 +17,8 @@
 // into a CUDA graph and replayed until the device flags the march done.
 #include "../../include/pdm1.h"
 #include "pdm1_math.cuh"
+#include "pdm1_device.cuh"
+#include "pdm1_stage.cuh"
 
 #include <cuda_runtime.h>
 
@@ -32,7 +34,6 @@ using namespace pdm1;
 
 namespace {
 
-constexpr int kMaxMat = 16;
 constexpr int kStepsPerGraph = 32;
 
 // fixed-size message buffer: reporting an error allocates nothing
@@ -51,129 +52,6 @@ int set_error(int code, const std::string &msg) { return set_error(code, msg.c_s
         if (e_ != cudaSuccess)                                                            \
             return set_error(PDM1_ERR_CUDA, std::string(#expr ": ") + cudaGetErrorString(e_)); \
     } while (0)
-
-// ---------------------------------------------------------------------------
-// Device-side plan data
-// ---------------------------------------------------------------------------
-struct MatDev {
-    TableView sp, tr, nuc;
-    double density, X0;
-};
-
-// A rectangular domain of the full grid: the whole grid, or the moving active box
-// (numerics/moving_active_domain.py), with its tile decomposition.
-struct DomainDev {
-    int i0, j0, k0;          // origin in the full grid
-    int nx, ny, nz;          // extent
-    int tiles_y, tiles_z, ntiles;
-    int inflow;              // the domain's z-min face is the beam entrance (k0 == 0)
-};
-
-struct ConfigDev {
-    int nx, ny, nz;
-    double dx, dy, dz;
-    int nm;
-    int scattering, nuclear, interp, scheme, unit_speeds;
-    int use_if;          // integrating factors active (IF_SSPRK3 with sources)
-    int strang;          // Strang-split sources around an SSPRK3 / Euler step
-    double cfl, max_dE, Emin, E_beam, sigma_E, rf;
-    int max_steps;
-    int step_limit;      // >= 0: stop (without error) after this many steps
-    int n_targets;
-    const int32_t *ids;
-    const double *spatial;
-    const double *targets;      // descending
-    // moving active box
-    int moving, vacuum_aware, guard;
-    double tol;                 // exp(-sigma_trunc^2 / 2)
-    DomainDev init_box;         // moving_active_domain.py:35-60
-    double *bufA, *bufB;        // compact-state ping-pong
-    unsigned long long *slab;   // max phi per x | y | z slab of the current box (double bits)
-    unsigned char *active;      // vacuum-aware activity mask on the current box
-    int grid_ctas;              // persistent grid of the stage kernels
-    MatDev mats[kMaxMat];
-};
-
-struct Coeffs {
-    double E, dE, E_next;
-    int active;
-    int snap_slot;
-    double S0[kMaxMat], S1[kMaxMat], S2[kMaxMat];
-    double c1p[kMaxMat], c1c[kMaxMat], c1ip[kMaxMat], c1ic[kMaxMat];
-    double c2p[kMaxMat], c2c[kMaxMat], c2ip[kMaxMat], c2ic[kMaxMat];
-    double Sb[4][kMaxMat];                  // S at E, E-dE/3, E-2dE/3, E-dE
-    double fip[4][kMaxMat], fic[4][kMaxMat];   // inverse factors at those depths
-    double ed[4];                           // spectrum at those energies
-    double ed_next;                         // spectrum at E_next (CFL inflow)
-    double hn[kMaxMat], hs[kMaxMat];        // Strang half-step factors
-    double S_cfl[kMaxMat];                  // moving box: S at the step's start energy
-    double ed_cfl;                          // moving box: spectrum at that energy
-};
-
-struct MarchState {
-    double E;
-    unsigned long long inv_bits;   // CFL max (non-negative double bits)
-    double forced_dE;              // > 0: one step with this dE (pdm1_advance)
-    int step, done, ti, taken, error;
-    DomainDev dom;                 // the domain the stage kernels work on
-    DomainDev prev;                // moving box before this step's rebox
-    double *Ua;                    // state on `dom`
-    double *Uprev;                 // state on `prev`
-    int reboxed;
-    unsigned long long newmax_bits;   // max phi over the new box (vacuum-aware CFL)
-    double pin_max;                // max inflow phi over the new box
-};
-
-__host__ __device__ inline DomainDev make_domain(int i0, int j0, int k0, int nx, int ny, int nz, int inflow);
-
-enum { ERR_DEV_RANGE = 1, ERR_DEV_MAXSTEPS = 2, ERR_DEV_NONFINITE = 4 };
-
-// ---------------------------------------------------------------------------
-// Material coefficients (device), mirroring physics/*.py
-// ---------------------------------------------------------------------------
-__device__ bool stopping_power_dev(const MatDev &m, double E, double &out) {
-    if (!clip_energy(m.sp, E)) return false;
-    if (E == m.sp.E[m.sp.n - 1]) { out = m.sp.v[m.sp.n - 1]; return true; }
-    out = pchip_eval(m.sp, E);
-    return true;
-}
-
-__device__ bool transport_dev(const ConfigDev &cf, const MatDev &m, double E, double &out) {
-    if (cf.scattering == PDM1_SCATTERING_OFF) { out = 0.0; return true; }
-    if (cf.scattering == PDM1_SCATTERING_ROSSI) {
-        double e = E > 1.0e-8 ? E : 1.0e-8;
-        double M = kProtonRestMev;
-        double pv = e * (e + 2.0 * M) / (e + M);
-        double r = kRossiEsMev / pv;
-        out = r * r / m.X0;
-        return true;
-    }
-    if (!clip_energy(m.tr, E)) return false;
-    out = cf.interp == PDM1_INTERP_LINEAR ? linear_eval(m.tr, E) : pchip_eval(m.tr, E);
-    return true;
-}
-
-__device__ bool nuclear_dev(const ConfigDev &cf, const MatDev &m, double E, double &out) {
-    if (!clip_energy(m.nuc, E)) return false;
-    out = cf.interp == PDM1_INTERP_LINEAR ? linear_eval(m.nuc, E) : pchip_eval(m.nuc, E);
-    return true;
-}
-
-// numerics/boundary.py:82-114 spectrum factor
-__device__ __forceinline__ double energy_density(const ConfigDev &cf, double E) {
-    double de = E - cf.E_beam;
-    double s = cf.sigma_E;
-    return dd_exp(-(de * de) / (2.0 * (s * s))) / (sqrt(2.0 * 3.141592653589793) * s);
-}
-
-__device__ __forceinline__ void source_factor(double ts, double tn, bool inverse, double &fp, double &fc) {
-    double sign = inverse ? 1.0 : -1.0;
-    double a = tn < kExpClamp ? tn : kExpClamp;
-    double tsum = tn + ts;
-    double b = tsum < kExpClamp ? tsum : kExpClamp;
-    fp = dd_exp(sign * a);
-    fc = dd_exp(sign * b);
-}
 
 // ---------------------------------------------------------------------------
 // init: state at the start energy, S and spectrum for the first CFL
@@ -201,6 +79,7 @@ __global__ void init_kernel(const ConfigDev *cfp, Coeffs *co, MarchState *st, do
         st->reboxed = 0;
         st->newmax_bits = 0ull;
         st->pin_max = 0.0;
+        st->cell_steps = 0.0;
         const bool moving = cf.moving && !full_domain;
         st->dom = moving ? cf.init_box : make_domain(0, 0, 0, cf.nx, cf.ny, cf.nz, 1);
         st->prev = st->dom;
@@ -260,6 +139,7 @@ __global__ void __launch_bounds__(256) prologue_kernel(const ConfigDev *cfp, Coe
                     }
                     st->step = step;
                     st->E = En;
+                    st->cell_steps += (double)st->dom.nx * st->dom.ny * st->dom.nz;
                     st->inv_bits = 0ull;
                     if (st->forced_dE > 0.0) st->done = 1;
                 }
@@ -353,428 +233,6 @@ __global__ void __launch_bounds__(256) prologue_kernel(const ConfigDev *cfp, Coe
         co->hs[m] = (cf.strang && cf.scattering != PDM1_SCATTERING_OFF)
                         ? dd_exp(-(th < kExpClamp ? th : kExpClamp)) : 1.0;
     }
-}
-
-// ---------------------------------------------------------------------------
-// The fused stage kernel
-// ---------------------------------------------------------------------------
-constexpr int TX = 4, TY = 8, TZ = 8;
-constexpr int NT = TX * TY * TZ;
-constexpr int NFX = (TX + 1) * TY * TZ;
-constexpr int NFY = TX * (TY + 1) * TZ;
-constexpr int NFZ = TX * TY * (TZ + 1);
-constexpr int NF = NFX + NFY + NFZ;
-constexpr int SX = (TX + 6) * TY * TZ;   // x-arm including the core
-constexpr int SY = TX * 6 * TZ;          // y halo
-constexpr int SZ = TX * TY * 6;          // z halo
-constexpr size_t kStageSmem = sizeof(double) * 4 * (SX + SY + SZ + NF);
-
-__host__ __device__ inline DomainDev make_domain(int i0, int j0, int k0, int nx, int ny, int nz, int inflow) {
-    DomainDev d;
-    d.i0 = i0; d.j0 = j0; d.k0 = k0;
-    d.nx = nx; d.ny = ny; d.nz = nz;
-    d.tiles_y = (ny + TY - 1) / TY;
-    d.tiles_z = (nz + TZ - 1) / TZ;
-    d.ntiles = ((nx + TX - 1) / TX) * d.tiles_y * d.tiles_z;
-    d.inflow = inflow;
-    return d;
-}
-
-enum StageMode { MODE_A = 0, MODE_B = 1, MODE_C = 2, MODE_EULER = 3, MODE_RHS = 4 };
-
-struct StageArgs {
-    const ConfigDev *cf;
-    const Coeffs *co;
-    MarchState *st;
-    double *U1;         // stage states (on the current domain)
-    double *U2;
-    double *V;          // marched variable of stage 1 / 2
-    double *qpart;      // (q0 + q1)/6 quadrature part
-    double *dose;       // accumulated dose (full grid), or NULL
-    double *edep;       // when non-NULL: energy deposition written instead of dose
-    double *snap;       // snapshot buffer base (slot * 4N, full grid)
-    double *rhs_out;    // MODE_RHS output
-    const double *bc_plane;   // MODE_RHS: explicit z-min boundary state (4,nx,ny)
-    double rhs_energy_density;
-};
-
-struct Smem {
-    double *X, *Y, *Z, *F;
-};
-
-__device__ __forceinline__ double sval(const Smem &s, int c, int i, int j, int k) {
-    if (j < 0) return s.Y[((c * TX + i) * 6 + (j + 3)) * TZ + k];
-    if (j >= TY) return s.Y[((c * TX + i) * 6 + (j - TY + 3)) * TZ + k];
-    if (k < 0) return s.Z[((c * TX + i) * TY + j) * 6 + (k + 3)];
-    if (k >= TZ) return s.Z[((c * TX + i) * TY + j) * 6 + (k - TZ + 3)];
-    return s.X[((c * (TX + 6) + (i + 3)) * TY + j) * TZ + k];
-}
-
-__device__ __forceinline__ size_t global_cell(const ConfigDev &cf, const DomainDev &d, int li, int lj, int lk) {
-    return ((size_t)(d.i0 + li) * cf.ny + (d.j0 + lj)) * cf.nz + (d.k0 + lk);
-}
-
-// Stencil source value at a domain cell; indices outside the domain are
-// clamped (zero-gradient ghosts, numerics/boundary.py:327-397).
-template <int MODE>
-__device__ __forceinline__ void load_cell(const ConfigDev &cf, const Coeffs &co, const DomainDev &d,
-                                          const double *src, int li, int lj, int lk, double out[4]) {
-    const int nx = d.nx, ny = d.ny, nz = d.nz;
-    const size_t N = (size_t)nx * ny * nz;
-    li = li < 0 ? 0 : (li >= nx ? nx - 1 : li);
-    lj = lj < 0 ? 0 : (lj >= ny ? ny - 1 : lj);
-    lk = lk >= nz ? nz - 1 : lk;
-    size_t o = ((size_t)li * ny + lj) * nz + lk;
-#pragma unroll
-    for (int c = 0; c < 4; ++c) out[c] = src[c * N + o];
-    if ((MODE == MODE_A || MODE == MODE_EULER) && cf.strang) {
-        int m = cf.ids[global_cell(cf, d, li, lj, lk)];
-        double hn = co.hn[m], hs = co.hs[m];
-        if (cf.nuclear)
-#pragma unroll
-            for (int c = 0; c < 4; ++c) out[c] *= hn;
-        if (cf.scattering != PDM1_SCATTERING_OFF)
-#pragma unroll
-            for (int c = 1; c < 4; ++c) out[c] *= hs;
-    }
-}
-
-// z-min boundary value of component c at domain column (li, lj) for this stage.
-// A moving box away from the entrance has zero inflow (moving_active_domain.py:85-95).
-template <int MODE>
-__device__ __forceinline__ double boundary_value(const StageArgs &a, const ConfigDev &cf, const Coeffs &co,
-                                                 const DomainDev &d, int c, int li, int lj) {
-    if (MODE == MODE_RHS && a.bc_plane)
-        return a.bc_plane[((size_t)c * d.nx + li) * d.ny + lj];
-    if (!d.inflow || c == 1 || c == 2) return 0.0;
-    const int gi = d.i0 + li, gj = d.j0 + lj;
-    double sp = cf.spatial[(size_t)gi * cf.ny + gj];
-    if (MODE == MODE_A || MODE == MODE_EULER || MODE == MODE_RHS) {
-        double ed = MODE == MODE_RHS ? a.rhs_energy_density : co.ed[0];
-        double phi = sp * ed;
-        return c == 0 ? phi : cf.rf * phi;
-    }
-    // RK-consistent stage traces, numerics/energy.py:348-455 (107-231 without sources)
-    int m = cf.ids[((size_t)gi * cf.ny + gj) * cf.nz];
-    double V[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        double phi = sp * co.ed[q];
-        double x = c == 0 ? phi : cf.rf * phi;
-        double B = co.Sb[q][m] * x;
-        if (q > 0 && cf.use_if) B *= (c == 0 ? co.fip[q][m] : co.fic[q][m]);
-        V[q] = B;
-    }
-    if (MODE == MODE_B) {
-        double vs1 = 0.5 * (-9.0 * V[0] + 18.0 * V[1] - 9.0 * V[2] + 2.0 * V[3]);
-        if (cf.use_if) vs1 *= (c == 0 ? co.c1p[m] : co.c1c[m]);
-        return vs1 / co.S1[m];
-    }
-    double vs2 = 0.25 * (11.0 * V[0] - 27.0 * V[1] + 27.0 * V[2] - 7.0 * V[3]);
-    if (cf.use_if) vs2 *= (c == 0 ? co.c2p[m] : co.c2c[m]);
-    return vs2 / co.S2[m];
-}
-
-// One cell's CFL term (numerics/energy.py:539-660): sum over axes of a/(S d).
-// `entrance`: the cell is on the domain's z-min layer, where the inflow state
-// (zero for a box away from the entrance) joins the z speeds.
-__device__ __forceinline__ double cfl_term(const ConfigDev &cf, const double u[4], double s, bool entrance,
-                                           double phi_in, const bool use[3]) {
-    double a0, a1, a2;
-    if (cf.unit_speeds) {
-        a0 = a1 = a2 = 1.0;
-    } else {
-        a0 = max_abs_speed(u[0], u[1], u[2], u[3], 0);
-        a1 = max_abs_speed(u[0], u[1], u[2], u[3], 1);
-        a2 = max_abs_speed(u[0], u[1], u[2], u[3], 2);
-        if (entrance) {
-            double jz = cf.rf * phi_in;
-            double ain = max_abs_speed(phi_in, 0.0, 0.0, jz, 2);
-            if (ain > a2) a2 = ain;
-        }
-    }
-    if (!use[0]) a0 = 0.0;
-    if (!use[1]) a1 = 0.0;
-    if (!use[2]) a2 = 0.0;
-    return a0 / (s * cf.dx) + a1 / (s * cf.dy) + a2 / (s * cf.dz);
-}
-
-__device__ __forceinline__ void block_max_atomic(double v, unsigned long long *target) {
-    // v >= 0 or NaN; NaN never wins (fmax), like the oracle's comparison loop
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-    __shared__ double wmax[NT / 32];
-    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    __syncthreads();
-    if (l == 0) wmax[w] = v;
-    __syncthreads();
-    if (w == 0) {
-        v = l < NT / 32 ? wmax[l] : 0.0;
-        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-        if (l == 0 && v > 0.0) atomicMax(target, (unsigned long long)__double_as_longlong(v));
-    }
-}
-
-__device__ __forceinline__ void atomic_max_double(unsigned long long *target, double v) {
-    if (v > 0.0) atomicMax(target, (unsigned long long)__double_as_longlong(v));
-}
-
-// Per-slab maxima of phi over one tile (moving box): cell values in `buf`
-// (TX*TY*TZ doubles, -1 for cells outside the box).
-__device__ __forceinline__ void tile_slab_max(const ConfigDev &cf, const DomainDev &d, const double *buf,
-                                              int i0, int j0, int k0) {
-    int t = threadIdx.x;
-    unsigned long long *sx = cf.slab, *sy = cf.slab + cf.nx, *sz = cf.slab + cf.nx + cf.ny;
-    if (t < TX) {
-        double m = 0.0;
-        for (int e = 0; e < TY * TZ; ++e) m = fmax(m, buf[t * TY * TZ + e]);
-        if (i0 + t < d.nx) atomic_max_double(&sx[i0 + t], m);
-    } else if (t < TX + TY) {
-        int j = t - TX;
-        double m = 0.0;
-        for (int i = 0; i < TX; ++i)
-            for (int k = 0; k < TZ; ++k) m = fmax(m, buf[(i * TY + j) * TZ + k]);
-        if (j0 + j < d.ny) atomic_max_double(&sy[j0 + j], m);
-    } else if (t < TX + TY + TZ) {
-        int k = t - TX - TY;
-        double m = 0.0;
-        for (int i = 0; i < TX; ++i)
-            for (int j = 0; j < TY; ++j) m = fmax(m, buf[(i * TY + j) * TZ + k]);
-        if (k0 + k < d.nz) atomic_max_double(&sz[k0 + k], m);
-    }
-}
-
-template <int MODE>
-__global__ void __launch_bounds__(NT, 2) stage_kernel(StageArgs a) {
-    const ConfigDev &cf = *a.cf;
-    const Coeffs &co = *a.co;
-    if (MODE != MODE_RHS && !co.active) return;
-    extern __shared__ double smem[];
-    Smem s;
-    s.X = smem;
-    s.Y = s.X + 4 * SX;
-    s.Z = s.Y + 4 * SY;
-    s.F = s.Z + 4 * SZ;
-    const DomainDev d = a.st->dom;
-    double *const Ua = a.st->Ua;
-    const int nx = d.nx, ny = d.ny, nz = d.nz;
-    const size_t N = (size_t)nx * ny * nz;
-    const int tid = threadIdx.x;
-    const double *src = (MODE == MODE_B) ? a.U1 : (MODE == MODE_C ? a.U2 : Ua);
-    const bool unit = cf.unit_speeds != 0;
-    const bool all_axes[3] = {true, true, true};
-    double cta_inv = 0.0;
-
-    for (int tile = blockIdx.x; tile < d.ntiles; tile += gridDim.x) {
-        const int tz = tile % d.tiles_z, ty = (tile / d.tiles_z) % d.tiles_y, tx = tile / (d.tiles_z * d.tiles_y);
-        const int i0 = tx * TX, j0 = ty * TY, k0 = tz * TZ;
-
-        // ---- 1. stage the stencil source + halo ----
-        for (int e = tid; e < SX; e += NT) {
-            int k = e % TZ, j = (e / TZ) % TY, ii = e / (TZ * TY);
-            double u[4];
-            load_cell<MODE>(cf, co, d, src, i0 + ii - 3, j0 + j, k0 + k, u);
-#pragma unroll
-            for (int c = 0; c < 4; ++c) s.X[((c * (TX + 6) + ii) * TY + j) * TZ + k] = u[c];
-        }
-        for (int e = tid; e < SY; e += NT) {
-            int k = e % TZ, jj = (e / TZ) % 6, i = e / (TZ * 6);
-            int gj = jj < 3 ? j0 + jj - 3 : j0 + TY + jj - 3;
-            double u[4];
-            load_cell<MODE>(cf, co, d, src, i0 + i, gj, k0 + k, u);
-#pragma unroll
-            for (int c = 0; c < 4; ++c) s.Y[((c * TX + i) * 6 + jj) * TZ + k] = u[c];
-        }
-        for (int e = tid; e < SZ; e += NT) {
-            int kk = e % 6, j = (e / 6) % TY, i = e / (6 * TY);
-            int gk = kk < 3 ? k0 + kk - 3 : k0 + TZ + kk - 3;
-            if (gk < 0) continue;   // z-min ghost, filled below
-            double u[4];
-            load_cell<MODE>(cf, co, d, src, i0 + i, j0 + j, gk, u);
-#pragma unroll
-            for (int c = 0; c < 4; ++c) s.Z[((c * TX + i) * TY + j) * 6 + kk] = u[c];
-        }
-        __syncthreads();
-        // ---- 2. z-min ghost cells: quartic extrapolation through the inflow ----
-        if (k0 == 0) {
-            for (int e = tid; e < 4 * TX * TY; e += NT) {
-                int j = e % TY, i = (e / TY) % TX, c = e / (TX * TY);
-                int li = i0 + i, lj = j0 + j;
-                if (li >= nx || lj >= ny) continue;
-                double ui = boundary_value<MODE>(a, cf, co, d, c, li, lj);
-                const double *col = &s.X[((c * (TX + 6) + (i + 3)) * TY + j) * TZ];
-                double u0 = col[0], u1 = col[1], u2 = col[2], u3 = col[3];
-                double *z = &s.Z[((c * TX + i) * TY + j) * 6];
-                z[2] = 5.0 * ui - (77.0 / 12.0) * u0 + (43.0 / 12.0) * u1 - (17.0 / 12.0) * u2 + 0.25 * u3;
-                z[1] = 25.0 * ui - (505.0 / 12.0) * u0 + (335.0 / 12.0) * u1 - (145.0 / 12.0) * u2 + (9.0 / 4.0) * u3;
-                z[0] = 75.0 * ui - (545.0 / 4.0) * u0 + (395.0 / 4.0) * u1 - (181.0 / 4.0) * u2 + (35.0 / 4.0) * u3;
-            }
-            __syncthreads();
-        }
-        // ---- 3. every face of the tile: WENO-Z, projection, HLL ----
-        for (int f = tid; f < NF; f += NT) {
-            int axis, i, j, k;
-            if (f < NFX) {
-                axis = 0; k = f % TZ; j = (f / TZ) % TY; i = f / (TZ * TY);
-            } else if (f < NFX + NFY) {
-                int u = f - NFX;
-                axis = 1; k = u % TZ; j = (u / TZ) % (TY + 1); i = u / (TZ * (TY + 1));
-            } else {
-                int u = f - NFX - NFY;
-                axis = 2; k = u % (TZ + 1); j = (u / (TZ + 1)) % TY; i = u / ((TZ + 1) * TY);
-            }
-            double L[4], R[4];
-            const int di = axis == 0, dj = axis == 1, dk = axis == 2;
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                double w[6];
-#pragma unroll
-                for (int q = 0; q < 6; ++q) {
-                    int o = q - 3;
-                    w[q] = sval(s, c, i + o * di, j + o * dj, k + o * dk);
-                }
-                L[c] = weno_left(w[0], w[1], w[2], w[3], w[4]);
-                R[c] = weno_left(w[5], w[4], w[3], w[2], w[1]);
-            }
-            project(L[0], L[1], L[2], L[3]);
-            project(R[0], R[1], R[2], R[3]);
-            double F[4];
-            hll_flux(L, R, axis, unit, F);
-#pragma unroll
-            for (int c = 0; c < 4; ++c) s.F[c * NF + f] = F[c];
-        }
-        __syncthreads();
-        // ---- 4. divergence and the stage update, one cell per thread ----
-        const int k = tid % TZ, j = (tid / TZ) % TY, i = tid / (TZ * TY);
-        const int li = i0 + i, lj = j0 + j, lk = k0 + k;
-        const bool valid = li < nx && lj < ny && lk < nz;
-        double phi_new = -1.0;   // for the moving box's slab maxima
-        if (valid) {
-            const int fx0 = (i * TY + j) * TZ + k, fx1 = ((i + 1) * TY + j) * TZ + k;
-            const int fy0 = NFX + (i * (TY + 1) + j) * TZ + k, fy1 = NFX + (i * (TY + 1) + j + 1) * TZ + k;
-            const int fz0 = NFX + NFY + (i * TY + j) * (TZ + 1) + k, fz1 = fz0 + 1;
-            double L[4];
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                const double *F = s.F + c * NF;
-                double gx = (F[fx1] - F[fx0]) / cf.dx;
-                double gy = (F[fy1] - F[fy0]) / cf.dy;
-                double gz = (F[fz1] - F[fz0]) / cf.dz;
-                L[c] = -(gx + gy + gz);
-            }
-            const size_t o = ((size_t)li * ny + lj) * nz + lk;
-            if (MODE == MODE_RHS) {
-#pragma unroll
-                for (int c = 0; c < 4; ++c) a.rhs_out[c * N + o] = L[c];
-            } else {
-                const size_t go = global_cell(cf, d, li, lj, lk);
-                const int m = cf.ids[go];
-                const double dE = co.dE;
-                // the accepted state at this cell (with the Strang half step applied)
-                double un[4];
-                if (MODE == MODE_A || MODE == MODE_EULER) {
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) un[c] = s.X[((c * (TX + 6) + (i + 3)) * TY + j) * TZ + k];
-                } else {
-                    load_cell<MODE_A>(cf, co, d, Ua, li, lj, lk, un);
-                }
-                const double s0 = co.S0[m];
-                if (MODE == MODE_A) {
-                    double u1[4], v1[4];
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) {
-                        double v0 = s0 * un[c];
-                        double v = L[c] * dE + v0;
-                        v1[c] = v;
-                        double w = v * (c == 0 ? co.c1p[m] : co.c1c[m]);
-                        u1[c] = w / co.S1[m];
-                    }
-                    project(u1[0], u1[1], u1[2], u1[3]);
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) {
-                        a.U1[c * N + o] = u1[c];
-                        a.V[c * N + o] = v1[c];
-                    }
-                    double q0 = un[0] * s0, q1 = u1[0] * co.S1[m];
-                    a.qpart[o] = 1.0 / 6.0 * q0 + 1.0 / 6.0 * q1;
-                } else if (MODE == MODE_B) {
-                    double u2[4];
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) {
-                        double r = L[c] * (c == 0 ? co.c1ip[m] : co.c1ic[m]);
-                        r = (r * dE + a.V[c * N + o]) * 0.25;
-                        double v = 0.75 * (s0 * un[c]) + r;
-                        a.V[c * N + o] = v;
-                        double w = v * (c == 0 ? co.c2p[m] : co.c2c[m]);
-                        u2[c] = w / co.S2[m];
-                    }
-                    project(u2[0], u2[1], u2[2], u2[3]);
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) a.U2[c * N + o] = u2[c];
-                } else {
-                    double unew[4];
-                    double ed;
-                    if (MODE == MODE_C) {
-#pragma unroll
-                        for (int c = 0; c < 4; ++c) {
-                            double r = L[c] * (c == 0 ? co.c2ip[m] : co.c2ic[m]);
-                            r = (r * dE + a.V[c * N + o]) * (2.0 / 3.0);
-                            double v = 1.0 / 3.0 * (s0 * un[c]) + r;
-                            double w = v * (c == 0 ? co.c1p[m] : co.c1c[m]);
-                            unew[c] = w / co.S1[m];
-                        }
-                        project(unew[0], unew[1], unew[2], unew[3]);
-                        double q2 = s.X[((0 * (TX + 6) + (i + 3)) * TY + j) * TZ + k] * co.S2[m];
-                        ed = dE * (a.qpart[o] + 2.0 / 3.0 * q2);
-                    } else {   // forward Euler, numerics/energy.py:663-722
-#pragma unroll
-                        for (int c = 0; c < 4; ++c) {
-                            double w = L[c] * dE + s0 * un[c];
-                            unew[c] = w / co.S1[m];
-                        }
-                        project(unew[0], unew[1], unew[2], unew[3]);
-                        ed = dE * un[0] * s0;
-                    }
-                    if (cf.strang) {
-                        if (cf.nuclear)
-#pragma unroll
-                            for (int c = 0; c < 4; ++c) unew[c] *= co.hn[m];
-                        if (cf.scattering != PDM1_SCATTERING_OFF)
-#pragma unroll
-                            for (int c = 1; c < 4; ++c) unew[c] *= co.hs[m];
-                    }
-                    double *dst = MODE == MODE_C ? Ua : a.U1;
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) dst[c * N + o] = unew[c];
-                    if (a.edep) a.edep[o] = ed;
-                    else a.dose[go] += ed * kMevToJoule / cf.mats[m].density;
-                    if (MODE == MODE_C) {
-                        if (co.snap_slot >= 0 && a.snap) {
-                            const size_t NG = (size_t)cf.nx * cf.ny * cf.nz;
-                            double *sn = a.snap + (size_t)co.snap_slot * 4 * NG;
-#pragma unroll
-                            for (int c = 0; c < 4; ++c) sn[c * NG + go] = unew[c];
-                        }
-                        if (!cf.moving) {
-                            double phi_in = 0.0;
-                            if (lk == 0 && d.inflow)
-                                phi_in = cf.spatial[(size_t)(d.i0 + li) * cf.ny + (d.j0 + lj)] * co.ed_next;
-                            double v = cfl_term(cf, unew, co.S1[m], lk == 0, phi_in, all_axes);
-                            cta_inv = fmax(cta_inv, v);
-                        }
-                        phi_new = unew[0];
-                    }
-                }
-            }
-        }
-        if (MODE == MODE_C && cf.moving) {
-            __syncthreads();
-            s.F[tid] = phi_new;   // the flux buffer is free after the divergence
-            __syncthreads();
-            tile_slab_max(cf, d, s.F, i0, j0, k0);
-        }
-        __syncthreads();   // shared memory is reused by the next tile
-    }
-    if (MODE == MODE_C && !cf.moving) block_max_atomic(cta_inv, &a.st->inv_bits);
 }
 
 // Forward Euler writes U1; this copies it back, snapshots, and either reduces
@@ -1278,6 +736,22 @@ int cell_blocks(const pdm1_problem &p) {
 }
 
 // Launch one energy step (prologue + stages) on `stream`; returns launches.
+// One stage launch in the plan's precision.
+void launch_stage(const pdm1_plan *pl, int mode, int grid, const StageArgs &a, cudaStream_t stream) {
+    if (pl->p.precision == PDM1_FP32_FP64) {
+        launch_stage_fp32(mode, grid, a, stream);
+        return;
+    }
+    const size_t bytes = stage_smem_bytes<double>();
+    switch (mode) {
+    case MODE_A: stage_kernel<double, MODE_A><<<grid, NT, bytes, stream>>>(a); break;
+    case MODE_B: stage_kernel<double, MODE_B><<<grid, NT, bytes, stream>>>(a); break;
+    case MODE_C: stage_kernel<double, MODE_C><<<grid, NT, bytes, stream>>>(a); break;
+    case MODE_EULER: stage_kernel<double, MODE_EULER><<<grid, NT, bytes, stream>>>(a); break;
+    default: stage_kernel<double, MODE_RHS><<<grid, NT, bytes, stream>>>(a); break;
+    }
+}
+
 // The moving box's per-step work ahead of the prologue: desired box, rebox,
 // activity mask, CFL bound over the new box.
 int launch_box_step(pdm1_plan *pl, cudaStream_t stream) {
@@ -1298,13 +772,13 @@ int launch_step(pdm1_plan *pl, const StageArgs &a, cudaStream_t stream) {
     const int grid = pl->cf.grid_ctas;
     prologue_kernel<<<1, 256, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, nullptr);
     if (p.energy_scheme == PDM1_SCHEME_FORWARD_EULER) {
-        stage_kernel<MODE_EULER><<<grid, NT, kStageSmem, stream>>>(a);
+        launch_stage(pl, MODE_EULER, grid, a, stream);
         euler_finish_kernel<<<cell_blocks(p), NT, 0, stream>>>(a);
         return 3;
     }
-    stage_kernel<MODE_A><<<grid, NT, kStageSmem, stream>>>(a);
-    stage_kernel<MODE_B><<<grid, NT, kStageSmem, stream>>>(a);
-    stage_kernel<MODE_C><<<grid, NT, kStageSmem, stream>>>(a);
+    launch_stage(pl, MODE_A, grid, a, stream);
+    launch_stage(pl, MODE_B, grid, a, stream);
+    launch_stage(pl, MODE_C, grid, a, stream);
     return 4;
 }
 
@@ -1319,12 +793,12 @@ int launch_step_with_energies(pdm1_plan *pl, const StageArgs &a, double *energie
     cudaEventRecordWithFlags(pl->ev[2 * slot], stream, cudaEventRecordExternal);
     int n;
     if (p.energy_scheme == PDM1_SCHEME_FORWARD_EULER) {
-        stage_kernel<MODE_EULER><<<grid, NT, kStageSmem, stream>>>(a);
+        launch_stage(pl, MODE_EULER, grid, a, stream);
         n = 1;
     } else {
-        stage_kernel<MODE_A><<<grid, NT, kStageSmem, stream>>>(a);
-        stage_kernel<MODE_B><<<grid, NT, kStageSmem, stream>>>(a);
-        stage_kernel<MODE_C><<<grid, NT, kStageSmem, stream>>>(a);
+        launch_stage(pl, MODE_A, grid, a, stream);
+        launch_stage(pl, MODE_B, grid, a, stream);
+        launch_stage(pl, MODE_C, grid, a, stream);
         n = 3;
     }
     cudaEventRecordWithFlags(pl->ev[2 * slot + 1], stream, cudaEventRecordExternal);
@@ -1339,11 +813,12 @@ int launch_step_with_energies(pdm1_plan *pl, const StageArgs &a, double *energie
 int set_smem_attributes() {
     static bool done = false;
     if (done) return PDM1_OK;
-    CUDA_TRY(cudaFuncSetAttribute(stage_kernel<MODE_A>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageSmem));
-    CUDA_TRY(cudaFuncSetAttribute(stage_kernel<MODE_B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageSmem));
-    CUDA_TRY(cudaFuncSetAttribute(stage_kernel<MODE_C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageSmem));
-    CUDA_TRY(cudaFuncSetAttribute(stage_kernel<MODE_EULER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageSmem));
-    CUDA_TRY(cudaFuncSetAttribute(stage_kernel<MODE_RHS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageSmem));
+    CUDA_TRY(cudaFuncSetAttribute(stage_kernel<double, MODE_A>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem_bytes<double>()));
+    CUDA_TRY(cudaFuncSetAttribute(stage_kernel<double, MODE_B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem_bytes<double>()));
+    CUDA_TRY(cudaFuncSetAttribute(stage_kernel<double, MODE_C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem_bytes<double>()));
+    CUDA_TRY(cudaFuncSetAttribute(stage_kernel<double, MODE_EULER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem_bytes<double>()));
+    CUDA_TRY(cudaFuncSetAttribute(stage_kernel<double, MODE_RHS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem_bytes<double>()));
+    CUDA_TRY((cudaError_t)stage_fp32_set_attributes());
     done = true;
     return PDM1_OK;
 }
@@ -1351,7 +826,7 @@ int set_smem_attributes() {
 int device_error_status(const MarchState &st) {
     if (st.error & ERR_DEV_RANGE) return set_error(PDM1_ERR_RANGE, "energy outside a coefficient table during the march");
     if (st.error & ERR_DEV_MAXSTEPS) return set_error(PDM1_ERR_MAX_STEPS, "energies buffer shorter than the march");
-    if (st.error & ERR_DEV_NONFINITE) return set_error(PDM1_ERR_NONFINITE, "non-finite or non-positive energy step");
+    if (st.error & ERR_DEV_NONFINITE) return set_error(PDM1_ERR_NONFINITE, "non-finite state or non-positive energy step during the march");
     return PDM1_OK;
 }
 
@@ -1633,6 +1108,7 @@ static int march_impl(pdm1_plan *pl, double *U, double *dose, double *energies, 
         info->kernel_launches = launches;
         info->stage_launches = stage_launches;
         info->stage_ms = stage_ms;
+        info->cell_steps = pl->h_st->cell_steps;
     }
     if (snap_E_out)
         for (int i = 0; i < pl->h_st->taken; ++i) snap_E_out[i] = tg[i];
@@ -1671,7 +1147,7 @@ int pdm1_spatial_operator(pdm1_plan *pl, const double *U, double energy, const d
     a.bc_plane = bc;
     double de = energy - pl->p.beam_energy, s = pl->p.energy_spread;
     a.rhs_energy_density = dd_exp(-(de * de) / (2.0 * (s * s))) / (std::sqrt(2.0 * 3.141592653589793) * s);
-    stage_kernel<MODE_RHS><<<pl->cf.grid_ctas, NT, kStageSmem, stream>>>(a);
+    launch_stage(pl, MODE_RHS, pl->cf.grid_ctas, a, stream);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(stream));
     return PDM1_OK;
@@ -1845,13 +1321,13 @@ void launch_step_plain(const pdm1_problem &p, ConfigDev *d_cf, Coeffs *d_co, Mar
                        const StageArgs &a, double *energies, int tiles, cudaStream_t stream) {
     prologue_kernel<<<1, 256, 0, stream>>>(d_cf, d_co, d_st, energies);
     if (p.energy_scheme == PDM1_SCHEME_FORWARD_EULER) {
-        stage_kernel<MODE_EULER><<<tiles, NT, kStageSmem, stream>>>(a);
+        stage_kernel<double, MODE_EULER><<<tiles, NT, stage_smem_bytes<double>(), stream>>>(a);
         euler_finish_kernel<<<cell_blocks(p), NT, 0, stream>>>(a);
         return;
     }
-    stage_kernel<MODE_A><<<tiles, NT, kStageSmem, stream>>>(a);
-    stage_kernel<MODE_B><<<tiles, NT, kStageSmem, stream>>>(a);
-    stage_kernel<MODE_C><<<tiles, NT, kStageSmem, stream>>>(a);
+    stage_kernel<double, MODE_A><<<tiles, NT, stage_smem_bytes<double>(), stream>>>(a);
+    stage_kernel<double, MODE_B><<<tiles, NT, stage_smem_bytes<double>(), stream>>>(a);
+    stage_kernel<double, MODE_C><<<tiles, NT, stage_smem_bytes<double>(), stream>>>(a);
 }
 
 }  // namespace
@@ -1919,10 +1395,10 @@ extern "C" int pdm1_march_noalloc(const pdm1_problem *problem, double *U, double
     if (!g_noalloc_base[dev]) {
         void *ptr = nullptr;
         CUDA_TRY(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
-        CUDA_TRY(cudaFuncSetAttribute(stage_kernel<MODE_A>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageSmem));
-        CUDA_TRY(cudaFuncSetAttribute(stage_kernel<MODE_B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageSmem));
-        CUDA_TRY(cudaFuncSetAttribute(stage_kernel<MODE_C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageSmem));
-        CUDA_TRY(cudaFuncSetAttribute(stage_kernel<MODE_EULER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageSmem));
+        CUDA_TRY(cudaFuncSetAttribute(stage_kernel<double, MODE_A>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem_bytes<double>()));
+        CUDA_TRY(cudaFuncSetAttribute(stage_kernel<double, MODE_B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem_bytes<double>()));
+        CUDA_TRY(cudaFuncSetAttribute(stage_kernel<double, MODE_C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem_bytes<double>()));
+        CUDA_TRY(cudaFuncSetAttribute(stage_kernel<double, MODE_EULER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem_bytes<double>()));
         g_noalloc_base[dev] = ptr;
     }
     unsigned char *base = static_cast<unsigned char *>(g_noalloc_base[dev]);
@@ -2021,6 +1497,7 @@ extern "C" int pdm1_march_noalloc(const pdm1_problem *problem, double *U, double
         info->kernel_launches = launches;
         info->stage_launches = 0;
         info->stage_ms = 0.0;
+        info->cell_steps = hs.cell_steps;
     }
     (void)chunks;
     return device_error_status(hs);

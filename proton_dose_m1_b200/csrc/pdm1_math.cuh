@@ -97,9 +97,28 @@ PDM1_HD T weno_left(T v0, T v1, T v2, T v3, T v4) {
     T r0 = tau5 / (beta0 + T(kWenoEps));
     T r1 = tau5 / (beta1 + T(kWenoEps));
     T r2 = tau5 / (beta2 + T(kWenoEps));
-    T al0 = T(0.1) * (T(1) + r0 * r0);
-    T al1 = T(0.6) * (T(1) + r1 * r1);
-    T al2 = T(0.3) * (T(1) + r2 * r2);
+    T al0, al1, al2;
+    if (sizeof(T) < sizeof(double)) {
+        // single precision: r^2 overflows above ~1.8e19, which a flat stencil
+        // next to a steep one reaches (beta ~ 0 against beta ~ phi^2 ~ 1e22);
+        // divide every alpha by rmax^2 first -- the weights are unchanged
+        T rmax = fmax(r0, fmax(r1, r2));
+        if (rmax > T(1e15)) {
+            T inv = T(1) / rmax;
+            T q0 = r0 * inv, q1 = r1 * inv, q2 = r2 * inv, e = inv * inv;
+            al0 = T(0.1) * (e + q0 * q0);
+            al1 = T(0.6) * (e + q1 * q1);
+            al2 = T(0.3) * (e + q2 * q2);
+        } else {
+            al0 = T(0.1) * (T(1) + r0 * r0);
+            al1 = T(0.6) * (T(1) + r1 * r1);
+            al2 = T(0.3) * (T(1) + r2 * r2);
+        }
+    } else {
+        al0 = T(0.1) * (T(1) + r0 * r0);
+        al1 = T(0.6) * (T(1) + r1 * r1);
+        al2 = T(0.3) * (T(1) + r2 * r2);
+    }
     T s = al0 + al1 + al2;
     T w0 = al0 / s, w1 = al1 / s, w2 = al2 / s;
     return w0 * p0 + w1 * p1 + w2 * p2;
@@ -169,14 +188,22 @@ PDM1_HD Closure<T> closure(T phi, T jx, T jy, T jz) {
     } else {
         f = T(0);
     }
-    T chi = (T(5) - T(2) * sqrt(T(4) - T(3) * f * f)) / T(3);
     if (c.jn > T(0)) {
         c.nx = jx / c.jn; c.ny = jy / c.jn; c.nz = jz / c.jn;
     } else {
         c.nx = c.ny = c.nz = T(0);
     }
-    c.iso = T(0.5) * (T(1) - chi);
-    c.dir = T(0.5) * (T(3) * chi - T(1));
+    if (sizeof(T) < sizeof(double)) {
+        // single precision: 0.5*(1 - chi) cancels as f -> 1; the same quantity
+        // without the cancellation is (1 - f^2) / (sqrt(4 - 3 f^2) + 1)
+        T root = sqrt(T(4) - T(3) * f * f);
+        c.iso = (T(1) - f) * (T(1) + f) / (root + T(1));
+        c.dir = T(2) - root;
+    } else {
+        T chi = (T(5) - T(2) * sqrt(T(4) - T(3) * f * f)) / T(3);
+        c.iso = T(0.5) * (T(1) - chi);
+        c.dir = T(0.5) * (T(3) * chi - T(1));
+    }
     return c;
 }
 
@@ -223,6 +250,14 @@ PDM1_HD void hll_flux(const T L[4], const T R[4], int axis, bool unit_speeds, T 
     }
     T den = sr - sl;
     T sp = sl * sr;
+    if (sizeof(T) < sizeof(double) && !(den > T(0))) {
+        // single precision only: |J|/phi rounds to 1 for an exactly directed
+        // state, both speeds normal to J are then 0 and the fan collapses;
+        // the HLL flux tends to the central flux as the fan closes
+#pragma unroll
+        for (int c = 0; c < 4; ++c) F[c] = T(0.5) * (FL[c] + FR[c]);
+        return;
+    }
 #pragma unroll
     for (int c = 0; c < 4; ++c) F[c] = (sr * FL[c] - sl * FR[c] + sp * (R[c] - L[c])) / den;
 }
