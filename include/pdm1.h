@@ -84,6 +84,15 @@ typedef struct {
     int precision;                     /* PDM1_FP64 or PDM1_FP32_FP64 */
 } pdm1_problem;
 
+/* One pencil beam of a field (numerics/boundary.py:63-114): its spectrum and
+ * angular spread, and its transverse profile on the phantom's z-min face. */
+typedef struct {
+    double energy;                  /* MeV */
+    double energy_spread;           /* MeV, > 0 */
+    double angular_spread;          /* rad */
+    const double *inflow_spatial;   /* host (nx, ny): n_protons * normalised profile */
+} pdm1_beam;
+
 typedef struct pdm1_plan pdm1_plan;
 
 typedef struct {
@@ -112,6 +121,23 @@ size_t pdm1_plan_workspace_bytes(const pdm1_plan *plan);
 int pdm1_march(pdm1_plan *plan, double *U, double *dose, double *energies, int max_steps,
                const double *snap_targets, int n_snap, double *snap_out,
                double *snap_energies_out, pdm1_march_info *info, pdm1_stream_t stream);
+
+/* A spot-scanning field: n_beams pencil beams on one phantom, each marching on
+ * its own moving active box with its own energy and CFL step, all of them in
+ * one persistent launch per stage (no reference counterpart: the reference
+ * solves one beam per Solver.solve and never batches).  `phantom` gives the
+ * grid, materials, physics and numerics (its beam fields are ignored;
+ * moving_active_domain must be set); every beam's compact buffers hold
+ * box_capacity_cells cells (0: the whole grid). */
+int pdm1_field_plan_create(const pdm1_problem *phantom, const pdm1_beam *beams, int n_beams,
+                           size_t box_capacity_cells, pdm1_plan **plan);
+
+/* March every beam of a field plan from zero to energy_min; field_dose
+ * (device, (nx,ny,nz)) receives the sum of the beams' doses (FP64 atomic
+ * accumulation, so the summation order across beams is not fixed);
+ * steps_per_beam (host, n_beams) may be NULL.  Synchronises `stream`. */
+int pdm1_field_march(pdm1_plan *plan, double *field_dose, int max_steps, int *steps_per_beam,
+                     pdm1_march_info *info, pdm1_stream_t stream);
 
 /* The first `step_limit` steps of the march (a bounded prefix, for timing
  * samples and prefix parity); otherwise as pdm1_march without snapshots. */

@@ -44,6 +44,11 @@ class Problem(C.Structure):
                 ("precision", C.c_int)]
 
 
+class BeamDesc(C.Structure):
+    _fields_ = [("energy", C.c_double), ("energy_spread", C.c_double),
+                ("angular_spread", C.c_double), ("inflow_spatial", _dp)]
+
+
 class MarchInfo(C.Structure):
     _fields_ = [("n_steps", C.c_int), ("n_snapshots", C.c_int), ("final_state_valid", C.c_int),
                 ("graph_replays", C.c_int), ("kernel_launches", C.c_int),
@@ -71,6 +76,9 @@ def lib():
         L.pdm1_plan_workspace_bytes.restype = C.c_size_t
         L.pdm1_march.argtypes = [_vp, _vp, _vp, _vp, C.c_int, _dp, C.c_int, _vp, _dp,
                                  C.POINTER(MarchInfo), _vp]
+        L.pdm1_field_plan_create.argtypes = [C.POINTER(Problem), C.POINTER(BeamDesc), C.c_int,
+                                             C.c_size_t, C.POINTER(_vp)]
+        L.pdm1_field_march.argtypes = [_vp, _vp, C.c_int, C.POINTER(C.c_int), C.POINTER(MarchInfo), _vp]
         L.pdm1_march_steps.argtypes = [_vp, _vp, _vp, _vp, C.c_int, C.c_int,
                                        C.POINTER(MarchInfo), _vp]
         L.pdm1_spatial_operator.argtypes = [_vp, _vp, C.c_double, _vp, _vp, _vp]
@@ -103,7 +111,7 @@ def check(rc: int) -> None:
 
 EXPORTED_SYMBOLS = (
     "pdm1_plan_create", "pdm1_plan_destroy", "pdm1_plan_workspace_bytes", "pdm1_march",
-    "pdm1_march_steps",
+    "pdm1_march_steps", "pdm1_field_plan_create", "pdm1_field_march",
     "pdm1_spatial_operator", "pdm1_energy_step", "pdm1_advance", "pdm1_coefficients",
     "pdm1_weno_batch", "pdm1_project_batch", "pdm1_eigen_batch", "pdm1_hll_batch",
     "pdm1_exp_batch", "pdm1_gamma", "pdm1_last_error", "pdm1_version",

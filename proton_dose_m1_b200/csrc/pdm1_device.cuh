@@ -12,7 +12,7 @@ namespace pdm1 {
 
 constexpr int kMaxMat = 16;
 
-enum { ERR_DEV_RANGE = 1, ERR_DEV_MAXSTEPS = 2, ERR_DEV_NONFINITE = 4 };
+enum { ERR_DEV_RANGE = 1, ERR_DEV_MAXSTEPS = 2, ERR_DEV_NONFINITE = 4, ERR_DEV_CAPACITY = 8 };
 // ---------------------------------------------------------------------------
 // Device-side plan data
 // ---------------------------------------------------------------------------
@@ -30,6 +30,20 @@ struct DomainDev {
     int inflow;              // the domain's z-min face is the beam entrance (k0 == 0)
 };
 
+// One pencil beam of a march (numerics/boundary.py:63-114): spectrum, angular
+// spread, transverse profile on the grid's z-min face, initial moving box.
+struct BeamDev {
+    double E_beam, sigma_E, rf;     // rf = exp(-angular_spread^2)
+    const double *spatial;          // (nx, ny): n_protons * normalised profile
+    DomainDev init_box;             // moving_active_domain.py:35-60
+};
+
+// What the host polls between graph replays.
+struct MarchSummary {
+    int active;         // beams that marched in the last step
+    int error;          // OR of the beams' error flags
+};
+
 struct ConfigDev {
     int nx, ny, nz;
     double dx, dy, dz;
@@ -37,21 +51,26 @@ struct ConfigDev {
     int scattering, nuclear, interp, scheme, unit_speeds;
     int use_if;          // integrating factors active (IF_SSPRK3 with sources)
     int strang;          // Strang-split sources around an SSPRK3 / Euler step
-    double cfl, max_dE, Emin, E_beam, sigma_E, rf;
+    double cfl, max_dE, Emin;
     int max_steps;
     int step_limit;      // >= 0: stop (without error) after this many steps
     int n_targets;
     const int32_t *ids;
-    const double *spatial;
     const double *targets;      // descending
+    // beams: per-beam buffers hold `cap` cells each (the beam's domain)
+    int nbeams;
+    size_t cap;
+    const BeamDev *beams;
+    int *tile_off;              // (nbeams + 1) prefix sums of the active beams' tiles
+    MarchSummary *summary;
     // moving active box
     int moving, vacuum_aware, guard;
     double tol;                 // exp(-sigma_trunc^2 / 2)
-    DomainDev init_box;         // moving_active_domain.py:35-60
-    double *bufA, *bufB;        // compact-state ping-pong
-    unsigned long long *slab;   // max phi per x | y | z slab of the current box (double bits)
-    unsigned char *active;      // vacuum-aware activity mask on the current box
+    double *bufA, *bufB;        // compact-state ping-pong, 4*cap per beam
+    unsigned long long *slab;   // max phi per x | y | z slab of the box (double bits), per beam
+    unsigned char *active;      // vacuum-aware activity mask on the box, cap per beam
     int grid_ctas;              // persistent grid of the stage kernels
+    int fp32;                   // FP32-stencil form: float eigenvalues in the CFL bound
     MatDev mats[kMaxMat];
 };
 
@@ -121,9 +140,9 @@ __device__ inline bool nuclear_dev(const ConfigDev &cf, const MatDev &m, double 
 }
 
 // numerics/boundary.py:82-114 spectrum factor
-__device__ __forceinline__ double energy_density(const ConfigDev &cf, double E) {
-    double de = E - cf.E_beam;
-    double s = cf.sigma_E;
+__device__ __forceinline__ double energy_density(const BeamDev &bm, double E) {
+    double de = E - bm.E_beam;
+    double s = bm.sigma_E;
     return dd_exp(-(de * de) / (2.0 * (s * s))) / (sqrt(2.0 * 3.141592653589793) * s);
 }
 
@@ -166,9 +185,9 @@ enum StageMode { MODE_A = 0, MODE_B = 1, MODE_C = 2, MODE_EULER = 3, MODE_RHS = 
 
 struct StageArgs {
     const ConfigDev *cf;
-    const Coeffs *co;
-    MarchState *st;
-    double *U1;         // stage states (on the current domain)
+    const Coeffs *co;   // per beam
+    MarchState *st;     // per beam
+    double *U1;         // stage states (on the beam's domain), 4*cap per beam
     double *U2;
     double *V;          // marched variable of stage 1 / 2
     double *qpart;      // (q0 + q1)/6 quadrature part
@@ -226,17 +245,17 @@ __device__ __forceinline__ void load_cell(const ConfigDev &cf, const Coeffs &co,
 // z-min boundary value of component c at domain column (li, lj) for this stage.
 // A moving box away from the entrance has zero inflow (moving_active_domain.py:85-95).
 template <int MODE>
-__device__ __forceinline__ double boundary_value(const StageArgs &a, const ConfigDev &cf, const Coeffs &co,
-                                                 const DomainDev &d, int c, int li, int lj) {
+__device__ __forceinline__ double boundary_value(const StageArgs &a, const ConfigDev &cf, const BeamDev &bm,
+                                                 const Coeffs &co, const DomainDev &d, int c, int li, int lj) {
     if (MODE == MODE_RHS && a.bc_plane)
         return a.bc_plane[((size_t)c * d.nx + li) * d.ny + lj];
     if (!d.inflow || c == 1 || c == 2) return 0.0;
     const int gi = d.i0 + li, gj = d.j0 + lj;
-    double sp = cf.spatial[(size_t)gi * cf.ny + gj];
+    double sp = bm.spatial[(size_t)gi * cf.ny + gj];
     if (MODE == MODE_A || MODE == MODE_EULER || MODE == MODE_RHS) {
         double ed = MODE == MODE_RHS ? a.rhs_energy_density : co.ed[0];
         double phi = sp * ed;
-        return c == 0 ? phi : cf.rf * phi;
+        return c == 0 ? phi : bm.rf * phi;
     }
     // RK-consistent stage traces, numerics/energy.py:348-455 (107-231 without sources)
     int m = cf.ids[((size_t)gi * cf.ny + gj) * cf.nz];
@@ -244,7 +263,7 @@ __device__ __forceinline__ double boundary_value(const StageArgs &a, const Confi
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         double phi = sp * co.ed[q];
-        double x = c == 0 ? phi : cf.rf * phi;
+        double x = c == 0 ? phi : bm.rf * phi;
         double B = co.Sb[q][m] * x;
         if (q > 0 && cf.use_if) B *= (c == 0 ? co.fip[q][m] : co.fic[q][m]);
         V[q] = B;
@@ -262,18 +281,23 @@ __device__ __forceinline__ double boundary_value(const StageArgs &a, const Confi
 // One cell's CFL term (numerics/energy.py:539-660): sum over axes of a/(S d).
 // `entrance`: the cell is on the domain's z-min layer, where the inflow state
 // (zero for a box away from the entrance) joins the z speeds.
-__device__ __forceinline__ double cfl_term(const ConfigDev &cf, const double u[4], double s, bool entrance,
-                                           double phi_in, const bool use[3]) {
+// T: the precision of the eigenvalues -- double for the FP64 march, float for
+// the FP32-stencil form (its step sequence need not match the FP64 one).
+template <typename T>
+__device__ __forceinline__ double cfl_term(const ConfigDev &cf, double rf, const double u[4], double s,
+                                           bool entrance, double phi_in, const bool use[3]) {
     double a0, a1, a2;
     if (cf.unit_speeds) {
         a0 = a1 = a2 = 1.0;
     } else {
-        a0 = max_abs_speed(u[0], u[1], u[2], u[3], 0);
-        a1 = max_abs_speed(u[0], u[1], u[2], u[3], 1);
-        a2 = max_abs_speed(u[0], u[1], u[2], u[3], 2);
+        const T p = T(u[0]), x = T(u[1]), y = T(u[2]), z = T(u[3]);
+        a0 = double(max_abs_speed(p, x, y, z, 0));
+        a1 = double(max_abs_speed(p, x, y, z, 1));
+        a2 = double(max_abs_speed(p, x, y, z, 2));
         if (entrance) {
-            double jz = cf.rf * phi_in;
-            double ain = max_abs_speed(phi_in, 0.0, 0.0, jz, 2);
+            T pin = T(phi_in);
+            T jz = T(rf) * pin;
+            double ain = double(max_abs_speed(pin, T(0), T(0), jz, 2));
             if (ain > a2) a2 = ain;
         }
     }
@@ -304,10 +328,10 @@ __device__ __forceinline__ void atomic_max_double(unsigned long long *target, do
 
 // Per-slab maxima of phi over one tile (moving box): cell values in `buf`
 // (TX*TY*TZ doubles, -1 for cells outside the box).
-__device__ __forceinline__ void tile_slab_max(const ConfigDev &cf, const DomainDev &d, const double *buf,
-                                              int i0, int j0, int k0) {
+__device__ __forceinline__ void tile_slab_max(const ConfigDev &cf, unsigned long long *slab, const DomainDev &d,
+                                              const double *buf, int i0, int j0, int k0) {
     int t = threadIdx.x;
-    unsigned long long *sx = cf.slab, *sy = cf.slab + cf.nx, *sz = cf.slab + cf.nx + cf.ny;
+    unsigned long long *sx = slab, *sy = slab + cf.nx, *sz = slab + cf.nx + cf.ny;
     if (t < TX) {
         double m = 0.0;
         for (int e = 0; e < TY * TZ; ++e) m = fmax(m, buf[t * TY * TZ + e]);
@@ -325,6 +349,21 @@ __device__ __forceinline__ void tile_slab_max(const ConfigDev &cf, const DomainD
             for (int j = 0; j < TY; ++j) m = fmax(m, buf[(i * TY + j) * TZ + k]);
         if (k0 + k < d.nz) atomic_max_double(&sz[k0 + k], m);
     }
+}
+
+// Beam owning global tile t of the step: tile_off holds the exclusive prefix
+// sums of the beams' tile counts (beams that do not march have none).
+__device__ __forceinline__ int beam_of_tile(const int *tile_off, int nbeams, int t) {
+    int lo = 0, hi = nbeams - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (tile_off[mid] <= t) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ unsigned long long *beam_slab(const ConfigDev &cf, int b) {
+    return cf.slab + (size_t)b * (cf.nx + cf.ny + cf.nz);
 }
 
 // Single-precision stencil kernels (pdm1_stage_fp32.cu, compiled with fast math).

@@ -56,9 +56,15 @@ int set_error(int code, const std::string &msg) { return set_error(code, msg.c_s
 // ---------------------------------------------------------------------------
 // init: state at the start energy, S and spectrum for the first CFL
 // ---------------------------------------------------------------------------
-__global__ void init_kernel(const ConfigDev *cfp, Coeffs *co, MarchState *st, double *energies,
-                            double E0, double *U, int full_domain) {
+// One CTA per beam.  E0 < 0: each beam starts at its own E + window * sigma_E.
+__global__ void init_kernel(const ConfigDev *cfp, Coeffs *cos, MarchState *sts, double *energies,
+                            double E0, double ews, double *U, int full_domain) {
     const ConfigDev &cf = *cfp;
+    const int b = blockIdx.x;
+    const BeamDev &bm = cf.beams[b];
+    Coeffs *co = cos + b;
+    MarchState *st = sts + b;
+    if (E0 < 0.0) E0 = bm.E_beam + ews * bm.sigma_E;
     int t = threadIdx.x;
     if (t < cf.nm) {
         double s;
@@ -66,7 +72,7 @@ __global__ void init_kernel(const ConfigDev *cfp, Coeffs *co, MarchState *st, do
         co->S1[t] = s;
     }
     if (t == 0) {
-        co->ed_next = energy_density(cf, E0);
+        co->ed_next = energy_density(bm, E0);
         co->E_next = E0;
         st->E = E0;
         st->inv_bits = 0ull;
@@ -81,11 +87,57 @@ __global__ void init_kernel(const ConfigDev *cfp, Coeffs *co, MarchState *st, do
         st->pin_max = 0.0;
         st->cell_steps = 0.0;
         const bool moving = cf.moving && !full_domain;
-        st->dom = moving ? cf.init_box : make_domain(0, 0, 0, cf.nx, cf.ny, cf.nz, 1);
+        st->dom = moving ? bm.init_box : make_domain(0, 0, 0, cf.nx, cf.ny, cf.nz, 1);
         st->prev = st->dom;
-        st->Ua = moving ? cf.bufA : U;
+        st->Ua = moving ? cf.bufA + 4 * (size_t)b * cf.cap : U;
         st->Uprev = st->Ua;
-        if (energies) energies[0] = E0;
+        if (energies && cf.nbeams == 1) energies[0] = E0;
+        if (b == 0) {
+            cf.tile_off[0] = 0;
+            cf.tile_off[1] = 0;
+            cf.summary->active = cf.nbeams;
+            cf.summary->error = 0;
+        }
+    }
+}
+
+// Exclusive prefix sums of the marching beams' tile counts, and the summary
+// the host polls.  One CTA; beams are processed in chunks of blockDim.x.
+__global__ void __launch_bounds__(1024) tiles_kernel(const ConfigDev *cfp, const Coeffs *co,
+                                                     const MarchState *st) {
+    const ConfigDev &cf = *cfp;
+    __shared__ int scan[1024];
+    __shared__ int carry, n_active, err;
+    const int t = threadIdx.x;
+    if (t == 0) { carry = 0; n_active = 0; err = 0; }
+    __syncthreads();
+    for (int base = 0; base < cf.nbeams; base += blockDim.x) {
+        const int b = base + t;
+        int n = 0;
+        if (b < cf.nbeams) {
+            if (co[b].active) {
+                n = st[b].dom.ntiles;
+                atomicAdd(&n_active, 1);
+            }
+            if (st[b].error) atomicOr(&err, st[b].error);
+        }
+        scan[t] = n;
+        __syncthreads();
+        for (int o = 1; o < (int)blockDim.x; o <<= 1) {
+            int v = t >= o ? scan[t - o] : 0;
+            __syncthreads();
+            scan[t] += v;
+            __syncthreads();
+        }
+        if (b < cf.nbeams) cf.tile_off[b + 1] = carry + scan[t];
+        __syncthreads();
+        if (t == blockDim.x - 1) carry += scan[t];
+        __syncthreads();
+    }
+    if (t == 0) {
+        cf.tile_off[0] = 0;
+        cf.summary->active = n_active;
+        cf.summary->error = err;
     }
 }
 
@@ -94,9 +146,15 @@ __global__ void init_kernel(const ConfigDev *cfp, Coeffs *co, MarchState *st, do
 // ---------------------------------------------------------------------------
 constexpr int kEvalPerMat = 13;   // 5 stage energies + 8 Gauss points
 
-__global__ void __launch_bounds__(256) prologue_kernel(const ConfigDev *cfp, Coeffs *co,
-                                                       MarchState *st, double *energies) {
+// One CTA per beam.
+__global__ void __launch_bounds__(256) prologue_kernel(const ConfigDev *cfp, Coeffs *cos,
+                                                       MarchState *sts, double *energies) {
     const ConfigDev &cf = *cfp;
+    const int b = blockIdx.x;
+    const BeamDev &bm = cf.beams[b];
+    Coeffs *co = cos + b;
+    MarchState *st = sts + b;
+    if (cf.nbeams > 1) energies = nullptr;
     __shared__ double sE, sdE, sEn;
     __shared__ int sActive, sSlot;
     __shared__ double eS[kMaxMat][kEvalPerMat], eTr[kMaxMat][8], eNu[kMaxMat][8];
@@ -147,6 +205,12 @@ __global__ void __launch_bounds__(256) prologue_kernel(const ConfigDev *cfp, Coe
         }
         sE = E; sdE = dE; sEn = En; sActive = active; sSlot = slot;
         co->E = E; co->dE = dE; co->E_next = En; co->active = active; co->snap_slot = slot;
+        if (cf.nbeams == 1) {
+            cf.tile_off[0] = 0;
+            cf.tile_off[1] = active ? st->dom.ntiles : 0;
+            cf.summary->active = active;
+            cf.summary->error = st->error;
+        }
     }
     __syncthreads();
     if (!sActive) return;
@@ -187,10 +251,11 @@ __global__ void __launch_bounds__(256) prologue_kernel(const ConfigDev *cfp, Coe
     } else if (t >= 224 && t < 229) {
         int q = t - 224;
         const double ed_e[5] = {E, E - dE / 3.0, E - 2.0 * dE / 3.0, E - dE, E - dE};
-        double v = energy_density(cf, ed_e[q]);
+        double v = energy_density(bm, ed_e[q]);
         if (q < 4) co->ed[q] = v; else co->ed_next = v;
     }
     __syncthreads();
+    __shared__ double sTs[kMaxMat][4], sTn[kMaxMat][4];
     if (t < nm) {
         int m = t;
         co->S0[m] = eS[m][0];
@@ -201,37 +266,56 @@ __global__ void __launch_bounds__(256) prologue_kernel(const ConfigDev *cfp, Coe
         co->Sb[2][m] = eS[m][2];
         co->Sb[3][m] = eS[m][3];
         // optical depths, physics/scattering.py:267-306 and nuclear.py:202-233
-        double ts[4], tn[4];
+        // depth index: 0 -> dE/3, 1 -> dE/2, 2 -> 2dE/3, 3 -> dE
         const double width[4] = {dE / 3.0, 0.5 * dE, 2.0 * dE / 3.0, dE};
         for (int d = 0; d < 4; ++d) {
             double half = 0.5 * width[d];
-            ts[d] = 0.0;
-            tn[d] = 0.0;
+            double ts = 0.0, tn = 0.0;
             if (cf.scattering != PDM1_SCATTERING_OFF)
-                ts[d] = half * (eTr[m][2 * d] / eS[m][5 + 2 * d] + eTr[m][2 * d + 1] / eS[m][6 + 2 * d]);
+                ts = half * (eTr[m][2 * d] / eS[m][5 + 2 * d] + eTr[m][2 * d + 1] / eS[m][6 + 2 * d]);
             if (cf.nuclear)
-                tn[d] = half * (eNu[m][2 * d] / eS[m][5 + 2 * d] + eNu[m][2 * d + 1] / eS[m][6 + 2 * d]);
+                tn = half * (eNu[m][2 * d] / eS[m][5 + 2 * d] + eNu[m][2 * d + 1] / eS[m][6 + 2 * d]);
+            sTs[m][d] = ts;
+            sTn[m][d] = tn;
         }
-        // depth index: 0 -> dE/3, 1 -> dE/2, 2 -> 2dE/3, 3 -> dE
-        double u1 = cf.use_if ? ts[3] : 0.0, n1 = cf.use_if ? tn[3] : 0.0;
-        double u2 = cf.use_if ? ts[1] : 0.0, n2 = cf.use_if ? tn[1] : 0.0;
-        source_factor(u1, n1, false, co->c1p[m], co->c1c[m]);
-        source_factor(u1, n1, true, co->c1ip[m], co->c1ic[m]);
-        source_factor(u2, n2, false, co->c2p[m], co->c2c[m]);
-        source_factor(u2, n2, true, co->c2ip[m], co->c2ic[m]);
         co->fip[0][m] = 1.0;
         co->fic[0][m] = 1.0;
-        const int didx[4] = {0, 0, 2, 3};
-        for (int q = 1; q < 4; ++q) {
-            double a = cf.use_if ? ts[didx[q]] : 0.0, b = cf.use_if ? tn[didx[q]] : 0.0;
-            source_factor(a, b, true, co->fip[q][m], co->fic[q][m]);
+    }
+    __syncthreads();
+    // the 16 exponentials per material, one thread each (energy.py:273-310,
+    // 1168-1191): integrating factors C(tau) and C(tau)^-1 over dE and dE/2,
+    // the inverse factors of the inflow trace at dE/3, 2dE/3, dE, and the
+    // Strang half-step factors
+    if (t < nm * 16) {
+        const int m = t / 16, f = t % 16;
+        double ts = 0.0, tn = 0.0, out = 1.0;
+        if (f < 14) {
+            // which depth, and which factor of source_factor()
+            const int depth[14] = {3, 3, 3, 3, 1, 1, 1, 1, 0, 0, 2, 2, 3, 3};
+            const bool inv[14] = {false, false, true, true, false, false, true, true, true, true, true, true, true, true};
+            const bool cur[14] = {false, true, false, true, false, true, false, true, false, true, false, true, false, true};
+            if (cf.use_if) {
+                ts = sTs[m][depth[f]];
+                tn = sTn[m][depth[f]];
+            }
+            double sign = inv[f] ? 1.0 : -1.0;
+            double a = tn < kExpClamp ? tn : kExpClamp;
+            double tsum = tn + ts;
+            double b = tsum < kExpClamp ? tsum : kExpClamp;
+            out = dd_exp(sign * (cur[f] ? b : a));
+            double *dst[14] = {&co->c1p[m], &co->c1c[m], &co->c1ip[m], &co->c1ic[m],
+                               &co->c2p[m], &co->c2c[m], &co->c2ip[m], &co->c2ic[m],
+                               &co->fip[1][m], &co->fic[1][m], &co->fip[2][m], &co->fic[2][m],
+                               &co->fip[3][m], &co->fic[3][m]};
+            *dst[f] = out;
+        } else if (f == 14) {
+            double th = 0.5 * sTn[m][3];
+            co->hn[m] = (cf.strang && cf.nuclear) ? dd_exp(-(th < kExpClamp ? th : kExpClamp)) : 1.0;
+        } else {
+            double th = 0.5 * sTs[m][3];
+            co->hs[m] = (cf.strang && cf.scattering != PDM1_SCATTERING_OFF)
+                            ? dd_exp(-(th < kExpClamp ? th : kExpClamp)) : 1.0;
         }
-        // Strang half steps over the full dE (energy.py:1168-1191, 1194-1260)
-        double th = 0.5 * tn[3];
-        co->hn[m] = (cf.strang && cf.nuclear) ? dd_exp(-(th < kExpClamp ? th : kExpClamp)) : 1.0;
-        th = 0.5 * ts[3];
-        co->hs[m] = (cf.strang && cf.scattering != PDM1_SCATTERING_OFF)
-                        ? dd_exp(-(th < kExpClamp ? th : kExpClamp)) : 1.0;
     }
 }
 
@@ -265,9 +349,12 @@ __global__ void __launch_bounds__(NT) euler_finish_kernel(StageArgs a) {
             atomic_max_double(&cf.slab[cf.nx + lj], u[0]);
             atomic_max_double(&cf.slab[cf.nx + cf.ny + lk], u[0]);
         } else {
+            const BeamDev &bm = cf.beams[0];
             double phi_in = 0.0;
-            if (lk == 0 && d.inflow) phi_in = cf.spatial[(size_t)(d.i0 + li) * cf.ny + (d.j0 + lj)] * co.ed_next;
-            inv = fmax(inv, cfl_term(cf, u, co.S1[cf.ids[go]], lk == 0, phi_in, all_axes));
+            if (lk == 0 && d.inflow) phi_in = bm.spatial[(size_t)(d.i0 + li) * cf.ny + (d.j0 + lj)] * co.ed_next;
+            double s = co.S1[cf.ids[go]];
+            inv = fmax(inv, cf.fp32 ? cfl_term<float>(cf, bm.rf, u, s, lk == 0, phi_in, all_axes)
+                                    : cfl_term<double>(cf, bm.rf, u, s, lk == 0, phi_in, all_axes));
         }
     }
     if (!cf.moving) block_max_atomic(inv, &a.st->inv_bits);
@@ -278,10 +365,14 @@ __global__ void __launch_bounds__(NT) euler_finish_kernel(StageArgs a) {
 // step) or co->S_cfl / ed_cfl (moving box, every step).  With vacuum-aware
 // masks (energy.py:459-537) a direction counts only within 3 cells, along that
 // axis, of an active cell.
-__global__ void __launch_bounds__(NT) cfl_kernel(const ConfigDev *cfp, const Coeffs *co, MarchState *st,
+__global__ void __launch_bounds__(NT) cfl_kernel(const ConfigDev *cfp, const Coeffs *cos, MarchState *sts,
                                                  int use_box_coeffs) {
     const ConfigDev &cf = *cfp;
-    if (st->done) return;
+    const int b = blockIdx.y;
+    const Coeffs *co = cos + b;
+    MarchState *st = sts + b;
+    const BeamDev &bm = cf.beams[b];
+    if (st->done || st->error) return;
     const DomainDev d = st->dom;
     const double *U = st->Ua;
     const size_t N = (size_t)d.nx * d.ny * d.nz;
@@ -300,7 +391,7 @@ __global__ void __launch_bounds__(NT) cfl_kernel(const ConfigDev *cfp, const Coe
         int lk = (int)(o % d.nz), lj = (int)((o / d.nz) % d.ny), li = (int)(o / ((size_t)d.nz * d.ny));
         bool use[3] = {true, true, true};
         if (masks) {
-            const unsigned char *act = cf.active;
+            const unsigned char *act = cf.active + (size_t)b * cf.cap;
             for (int ax = 0; ax < 3; ++ax) {
                 int lo, hi, pos;
                 size_t stride;
@@ -313,8 +404,10 @@ __global__ void __launch_bounds__(NT) cfl_kernel(const ConfigDev *cfp, const Coe
             }
         }
         double phi_in = 0.0;
-        if (lk == 0 && d.inflow) phi_in = cf.spatial[(size_t)(d.i0 + li) * cf.ny + (d.j0 + lj)] * ed;
-        inv = fmax(inv, cfl_term(cf, u, S[cf.ids[global_cell(cf, d, li, lj, lk)]], lk == 0, phi_in, use));
+        if (lk == 0 && d.inflow) phi_in = bm.spatial[(size_t)(d.i0 + li) * cf.ny + (d.j0 + lj)] * ed;
+        double s = S[cf.ids[global_cell(cf, d, li, lj, lk)]];
+        inv = fmax(inv, cf.fp32 ? cfl_term<float>(cf, bm.rf, u, s, lk == 0, phi_in, use)
+                                : cfl_term<double>(cf, bm.rf, u, s, lk == 0, phi_in, use));
     }
     block_max_atomic(inv, &st->inv_bits);
 }
@@ -325,31 +418,41 @@ __global__ void __launch_bounds__(NT) cfl_kernel(const ConfigDev *cfp, const Coe
 
 // Start of the march: the initial box, the compact state copied from the
 // caller's full-grid U, and the slab maxima of that state.
+// blockIdx.y = beam; with Ufull == NULL the beams start from zero.
 __global__ void __launch_bounds__(NT) box_init_kernel(const ConfigDev *cfp, MarchState *st, const double *Ufull) {
     const ConfigDev &cf = *cfp;
-    const DomainDev d = cf.init_box;
+    const int b = blockIdx.y;
+    const DomainDev d = cf.beams[b].init_box;
     const size_t N = (size_t)d.nx * d.ny * d.nz, NG = (size_t)cf.nx * cf.ny * cf.nz;
+    double *Ua = cf.bufA + 4 * (size_t)b * cf.cap;
+    unsigned long long *slab = beam_slab(cf, b);
     for (size_t o = (size_t)blockIdx.x * NT + threadIdx.x; o < N; o += (size_t)gridDim.x * NT) {
         int lk = (int)(o % d.nz), lj = (int)((o / d.nz) % d.ny), li = (int)(o / ((size_t)d.nz * d.ny));
         size_t go = global_cell(cf, d, li, lj, lk);
         double u0 = 0.0;
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-            double v = Ufull[c * NG + go];
-            cf.bufA[c * N + o] = v;
+            double v = Ufull ? Ufull[c * NG + go] : 0.0;
+            Ua[c * N + o] = v;
             if (c == 0) u0 = v;
         }
-        atomic_max_double(&cf.slab[li], u0);
-        atomic_max_double(&cf.slab[cf.nx + lj], u0);
-        atomic_max_double(&cf.slab[cf.nx + cf.ny + lk], u0);
+        atomic_max_double(&slab[li], u0);
+        atomic_max_double(&slab[cf.nx + lj], u0);
+        atomic_max_double(&slab[cf.nx + cf.ny + lk], u0);
     }
 }
 
 // One CTA at the start of every step: desired_box (moving_active_domain.py:
 // 107-193) from the slab maxima of the current state and the inflow at the
 // step's energy; the switch to the new box; S and spectrum for the CFL.
-__global__ void __launch_bounds__(256) box_kernel(const ConfigDev *cfp, Coeffs *co, MarchState *st) {
+// One CTA per beam.
+__global__ void __launch_bounds__(256) box_kernel(const ConfigDev *cfp, Coeffs *cos, MarchState *sts) {
     const ConfigDev &cf = *cfp;
+    const int b = blockIdx.x;
+    const BeamDev &bm = cf.beams[b];
+    Coeffs *co = cos + b;
+    MarchState *st = sts + b;
+    unsigned long long *slab = beam_slab(cf, b);
     __shared__ double red[256];
     __shared__ double s_ed, s_scale;
     __shared__ int s_lo[3], s_hi[3];
@@ -360,7 +463,7 @@ __global__ void __launch_bounds__(256) box_kernel(const ConfigDev *cfp, Coeffs *
     if (s_done) return;
     const DomainDev d = st->dom;
     const double E = st->E;
-    if (t == 0) s_ed = energy_density(cf, E);
+    if (t == 0) s_ed = energy_density(bm, E);
     if (t < cf.nm) {
         double sv = 1.0;
         if (!stopping_power_dev(cf.mats[t], E, sv)) atomicOr(&st->error, ERR_DEV_RANGE);
@@ -368,7 +471,7 @@ __global__ void __launch_bounds__(256) box_kernel(const ConfigDev *cfp, Coeffs *
     }
     __syncthreads();
     const double ed = s_ed;
-    const unsigned long long *sx = cf.slab, *sy = cf.slab + cf.nx, *sz = cf.slab + cf.nx + cf.ny;
+    const unsigned long long *sx = slab, *sy = slab + cf.nx, *sz = slab + cf.nx + cf.ny;
     auto as_d = [](unsigned long long b) { return __longlong_as_double((long long)b); };
     // scale = max(max phi, max phi_in)   (phi_in only while the box touches z = 0)
     double m = 0.0;
@@ -376,7 +479,7 @@ __global__ void __launch_bounds__(256) box_kernel(const ConfigDev *cfp, Coeffs *
     if (d.inflow)
         for (int e = t; e < d.nx * d.ny; e += 256) {
             int i = e / d.ny, j = e % d.ny;
-            m = fmax(m, cf.spatial[(size_t)(d.i0 + i) * cf.ny + (d.j0 + j)] * ed);
+            m = fmax(m, bm.spatial[(size_t)(d.i0 + i) * cf.ny + (d.j0 + j)] * ed);
         }
     red[t] = m;
     __syncthreads();
@@ -398,31 +501,31 @@ __global__ void __launch_bounds__(256) box_kernel(const ConfigDev *cfp, Coeffs *
             bool act = as_d(sx[i]) > thr;
             if (!act && d.inflow)
                 for (int j = 0; j < d.ny && !act; ++j)
-                    act = cf.spatial[(size_t)(d.i0 + i) * cf.ny + (d.j0 + j)] * ed > thr;
+                    act = bm.spatial[(size_t)(d.i0 + i) * cf.ny + (d.j0 + j)] * ed > thr;
             if (act) { atomicMin(&s_lo[0], i); atomicMax(&s_hi[0], i); }
         }
         for (int j = t; j < d.ny; j += 256) {
             bool act = as_d(sy[j]) > thr;
             if (!act && d.inflow)
                 for (int i = 0; i < d.nx && !act; ++i)
-                    act = cf.spatial[(size_t)(d.i0 + i) * cf.ny + (d.j0 + j)] * ed > thr;
+                    act = bm.spatial[(size_t)(d.i0 + i) * cf.ny + (d.j0 + j)] * ed > thr;
             if (act) { atomicMin(&s_lo[1], j); atomicMax(&s_hi[1], j); }
         }
         for (int k = t; k < d.nz; k += 256) {
             bool act = as_d(sz[k]) > thr;
             if (!act && k == 0 && d.inflow)
                 for (int e = 0; e < d.nx * d.ny && !act; ++e)
-                    act = cf.spatial[(size_t)(d.i0 + e / d.ny) * cf.ny + (d.j0 + e % d.ny)] * ed > thr;
+                    act = bm.spatial[(size_t)(d.i0 + e / d.ny) * cf.ny + (d.j0 + e % d.ny)] * ed > thr;
             if (act) { atomicMin(&s_lo[2], k); atomicMax(&s_hi[2], k); }
         }
     }
     __syncthreads();
     // reset the slab maxima for this step's stage C
-    for (int e = t; e < cf.nx + cf.ny + cf.nz; e += 256) cf.slab[e] = 0ull;
+    for (int e = t; e < cf.nx + cf.ny + cf.nz; e += 256) slab[e] = 0ull;
     if (t == 0) {
         DomainDev nb;
         if (scale == 0.0 || s_hi[0] < 0 || s_hi[1] < 0 || s_hi[2] < 0) {
-            nb = cf.init_box;
+            nb = bm.init_box;
         } else {
             const int g = cf.guard;
             int ai0 = d.i0 + s_lo[0], ai1 = d.i0 + s_hi[0] + 1;
@@ -434,11 +537,16 @@ __global__ void __launch_bounds__(256) box_kernel(const ConfigDev *cfp, Coeffs *
             nb = make_domain(bi0, bj0, bk0, bi1 - bi0, bj1 - bj0, bk1 - bk0, bk0 == 0);
         }
         bool same = nb.i0 == d.i0 && nb.j0 == d.j0 && nb.k0 == d.k0 && nb.nx == d.nx && nb.ny == d.ny && nb.nz == d.nz;
+        if (!same && (size_t)nb.nx * nb.ny * nb.nz > cf.cap) {
+            st->error |= ERR_DEV_CAPACITY;   // the box outgrew the beam's buffers
+            same = true;
+        }
         st->reboxed = same ? 0 : 1;
         if (!same) {
             st->prev = d;
             st->Uprev = st->Ua;
-            st->Ua = st->Ua == cf.bufA ? cf.bufB : cf.bufA;
+            double *a_buf = cf.bufA + 4 * (size_t)b * cf.cap, *b_buf = cf.bufB + 4 * (size_t)b * cf.cap;
+            st->Ua = st->Ua == a_buf ? b_buf : a_buf;
             st->dom = nb;
         }
         st->inv_bits = 0ull;
@@ -448,7 +556,7 @@ __global__ void __launch_bounds__(256) box_kernel(const ConfigDev *cfp, Coeffs *
         double pin = 0.0;
         if (cf.vacuum_aware && nb.inflow)
             for (int e = 0; e < nb.nx * nb.ny; ++e)
-                pin = fmax(pin, cf.spatial[(size_t)(nb.i0 + e / nb.ny) * cf.ny + (nb.j0 + e % nb.ny)] * ed);
+                pin = fmax(pin, bm.spatial[(size_t)(nb.i0 + e / nb.ny) * cf.ny + (nb.j0 + e % nb.ny)] * ed);
         st->pin_max = pin;
     }
 }
@@ -456,9 +564,10 @@ __global__ void __launch_bounds__(256) box_kernel(const ConfigDev *cfp, Coeffs *
 // Copy the overlap of the previous box into the new one (zeros elsewhere,
 // moving_active_domain.py:196-232); for the vacuum-aware CFL also the max phi
 // of the new box.
-__global__ void __launch_bounds__(NT) rebox_kernel(const ConfigDev *cfp, MarchState *st) {
+__global__ void __launch_bounds__(NT) rebox_kernel(const ConfigDev *cfp, MarchState *sts) {
     const ConfigDev &cf = *cfp;
-    if (st->done) return;
+    MarchState *st = sts + blockIdx.y;
+    if (st->done || st->error) return;
     const DomainDev d = st->dom;
     const bool moved = st->reboxed != 0;
     if (!moved && !cf.vacuum_aware) return;
@@ -483,9 +592,14 @@ __global__ void __launch_bounds__(NT) rebox_kernel(const ConfigDev *cfp, MarchSt
 
 // Activity mask of the vacuum-aware CFL: phi above tol * max(phi, phi_in),
 // plus the inflow at the entrance layer (numerics/energy.py:496-537).
-__global__ void __launch_bounds__(NT) mask_kernel(const ConfigDev *cfp, const Coeffs *co, const MarchState *st) {
+__global__ void __launch_bounds__(NT) mask_kernel(const ConfigDev *cfp, const Coeffs *cos, const MarchState *sts) {
     const ConfigDev &cf = *cfp;
-    if (st->done) return;
+    const int b = blockIdx.y;
+    const Coeffs *co = cos + b;
+    const MarchState *st = sts + b;
+    const BeamDev &bm = cf.beams[b];
+    unsigned char *active = cf.active + (size_t)b * cf.cap;
+    if (st->done || st->error) return;
     const DomainDev d = st->dom;
     const double *Ua = st->Ua;
     const double scale = fmax(__longlong_as_double((long long)st->newmax_bits), st->pin_max);
@@ -497,8 +611,8 @@ __global__ void __launch_bounds__(NT) mask_kernel(const ConfigDev *cfp, const Co
         int lk = (int)(o % d.nz), lj = (int)((o / d.nz) % d.ny), li = (int)(o / ((size_t)d.nz * d.ny));
         bool act = Ua[o] > thr;
         if (lk == 0 && d.inflow)
-            act = act || cf.spatial[(size_t)(d.i0 + li) * cf.ny + (d.j0 + lj)] * ed > thr;
-        cf.active[o] = act ? 1 : 0;
+            act = act || bm.spatial[(size_t)(d.i0 + li) * cf.ny + (d.j0 + lj)] * ed > thr;
+        active[o] = act ? 1 : 0;
     }
 }
 
@@ -607,21 +721,27 @@ std::vector<double> pchip_slopes(const double *E, const double *v, int n) {
 struct pdm1_plan {
     pdm1_problem p{};
     ConfigDev cf{};
+    int nbeams = 1;
+    bool field = false;              // created by pdm1_field_plan_create
+    size_t cap = 0;
     ConfigDev *d_cf = nullptr;
-    Coeffs *d_co = nullptr;
-    MarchState *d_st = nullptr;
-    MarchState *h_st = nullptr;   // pinned
+    Coeffs *d_co = nullptr;         // nbeams
+    MarchState *d_st = nullptr;     // nbeams
+    MarchState *h_st = nullptr;     // pinned, nbeams
+    MarchSummary *d_sum = nullptr;
+    MarchSummary *h_sum = nullptr;  // pinned
+    BeamDev *d_beams = nullptr;
+    int *d_tile_off = nullptr;
     double *d_tables = nullptr;
     int32_t *d_ids = nullptr;
-    double *d_spatial = nullptr;
+    double *d_spatial = nullptr;    // nbeams x (nx, ny)
     double *d_targets = nullptr;
     double *d_U1 = nullptr, *d_U2 = nullptr, *d_V = nullptr, *d_q = nullptr;
     double *d_bufA = nullptr, *d_bufB = nullptr;   // moving box: compact-state ping-pong
     unsigned long long *d_slab = nullptr;
     unsigned char *d_active = nullptr;
     size_t workspace = 0;
-    std::vector<int32_t> h_ids;
-    std::vector<double> h_spatial;
+    std::vector<BeamDev> h_beams;   // host copy (device spatial pointers)
     // per material: [lo, hi] of the stopping-power, transport, nuclear tables
     std::vector<double> range[3][2];
     cudaStream_t own_stream = nullptr;
@@ -638,7 +758,7 @@ bool table_ok(const pdm1_table &t) {
     return true;
 }
 
-// Upload one table; return its TableView (device pointers).
+// Upload one table; return its TableView (device pointers patched later).
 TableView add_table(std::vector<double> &blob, std::vector<std::pair<size_t, int>> &fix,
                     const pdm1_table &t) {
     TableView v{};
@@ -665,10 +785,8 @@ int validate_problem(const pdm1_problem *p) {
     if (p->nx <= 0 || p->ny <= 0 || p->nz <= 0) return set_error(PDM1_ERR_ARGUMENT, "grid dimensions must be positive");
     if (p->nz < 4) return set_error(PDM1_ERR_ARGUMENT, "WENO-Z inflow extrapolation requires at least four z cells.");
     if (p->n_materials < 1 || p->n_materials > kMaxMat) return set_error(PDM1_ERR_ARGUMENT, "n_materials must be in 1..16");
-    if (!p->materials || !p->ids || !p->inflow_spatial) return set_error(PDM1_ERR_ARGUMENT, "NULL materials/ids/inflow");
+    if (!p->materials || !p->ids) return set_error(PDM1_ERR_ARGUMENT, "NULL materials/ids");
     if (!(p->dx > 0 && p->dy > 0 && p->dz > 0)) return set_error(PDM1_ERR_ARGUMENT, "spacings must be positive");
-    if (!(p->energy_spread > 0.0))
-        return set_error(PDM1_ERR_ARGUMENT, "Zero energy spread is not supported by the Gaussian inflow.");
     if (!(p->cfl > 0.0 && p->cfl <= 1.0)) return set_error(PDM1_ERR_ARGUMENT, "cfl must lie in (0, 1].");
     if (!(p->max_energy_step > 0.0)) return set_error(PDM1_ERR_ARGUMENT, "max_energy_step must be positive.");
     if (p->energy_scheme < 0 || p->energy_scheme > 2) return set_error(PDM1_ERR_UNSUPPORTED, "unknown energy scheme");
@@ -689,9 +807,17 @@ int validate_problem(const pdm1_problem *p) {
     return PDM1_OK;
 }
 
+int validate_beam(const pdm1_beam &b) {
+    if (!b.inflow_spatial) return set_error(PDM1_ERR_ARGUMENT, "beam inflow profile is NULL");
+    if (!(b.energy_spread > 0.0))
+        return set_error(PDM1_ERR_ARGUMENT, "Zero energy spread is not supported by the Gaussian inflow.");
+    if (!(b.energy > 0.0)) return set_error(PDM1_ERR_ARGUMENT, "beam energy must be positive");
+    return PDM1_OK;
+}
+
 bool is_close(double a, double b) { return std::fabs(a - b) <= 1e-8 + 1e-5 * std::fabs(b); }
 
-// Energy range the march will evaluate tables at: [energy_min, E_start]
+// Energy range the march will evaluate tables at: [e_lo, e_hi]
 int check_energy_range(const pdm1_plan *pl, double e_hi, double e_lo) {
     const pdm1_problem &p = pl->p;
     const bool used[3] = {true, p.scattering == PDM1_SCATTERING_WENTZEL, p.nuclear != 0};
@@ -710,6 +836,10 @@ int check_energy_range(const pdm1_plan *pl, double e_hi, double e_lo) {
     return PDM1_OK;
 }
 
+double beam_start_energy(const pdm1_plan *pl, int b) {
+    return pl->h_beams[b].E_beam + pl->p.energy_window_sigma * pl->h_beams[b].sigma_E;
+}
+
 StageArgs make_args(pdm1_plan *pl, double *dose, double *edep, double *snap) {
     StageArgs a{};
     a.cf = pl->d_cf;
@@ -725,17 +855,12 @@ StageArgs make_args(pdm1_plan *pl, double *dose, double *edep, double *snap) {
     return a;
 }
 
-int n_tiles(const pdm1_problem &p) {
-    return ((p.nx + TX - 1) / TX) * ((p.ny + TY - 1) / TY) * ((p.nz + TZ - 1) / TZ);
+// blocks of the per-cell kernels, per beam: enough for the largest domain
+int cell_blocks(const pdm1_plan *pl) {
+    size_t b = (pl->cap + NT - 1) / NT;
+    return (int)std::max<size_t>(1, std::min<size_t>(b, pl->nbeams > 1 ? 64 : 148 * 8));
 }
 
-int cell_blocks(const pdm1_problem &p) {
-    size_t n = (size_t)p.nx * p.ny * p.nz;
-    size_t b = (n + NT - 1) / NT;
-    return (int)std::min<size_t>(b, 148 * 8);
-}
-
-// Launch one energy step (prologue + stages) on `stream`; returns launches.
 // One stage launch in the plan's precision.
 void launch_stage(const pdm1_plan *pl, int mode, int grid, const StageArgs &a, cudaStream_t stream) {
     if (pl->p.precision == PDM1_FP32_FP64) {
@@ -753,58 +878,49 @@ void launch_stage(const pdm1_plan *pl, int mode, int grid, const StageArgs &a, c
 }
 
 // The moving box's per-step work ahead of the prologue: desired box, rebox,
-// activity mask, CFL bound over the new box.
+// activity mask, CFL bound over the new box -- for every beam at once.
 int launch_box_step(pdm1_plan *pl, cudaStream_t stream) {
     const pdm1_problem &p = pl->p;
-    box_kernel<<<1, 256, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st);
-    rebox_kernel<<<cell_blocks(p), NT, 0, stream>>>(pl->d_cf, pl->d_st);
+    const dim3 cells(cell_blocks(pl), pl->nbeams);
+    box_kernel<<<pl->nbeams, 256, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st);
+    rebox_kernel<<<cells, NT, 0, stream>>>(pl->d_cf, pl->d_st);
     int n = 3;
     if (p.vacuum_aware_cfl) {
-        mask_kernel<<<cell_blocks(p), NT, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st);
+        mask_kernel<<<cells, NT, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st);
         ++n;
     }
-    cfl_kernel<<<cell_blocks(p), NT, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, 1);
+    cfl_kernel<<<cells, NT, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, 1);
     return n;
 }
 
-int launch_step(pdm1_plan *pl, const StageArgs &a, cudaStream_t stream) {
-    const pdm1_problem &p = pl->p;
-    const int grid = pl->cf.grid_ctas;
-    prologue_kernel<<<1, 256, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, nullptr);
-    if (p.energy_scheme == PDM1_SCHEME_FORWARD_EULER) {
-        launch_stage(pl, MODE_EULER, grid, a, stream);
-        euler_finish_kernel<<<cell_blocks(p), NT, 0, stream>>>(a);
-        return 3;
-    }
-    launch_stage(pl, MODE_A, grid, a, stream);
-    launch_stage(pl, MODE_B, grid, a, stream);
-    launch_stage(pl, MODE_C, grid, a, stream);
-    return 4;
-}
-
-int launch_step_with_energies(pdm1_plan *pl, const StageArgs &a, double *energies, cudaStream_t stream,
-                              int slot) {
+// One energy step of every beam on `stream`; `slot` >= 0 brackets the stage
+// kernels with timing events.  Returns the kernels launched.
+int launch_step(pdm1_plan *pl, const StageArgs &a, double *energies, cudaStream_t stream, int slot,
+                bool box_step = true) {
     const pdm1_problem &p = pl->p;
     const int grid = pl->cf.grid_ctas;
     int launched = 0;
-    if (p.moving_active_domain) launched += launch_box_step(pl, stream);
-    prologue_kernel<<<1, 256, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, energies);
+    if (p.moving_active_domain && box_step) launched += launch_box_step(pl, stream);
+    prologue_kernel<<<pl->nbeams, 256, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, energies);
+    ++launched;
+    if (pl->nbeams > 1) {
+        tiles_kernel<<<1, 1024, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st);
+        ++launched;
+    }
     // external event nodes: real timestamps when the step is replayed from a graph
-    cudaEventRecordWithFlags(pl->ev[2 * slot], stream, cudaEventRecordExternal);
-    int n;
+    if (slot >= 0) cudaEventRecordWithFlags(pl->ev[2 * slot], stream, cudaEventRecordExternal);
     if (p.energy_scheme == PDM1_SCHEME_FORWARD_EULER) {
         launch_stage(pl, MODE_EULER, grid, a, stream);
-        n = 1;
+        ++launched;
     } else {
         launch_stage(pl, MODE_A, grid, a, stream);
         launch_stage(pl, MODE_B, grid, a, stream);
         launch_stage(pl, MODE_C, grid, a, stream);
-        n = 3;
+        launched += 3;
     }
-    cudaEventRecordWithFlags(pl->ev[2 * slot + 1], stream, cudaEventRecordExternal);
-    launched += n + 1;
+    if (slot >= 0) cudaEventRecordWithFlags(pl->ev[2 * slot + 1], stream, cudaEventRecordExternal);
     if (p.energy_scheme == PDM1_SCHEME_FORWARD_EULER) {
-        euler_finish_kernel<<<cell_blocks(p), NT, 0, stream>>>(a);
+        euler_finish_kernel<<<cell_blocks(pl), NT, 0, stream>>>(a);
         ++launched;
     }
     return launched;
@@ -823,26 +939,47 @@ int set_smem_attributes() {
     return PDM1_OK;
 }
 
-int device_error_status(const MarchState &st) {
-    if (st.error & ERR_DEV_RANGE) return set_error(PDM1_ERR_RANGE, "energy outside a coefficient table during the march");
-    if (st.error & ERR_DEV_MAXSTEPS) return set_error(PDM1_ERR_MAX_STEPS, "energies buffer shorter than the march");
-    if (st.error & ERR_DEV_NONFINITE) return set_error(PDM1_ERR_NONFINITE, "non-finite state or non-positive energy step during the march");
+int device_error_status(int error) {
+    if (error & ERR_DEV_RANGE) return set_error(PDM1_ERR_RANGE, "energy outside a coefficient table during the march");
+    if (error & ERR_DEV_MAXSTEPS) return set_error(PDM1_ERR_MAX_STEPS, "energies buffer shorter than the march");
+    if (error & ERR_DEV_NONFINITE) return set_error(PDM1_ERR_NONFINITE, "non-finite state or non-positive energy step during the march");
+    if (error & ERR_DEV_CAPACITY) return set_error(PDM1_ERR_ARGUMENT, "a beam's moving box outgrew the plan's box capacity");
     return PDM1_OK;
 }
 
-}  // namespace
+int device_error_status(const MarchState &st) { return device_error_status(st.error); }
 
-extern "C" {
+// Initial box of a beam from its inflow support (moving_active_domain.py:35-60).
+int initial_box(const pdm1_problem &p, const double *spatial, DomainDev &box) {
+    int ilo = -1, ihi = -1, jlo = -1, jhi = -1;
+    for (int i = 0; i < p.nx; ++i)
+        for (int j = 0; j < p.ny; ++j)
+            if (spatial[(size_t)i * p.ny + j] > 0.0) {
+                if (ilo < 0 || i < ilo) ilo = i;
+                if (i > ihi) ihi = i;
+                if (jlo < 0 || j < jlo) jlo = j;
+                if (j > jhi) jhi = j;
+            }
+    if (ilo < 0) return set_error(PDM1_ERR_NO_BEAM, "Beam inflow has empty transverse support.");
+    const int g = p.active_guard_cells;
+    int i0 = std::max(0, ilo - g), i1 = std::min(p.nx, ihi + 1 + g);
+    int j0 = std::max(0, jlo - g), j1 = std::min(p.ny, jhi + 1 + g);
+    int k1 = std::min(p.nz, 1 + g);
+    box = make_domain(i0, j0, 0, i1 - i0, j1 - j0, k1, 1);
+    if (k1 < 4) return set_error(PDM1_ERR_ARGUMENT, "WENO-Z inflow extrapolation requires at least four z cells.");
+    return PDM1_OK;
+}
 
-const char *pdm1_last_error(void) { return g_error; }
-const char *pdm1_version(void) { return "pdm1 0.1 sm_100a"; }
-
-void pdm1_plan_destroy(pdm1_plan *pl) {
+void destroy_plan(pdm1_plan *pl) {
     if (!pl) return;
     cudaFree(pl->d_cf);
     cudaFree(pl->d_co);
     cudaFree(pl->d_st);
     cudaFreeHost(pl->h_st);
+    cudaFree(pl->d_sum);
+    cudaFreeHost(pl->h_sum);
+    cudaFree(pl->d_beams);
+    cudaFree(pl->d_tile_off);
     cudaFree(pl->d_tables);
     cudaFree(pl->d_ids);
     cudaFree(pl->d_spatial);
@@ -862,22 +999,20 @@ void pdm1_plan_destroy(pdm1_plan *pl) {
     delete pl;
 }
 
-int pdm1_plan_create(const pdm1_problem *problem, pdm1_plan **out) {
-    if (!out) return set_error(PDM1_ERR_ARGUMENT, "out is NULL");
-    *out = nullptr;
-    int rc = validate_problem(problem);
-    if (rc) return rc;
-    rc = set_smem_attributes();
+// A plan for `nbeams` beams on one phantom; every beam's buffers hold `cap` cells.
+int create_plan(const pdm1_problem *problem, const pdm1_beam *beams, int nbeams, size_t cap, pdm1_plan **out) {
+    int rc = set_smem_attributes();
     if (rc) return rc;
     pdm1_plan *pl = new pdm1_plan();
     pl->p = *problem;
-    const pdm1_problem &p = pl->p;
-    size_t N = (size_t)p.nx * p.ny * p.nz;
-    pl->h_ids.assign(problem->ids, problem->ids + N);
-    pl->h_spatial.assign(problem->inflow_spatial, problem->inflow_spatial + (size_t)p.nx * p.ny);
-    pl->p.ids = pl->h_ids.data();
-    pl->p.inflow_spatial = pl->h_spatial.data();
     pl->p.materials = nullptr;   // tables are copied below; host pointers are not kept
+    pl->p.ids = nullptr;
+    pl->p.inflow_spatial = nullptr;
+    pl->nbeams = nbeams;
+    pl->cap = cap;
+    const pdm1_problem &p = pl->p;
+    const size_t N = (size_t)p.nx * p.ny * p.nz, NXY = (size_t)p.nx * p.ny;
+    const size_t B = (size_t)nbeams;
 
     std::vector<double> blob;
     std::vector<std::pair<size_t, int>> fix;
@@ -896,9 +1031,6 @@ int pdm1_plan_create(const pdm1_problem *problem, pdm1_plan **out) {
     cf.cfl = p.cfl;
     cf.max_dE = p.max_energy_step;
     cf.Emin = p.energy_min;
-    cf.E_beam = p.beam_energy;
-    cf.sigma_E = p.energy_spread;
-    cf.rf = dd_exp(-(p.angular_spread * p.angular_spread));
     for (int m = 0; m < p.n_materials; ++m) {
         const pdm1_material &mt = problem->materials[m];
         cf.mats[m].sp = add_table(blob, fix, mt.stopping_power);
@@ -912,7 +1044,22 @@ int pdm1_plan_create(const pdm1_problem *problem, pdm1_plan **out) {
             pl->range[q][1].push_back(tabs[q]->energy[tabs[q]->n_nodes - 1]);
         }
     }
-    auto fail = [&](int code) { pdm1_plan_destroy(pl); return code; };
+    auto fail = [&](int code) { destroy_plan(pl); return code; };
+    // beams: spectrum, angular factor, initial boxes
+    pl->h_beams.resize(B);
+    for (int b = 0; b < nbeams; ++b) {
+        BeamDev &bd = pl->h_beams[b];
+        bd.E_beam = beams[b].energy;
+        bd.sigma_E = beams[b].energy_spread;
+        bd.rf = dd_exp(-(beams[b].angular_spread * beams[b].angular_spread));
+        bd.init_box = make_domain(0, 0, 0, p.nx, p.ny, p.nz, 1);
+        if (p.moving_active_domain) {
+            rc = initial_box(p, beams[b].inflow_spatial, bd.init_box);
+            if (rc) return fail(rc);
+            if ((size_t)bd.init_box.nx * bd.init_box.ny * bd.init_box.nz > cap)
+                return fail(set_error(PDM1_ERR_ARGUMENT, "box capacity smaller than a beam's initial box"));
+        }
+    }
     cudaError_t e;
 #define ALLOC(ptr, bytes)                                                      \
     e = cudaMalloc((void **)&(ptr), (bytes));                                  \
@@ -922,24 +1069,28 @@ int pdm1_plan_create(const pdm1_problem *problem, pdm1_plan **out) {
     }
     ALLOC(pl->d_tables, blob.size() * sizeof(double));
     ALLOC(pl->d_cf, sizeof(ConfigDev));
-    ALLOC(pl->d_co, sizeof(Coeffs));
-    ALLOC(pl->d_st, sizeof(MarchState));
+    ALLOC(pl->d_co, B * sizeof(Coeffs));
+    ALLOC(pl->d_st, B * sizeof(MarchState));
+    ALLOC(pl->d_sum, sizeof(MarchSummary));
+    ALLOC(pl->d_beams, B * sizeof(BeamDev));
+    ALLOC(pl->d_tile_off, (B + 1) * sizeof(int));
     ALLOC(pl->d_ids, N * sizeof(int32_t));
-    ALLOC(pl->d_spatial, (size_t)p.nx * p.ny * sizeof(double));
+    ALLOC(pl->d_spatial, B * NXY * sizeof(double));
     ALLOC(pl->d_targets, 64 * sizeof(double));
-    ALLOC(pl->d_U1, 4 * N * sizeof(double));
-    ALLOC(pl->d_U2, 4 * N * sizeof(double));
-    ALLOC(pl->d_V, 4 * N * sizeof(double));
-    ALLOC(pl->d_q, N * sizeof(double));
+    ALLOC(pl->d_U1, B * 4 * cap * sizeof(double));
+    ALLOC(pl->d_U2, B * 4 * cap * sizeof(double));
+    ALLOC(pl->d_V, B * 4 * cap * sizeof(double));
+    ALLOC(pl->d_q, B * cap * sizeof(double));
     if (p.moving_active_domain) {
-        ALLOC(pl->d_bufA, 4 * N * sizeof(double));
-        ALLOC(pl->d_bufB, 4 * N * sizeof(double));
-        ALLOC(pl->d_slab, (size_t)(p.nx + p.ny + p.nz) * sizeof(unsigned long long));
-        ALLOC(pl->d_active, N);
+        ALLOC(pl->d_bufA, B * 4 * cap * sizeof(double));
+        ALLOC(pl->d_bufB, B * 4 * cap * sizeof(double));
+        ALLOC(pl->d_slab, B * (size_t)(p.nx + p.ny + p.nz) * sizeof(unsigned long long));
+        ALLOC(pl->d_active, B * cap);
     }
 #undef ALLOC
-    pl->workspace = (13 * N) * sizeof(double);
-    if (cudaMallocHost((void **)&pl->h_st, sizeof(MarchState)) != cudaSuccess ||
+    pl->workspace = B * cap * ((p.moving_active_domain ? 21 : 13) * sizeof(double) + (p.moving_active_domain ? 1 : 0));
+    if (cudaMallocHost((void **)&pl->h_st, B * sizeof(MarchState)) != cudaSuccess ||
+        cudaMallocHost((void **)&pl->h_sum, sizeof(MarchSummary)) != cudaSuccess ||
         cudaStreamCreateWithFlags(&pl->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&pl->ready, cudaEventDisableTiming) != cudaSuccess)
         return fail(set_error(PDM1_ERR_CUDA, "cudaMallocHost/stream/event creation failed"));
@@ -956,11 +1107,16 @@ int pdm1_plan_create(const pdm1_problem *problem, pdm1_plan **out) {
             v->slope = pl->d_tables + base + 2 * v->n;
         }
     }
+    for (int b = 0; b < nbeams; ++b) pl->h_beams[b].spatial = pl->d_spatial + (size_t)b * NXY;
     cf.ids = pl->d_ids;
-    cf.spatial = pl->d_spatial;
     cf.targets = pl->d_targets;
-    // moving active box: initial box from the inflow support (moving_active_domain.py:35-60)
+    cf.nbeams = nbeams;
+    cf.cap = cap;
+    cf.beams = pl->d_beams;
+    cf.tile_off = pl->d_tile_off;
+    cf.summary = pl->d_sum;
     cf.moving = p.moving_active_domain ? 1 : 0;
+    cf.fp32 = p.precision == PDM1_FP32_FP64 ? 1 : 0;
     cf.vacuum_aware = (p.moving_active_domain && p.vacuum_aware_cfl) ? 1 : 0;
     cf.guard = p.active_guard_cells;
     cf.tol = p.active_relative_tolerance;
@@ -968,47 +1124,37 @@ int pdm1_plan_create(const pdm1_problem *problem, pdm1_plan **out) {
     cf.bufB = pl->d_bufB;
     cf.slab = pl->d_slab;
     cf.active = pl->d_active;
-    if (p.moving_active_domain) {
-        int ilo = -1, ihi = -1, jlo = -1, jhi = -1;
-        for (int i = 0; i < p.nx; ++i)
-            for (int j = 0; j < p.ny; ++j)
-                if (pl->h_spatial[(size_t)i * p.ny + j] > 0.0) {
-                    if (ilo < 0 || i < ilo) ilo = i;
-                    if (i > ihi) ihi = i;
-                    if (jlo < 0 || j < jlo) jlo = j;
-                    if (j > jhi) jhi = j;
-                }
-        if (ilo < 0) return fail(set_error(PDM1_ERR_NO_BEAM, "Beam inflow has empty transverse support."));
-        const int g = p.active_guard_cells;
-        int i0 = std::max(0, ilo - g), i1 = std::min(p.nx, ihi + 1 + g);
-        int j0 = std::max(0, jlo - g), j1 = std::min(p.ny, jhi + 1 + g);
-        int k1 = std::min(p.nz, 1 + g);
-        cf.init_box = make_domain(i0, j0, 0, i1 - i0, j1 - j0, k1, 1);
-        if (k1 < 4)
-            return fail(set_error(PDM1_ERR_ARGUMENT, "WENO-Z inflow extrapolation requires at least four z cells."));
-    }
     {
         int dev = 0, sms = 148;
         if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        int tiles = make_domain(0, 0, 0, p.nx, p.ny, p.nz, 1).ntiles;
-        cf.grid_ctas = std::max(1, std::min(tiles, 2 * sms));
+        // resident CTAs per SM of the stage kernel: 2 in double, 3 in float
+        int per_sm = p.precision == PDM1_FP32_FP64 ? 3 : 2;
+        size_t tiles = (size_t)make_domain(0, 0, 0, p.nx, p.ny, p.nz, 1).ntiles * B;
+        cf.grid_ctas = (int)std::max<size_t>(1, std::min<size_t>(tiles, (size_t)per_sm * sms));
     }
-    if (cudaMemcpy(pl->d_tables, blob.data(), blob.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(pl->d_ids, pl->h_ids.data(), N * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(pl->d_spatial, pl->h_spatial.data(), (size_t)p.nx * p.ny * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(pl->d_cf, &cf, sizeof(ConfigDev), cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemset(pl->d_co, 0, sizeof(Coeffs)) != cudaSuccess)
-        return fail(set_error(PDM1_ERR_CUDA, "plan upload failed"));
+    bool ok = cudaMemcpy(pl->d_tables, blob.data(), blob.size() * sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemcpy(pl->d_ids, problem->ids, N * sizeof(int32_t), cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemcpy(pl->d_beams, pl->h_beams.data(), B * sizeof(BeamDev), cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemcpy(pl->d_cf, &cf, sizeof(ConfigDev), cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemset(pl->d_co, 0, B * sizeof(Coeffs)) == cudaSuccess &&
+              cudaMemset(pl->d_st, 0, B * sizeof(MarchState)) == cudaSuccess;
+    for (int b = 0; ok && b < nbeams; ++b)
+        ok = cudaMemcpy(pl->d_spatial + (size_t)b * NXY, beams[b].inflow_spatial, NXY * sizeof(double),
+                        cudaMemcpyHostToDevice) == cudaSuccess;
+    if (!ok) return fail(set_error(PDM1_ERR_CUDA, "plan upload failed"));
     *out = pl;
     return PDM1_OK;
 }
 
-size_t pdm1_plan_workspace_bytes(const pdm1_plan *pl) { return pl ? pl->workspace : 0; }
-
-static int march_impl(pdm1_plan *pl, double *U, double *dose, double *energies, int max_steps,
-                      const double *snap_targets, int n_snap, double *snap_out, double *snap_E_out,
-                      pdm1_march_info *info, pdm1_stream_t stream_, int step_limit) {
-    if (!pl || !U || !dose || !energies || max_steps < 1)
+// The march of every beam of a plan.  One beam: U (full grid, in/out), energies
+// and snapshots as numerics/energy.py:energy_march.  Several beams (a field):
+// U, energies and snapshots are not used, every beam starts from zero and the
+// dose is their sum.
+int march_impl(pdm1_plan *pl, double *U, double *dose, double *energies, int max_steps,
+               const double *snap_targets, int n_snap, double *snap_out, double *snap_E_out,
+               pdm1_march_info *info, pdm1_stream_t stream_, int step_limit, int *steps_per_beam) {
+    const bool field = pl->field;
+    if (!dose || max_steps < 1 || (!field && (!U || !energies)))
         return set_error(PDM1_ERR_ARGUMENT, "pdm1_march: NULL buffer or max_steps < 1");
     cudaStream_t stream = (cudaStream_t)stream_;
     if (stream == nullptr) {
@@ -1019,15 +1165,19 @@ static int march_impl(pdm1_plan *pl, double *U, double *dose, double *energies, 
         stream = pl->own_stream;
     }
     const pdm1_problem &p = pl->p;
-    double E0 = p.beam_energy + p.energy_window_sigma * p.energy_spread;
-    int rc = check_energy_range(pl, E0, p.energy_min);
+    const int B = pl->nbeams;
+    int rc;
+    double E0max = 0.0;
+    for (int b = 0; b < B; ++b) E0max = std::max(E0max, beam_start_energy(pl, b));
+    rc = check_energy_range(pl, E0max, p.energy_min);
     if (rc) return rc;
     // sorted unique targets in [energy_min, E0], descending (energy.py:1531-1538)
     std::vector<double> tg;
-    for (int i = 0; i < n_snap; ++i) {
-        double t = snap_targets[i];
-        if (p.energy_min <= t && t <= E0 && std::find(tg.begin(), tg.end(), t) == tg.end()) tg.push_back(t);
-    }
+    if (!field)
+        for (int i = 0; i < n_snap; ++i) {
+            double t = snap_targets[i];
+            if (p.energy_min <= t && t <= E0max && std::find(tg.begin(), tg.end(), t) == tg.end()) tg.push_back(t);
+        }
     std::sort(tg.begin(), tg.end(), [](double a, double b) { return a > b; });
     if (tg.size() > 64) return set_error(PDM1_ERR_ARGUMENT, "at most 64 snapshot energies");
     if (!tg.empty() && !snap_out) return set_error(PDM1_ERR_ARGUMENT, "snap_out is NULL");
@@ -1037,28 +1187,30 @@ static int march_impl(pdm1_plan *pl, double *U, double *dose, double *energies, 
     CUDA_TRY(cudaMemcpyAsync(pl->d_cf, &pl->cf, sizeof(ConfigDev), cudaMemcpyHostToDevice, stream));
     if (!tg.empty())
         CUDA_TRY(cudaMemcpyAsync(pl->d_targets, tg.data(), tg.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
-    size_t N = (size_t)p.nx * p.ny * p.nz;
+    const size_t N = (size_t)p.nx * p.ny * p.nz;
     CUDA_TRY(cudaMemsetAsync(dose, 0, N * sizeof(double), stream));
     if (p.moving_active_domain && !tg.empty())
         CUDA_TRY(cudaMemsetAsync(snap_out, 0, tg.size() * 4 * N * sizeof(double), stream));
     (void)cudaGetLastError();   // start from a clean launch-error state
-    init_kernel<<<1, 32, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, energies, E0, U, 0);
+    init_kernel<<<B, 32, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, field ? nullptr : energies, -1.0,
+                                      p.energy_window_sigma, U, 0);
     if (p.moving_active_domain) {
-        CUDA_TRY(cudaMemsetAsync(pl->d_slab, 0, (size_t)(p.nx + p.ny + p.nz) * sizeof(unsigned long long), stream));
-        box_init_kernel<<<cell_blocks(p), NT, 0, stream>>>(pl->d_cf, pl->d_st, U);
+        CUDA_TRY(cudaMemsetAsync(pl->d_slab, 0, (size_t)B * (p.nx + p.ny + p.nz) * sizeof(unsigned long long), stream));
+        box_init_kernel<<<dim3(cell_blocks(pl), B), NT, 0, stream>>>(pl->d_cf, pl->d_st, field ? nullptr : U);
     } else {
-        cfl_kernel<<<cell_blocks(p), NT, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, 0);
+        cfl_kernel<<<dim3(cell_blocks(pl), B), NT, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, 0);
     }
     CUDA_TRY(cudaGetLastError());
     int launches = 2;
     StageArgs a = make_args(pl, dose, nullptr, snap_out);
-    // capture a chunk of steps into a graph; replay until the device says done
+    double *step_energies = field ? nullptr : energies;
+    // capture a chunk of steps into a graph; replay until no beam marches
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int per_step = 0;
     bool use_graph = true;
     if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
-        for (int s = 0; s < kStepsPerGraph; ++s) per_step = launch_step_with_energies(pl, a, energies, stream, s);
+        for (int s = 0; s < kStepsPerGraph; ++s) per_step = launch_step(pl, a, step_energies, stream, s);
         if (cudaStreamEndCapture(stream, &graph) != cudaSuccess ||
             cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
             use_graph = false;
@@ -1067,7 +1219,7 @@ static int march_impl(pdm1_plan *pl, double *U, double *dose, double *energies, 
         use_graph = false;
     }
     (void)cudaGetLastError();   // a refused capture falls back to direct launches
-    int replays = 0, prev_step = 0, stage_launches = 0;
+    int replays = 0, chunk_steps = 0, stage_launches = 0;
     double stage_ms = 0.0;
     const int stages_per_step = p.energy_scheme == PDM1_SCHEME_FORWARD_EULER ? 1 : 3;
     for (;;) {
@@ -1075,77 +1227,151 @@ static int march_impl(pdm1_plan *pl, double *U, double *dose, double *energies, 
             CUDA_TRY(cudaGraphLaunch(exec, stream));
             replays++;
         } else {
-            for (int s = 0; s < kStepsPerGraph; ++s) per_step = launch_step_with_energies(pl, a, energies, stream, s);
+            for (int s = 0; s < kStepsPerGraph; ++s) per_step = launch_step(pl, a, step_energies, stream, s);
             CUDA_TRY(cudaGetLastError());
         }
-        CUDA_TRY(cudaMemcpyAsync(pl->h_st, pl->d_st, sizeof(MarchState), cudaMemcpyDeviceToHost, stream));
+        launches += kStepsPerGraph * per_step;
+        CUDA_TRY(cudaMemcpyAsync(pl->h_sum, pl->d_sum, sizeof(MarchSummary), cudaMemcpyDeviceToHost, stream));
         CUDA_TRY(cudaStreamSynchronize(stream));
-        int ran = pl->h_st->step - prev_step;   // steps of this chunk that did work
-        prev_step = pl->h_st->step;
-        launches += ran * per_step + (kStepsPerGraph - ran) * per_step;
-        for (int s = 0; s < ran && s < kStepsPerGraph; ++s) {
+        ++chunk_steps;
+        for (int s = 0; s < kStepsPerGraph; ++s) {
             float ms = 0.f;
             CUDA_TRY(cudaEventElapsedTime(&ms, pl->ev[2 * s], pl->ev[2 * s + 1]));
             stage_ms += ms;
         }
-        stage_launches += ran * stages_per_step;
-        if (pl->h_st->done || pl->h_st->error) break;
+        stage_launches += kStepsPerGraph * stages_per_step;
+        if (pl->h_sum->active == 0 || pl->h_sum->error) break;
     }
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
-    if (p.moving_active_domain) {
-        embed_kernel<<<cell_blocks(p), NT, 0, stream>>>(pl->d_cf, pl->d_st, U);
+    if (p.moving_active_domain && !field) {
+        embed_kernel<<<cell_blocks(pl), NT, 0, stream>>>(pl->d_cf, pl->d_st, U);
         CUDA_TRY(cudaGetLastError());
-        CUDA_TRY(cudaStreamSynchronize(stream));
         ++launches;
     }
-    rc = device_error_status(*pl->h_st);
+    CUDA_TRY(cudaMemcpyAsync(pl->h_st, pl->d_st, (size_t)B * sizeof(MarchState), cudaMemcpyDeviceToHost, stream));
+    CUDA_TRY(cudaStreamSynchronize(stream));
+    int err = 0, max_step = 0;
+    double cells = 0.0;
+    for (int b = 0; b < B; ++b) {
+        err |= pl->h_st[b].error;
+        max_step = std::max(max_step, pl->h_st[b].step);
+        cells += pl->h_st[b].cell_steps;
+        if (steps_per_beam) steps_per_beam[b] = pl->h_st[b].step;
+    }
+    rc = device_error_status(err);
     if (info) {
-        info->n_steps = pl->h_st->step;
-        info->n_snapshots = pl->h_st->taken;
-        info->final_state_valid = 1;
+        info->n_steps = field ? max_step : pl->h_st[0].step;
+        info->n_snapshots = field ? 0 : pl->h_st[0].taken;
+        info->final_state_valid = field ? 0 : 1;
         info->graph_replays = replays;
         info->kernel_launches = launches;
+        // the stage events bracket every step slot of every chunk, including
+        // slots after the last beam finished (those kernels return at once)
         info->stage_launches = stage_launches;
         info->stage_ms = stage_ms;
-        info->cell_steps = pl->h_st->cell_steps;
+        info->cell_steps = cells;
     }
-    if (snap_E_out)
-        for (int i = 0; i < pl->h_st->taken; ++i) snap_E_out[i] = tg[i];
+    if (snap_E_out && !field)
+        for (int i = 0; i < pl->h_st[0].taken; ++i) snap_E_out[i] = tg[i];
+    (void)chunk_steps;
     return rc;
 }
+
+}  // namespace
+
+extern "C" {
+
+const char *pdm1_last_error(void) { return g_error; }
+const char *pdm1_version(void) { return "pdm1 0.2 sm_100a"; }
+
+void pdm1_plan_destroy(pdm1_plan *pl) { destroy_plan(pl); }
+
+int pdm1_plan_create(const pdm1_problem *problem, pdm1_plan **out) {
+    if (!out) return set_error(PDM1_ERR_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    int rc = validate_problem(problem);
+    if (rc) return rc;
+    pdm1_beam beam{problem->beam_energy, problem->energy_spread, problem->angular_spread, problem->inflow_spatial};
+    rc = validate_beam(beam);
+    if (rc) return rc;
+    return create_plan(problem, &beam, 1, (size_t)problem->nx * problem->ny * problem->nz, out);
+}
+
+int pdm1_field_plan_create(const pdm1_problem *phantom, const pdm1_beam *beams, int n_beams,
+                           size_t box_capacity_cells, pdm1_plan **out) {
+    if (!out) return set_error(PDM1_ERR_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    int rc = validate_problem(phantom);
+    if (rc) return rc;
+    if (!beams || n_beams < 1) return set_error(PDM1_ERR_ARGUMENT, "a field needs at least one beam");
+    if (!phantom->moving_active_domain)
+        return set_error(PDM1_ERR_UNSUPPORTED, "a batched field marches every beam on its moving active box");
+    if (phantom->energy_scheme == PDM1_SCHEME_FORWARD_EULER)
+        return set_error(PDM1_ERR_UNSUPPORTED, "a batched field needs an SSPRK3 integrator");
+    for (int b = 0; b < n_beams; ++b) {
+        rc = validate_beam(beams[b]);
+        if (rc) return rc;
+    }
+    size_t N = (size_t)phantom->nx * phantom->ny * phantom->nz;
+    size_t cap = box_capacity_cells ? std::min(box_capacity_cells, N) : N;
+    rc = create_plan(phantom, beams, n_beams, cap, out);
+    if (rc == PDM1_OK) (*out)->field = true;
+    return rc;
+}
+
+int pdm1_field_march(pdm1_plan *pl, double *field_dose, int max_steps, int *steps_per_beam,
+                     pdm1_march_info *info, pdm1_stream_t stream) {
+    if (!pl) return set_error(PDM1_ERR_ARGUMENT, "plan is NULL");
+    if (!pl->field) return set_error(PDM1_ERR_ARGUMENT, "pdm1_field_march takes a field plan");
+    return march_impl(pl, nullptr, field_dose, nullptr, max_steps, nullptr, 0, nullptr, nullptr, info, stream,
+                      -1, steps_per_beam);
+}
+
+size_t pdm1_plan_workspace_bytes(const pdm1_plan *pl) { return pl ? pl->workspace : 0; }
 
 int pdm1_march(pdm1_plan *pl, double *U, double *dose, double *energies, int max_steps,
                const double *snap_targets, int n_snap, double *snap_out, double *snap_E_out,
                pdm1_march_info *info, pdm1_stream_t stream) {
+    if (!pl) return set_error(PDM1_ERR_ARGUMENT, "plan is NULL");
+    if (pl->field) return set_error(PDM1_ERR_ARGUMENT, "pdm1_march takes a one-beam plan; use pdm1_field_march");
     return march_impl(pl, U, dose, energies, max_steps, snap_targets, n_snap, snap_out, snap_E_out,
-                      info, stream, -1);
+                      info, stream, -1, nullptr);
 }
 
 int pdm1_march_steps(pdm1_plan *pl, double *U, double *dose, double *energies, int max_steps,
                      int step_limit, pdm1_march_info *info, pdm1_stream_t stream) {
+    if (!pl || pl->field) return set_error(PDM1_ERR_ARGUMENT, "pdm1_march_steps takes a one-beam plan");
     if (step_limit < 0) return set_error(PDM1_ERR_ARGUMENT, "step_limit must be >= 0");
     return march_impl(pl, U, dose, energies, max_steps, nullptr, 0, nullptr, nullptr, info, stream,
-                      step_limit);
+                      step_limit, nullptr);
+}
+
+// The building blocks act on the full grid of beam 0 of a one-beam plan.
+static int full_domain_state(pdm1_plan *pl, double *U, double energy, double forced_dE, cudaStream_t stream) {
+    MarchState st{};
+    st.E = energy;
+    st.forced_dE = forced_dE;
+    st.dom = make_domain(0, 0, 0, pl->p.nx, pl->p.ny, pl->p.nz, 1);
+    st.prev = st.dom;
+    st.Ua = U;
+    st.Uprev = U;
+    CUDA_TRY(cudaMemcpyAsync(pl->d_st, &st, sizeof st, cudaMemcpyHostToDevice, stream));
+    return PDM1_OK;
 }
 
 int pdm1_spatial_operator(pdm1_plan *pl, const double *U, double energy, const double *bc, double *rhs,
                           pdm1_stream_t stream_) {
     (void)cudaGetLastError();
-    if (!pl || !U || !rhs) return set_error(PDM1_ERR_ARGUMENT, "NULL argument");
+    if (!pl || !U || !rhs || pl->nbeams != 1) return set_error(PDM1_ERR_ARGUMENT, "NULL argument or field plan");
     cudaStream_t stream = (cudaStream_t)stream_;
-    {
-        MarchState st{};
-        st.dom = make_domain(0, 0, 0, pl->p.nx, pl->p.ny, pl->p.nz, 1);
-        st.prev = st.dom;
-        st.Ua = const_cast<double *>(U);
-        st.Uprev = st.Ua;
-        CUDA_TRY(cudaMemcpyAsync(pl->d_st, &st, sizeof st, cudaMemcpyHostToDevice, stream));
-    }
+    int rc = full_domain_state(pl, const_cast<double *>(U), energy, 0.0, stream);
+    if (rc) return rc;
     StageArgs a = make_args(pl, nullptr, nullptr, nullptr);
     a.rhs_out = rhs;
     a.bc_plane = bc;
-    double de = energy - pl->p.beam_energy, s = pl->p.energy_spread;
+    const BeamDev &bm = pl->h_beams[0];
+    double de = energy - bm.E_beam, s = bm.sigma_E;
     a.rhs_energy_density = dd_exp(-(de * de) / (2.0 * (s * s))) / (std::sqrt(2.0 * 3.141592653589793) * s);
     launch_stage(pl, MODE_RHS, pl->cf.grid_ctas, a, stream);
     CUDA_TRY(cudaGetLastError());
@@ -1155,12 +1381,13 @@ int pdm1_spatial_operator(pdm1_plan *pl, const double *U, double energy, const d
 
 int pdm1_energy_step(pdm1_plan *pl, const double *U, double energy, double *dE_out, pdm1_stream_t stream_) {
     (void)cudaGetLastError();
-    if (!pl || !U || !dE_out) return set_error(PDM1_ERR_ARGUMENT, "NULL argument");
+    if (!pl || !U || !dE_out || pl->nbeams != 1) return set_error(PDM1_ERR_ARGUMENT, "NULL argument or field plan");
     cudaStream_t stream = (cudaStream_t)stream_;
     int rc = check_energy_range(pl, energy, energy);
     if (rc) return rc;
-    init_kernel<<<1, 32, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, nullptr, energy, const_cast<double *>(U), 1);
-    cfl_kernel<<<cell_blocks(pl->p), NT, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, 0);
+    init_kernel<<<1, 32, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, nullptr, energy, pl->p.energy_window_sigma,
+                                      const_cast<double *>(U), 1);
+    cfl_kernel<<<dim3(cell_blocks(pl), 1), NT, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, 0);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(pl->h_st, pl->d_st, sizeof(MarchState), cudaMemcpyDeviceToHost, stream));
     CUDA_TRY(cudaStreamSynchronize(stream));
@@ -1176,7 +1403,7 @@ int pdm1_energy_step(pdm1_plan *pl, const double *U, double energy, double *dE_o
 
 int pdm1_advance(pdm1_plan *pl, double *U, double energy, double dE, double *edep, pdm1_stream_t stream_) {
     (void)cudaGetLastError();
-    if (!pl || !U || !edep || !(dE > 0.0)) return set_error(PDM1_ERR_ARGUMENT, "dE must be positive.");
+    if (!pl || !U || !edep || !(dE > 0.0) || pl->nbeams != 1) return set_error(PDM1_ERR_ARGUMENT, "dE must be positive.");
     cudaStream_t stream = (cudaStream_t)stream_;
     int rc = check_energy_range(pl, energy, energy - dE);
     if (rc) return rc;
@@ -1184,17 +1411,11 @@ int pdm1_advance(pdm1_plan *pl, double *U, double energy, double dE, double *ede
     pl->cf.max_steps = 1;
     pl->cf.step_limit = -1;
     CUDA_TRY(cudaMemcpyAsync(pl->d_cf, &pl->cf, sizeof(ConfigDev), cudaMemcpyHostToDevice, stream));
-    init_kernel<<<1, 32, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, nullptr, energy, U, 1);
-    MarchState st{};
-    st.E = energy;
-    st.forced_dE = dE;
-    st.dom = make_domain(0, 0, 0, pl->p.nx, pl->p.ny, pl->p.nz, 1);
-    st.prev = st.dom;
-    st.Ua = U;
-    st.Uprev = U;
-    CUDA_TRY(cudaMemcpyAsync(pl->d_st, &st, sizeof st, cudaMemcpyHostToDevice, stream));
+    init_kernel<<<1, 32, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, nullptr, energy, pl->p.energy_window_sigma, U, 1);
+    rc = full_domain_state(pl, U, energy, dE, stream);
+    if (rc) return rc;
     StageArgs a = make_args(pl, nullptr, edep, nullptr);
-    launch_step(pl, a, stream);
+    launch_step(pl, a, nullptr, stream, -1, false);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(pl->h_st, pl->d_st, sizeof(MarchState), cudaMemcpyDeviceToHost, stream));
     CUDA_TRY(cudaStreamSynchronize(stream));
@@ -1322,7 +1543,8 @@ void launch_step_plain(const pdm1_problem &p, ConfigDev *d_cf, Coeffs *d_co, Mar
     prologue_kernel<<<1, 256, 0, stream>>>(d_cf, d_co, d_st, energies);
     if (p.energy_scheme == PDM1_SCHEME_FORWARD_EULER) {
         stage_kernel<double, MODE_EULER><<<tiles, NT, stage_smem_bytes<double>(), stream>>>(a);
-        euler_finish_kernel<<<cell_blocks(p), NT, 0, stream>>>(a);
+        const size_t N = (size_t)p.nx * p.ny * p.nz;
+        euler_finish_kernel<<<(int)std::max<size_t>(1, std::min<size_t>((N + NT - 1) / NT, 148 * 8)), NT, 0, stream>>>(a);
         return;
     }
     stage_kernel<double, MODE_A><<<tiles, NT, stage_smem_bytes<double>(), stream>>>(a);
@@ -1349,6 +1571,9 @@ extern "C" int pdm1_march_noalloc(const pdm1_problem *problem, double *U, double
     const size_t o_cf = off; off = align256(off + sizeof(ConfigDev));
     const size_t o_co = off; off = align256(off + sizeof(Coeffs));
     const size_t o_st = off; off = align256(off + sizeof(MarchState));
+    const size_t o_bm = off; off = align256(off + sizeof(BeamDev));
+    const size_t o_to = off; off = align256(off + 2 * sizeof(int));
+    const size_t o_sm = off; off = align256(off + sizeof(MarchSummary));
     size_t o_tab[kMaxMat][3];
     for (int m = 0; m < p.n_materials; ++m) {
         const pdm1_table *tabs[3] = {&p.materials[m].stopping_power, &p.materials[m].transport,
@@ -1423,9 +1648,6 @@ extern "C" int pdm1_march_noalloc(const pdm1_problem *problem, double *U, double
     cf.cfl = p.cfl;
     cf.max_dE = p.max_energy_step;
     cf.Emin = p.energy_min;
-    cf.E_beam = p.beam_energy;
-    cf.sigma_E = p.energy_spread;
-    cf.rf = dd_exp(-(p.angular_spread * p.angular_spread));
     cf.max_steps = max_steps;
     cf.step_limit = -1;
     cf.n_targets = 0;
@@ -1436,7 +1658,17 @@ extern "C" int pdm1_march_noalloc(const pdm1_problem *problem, double *U, double
         cf.grid_ctas = std::max(1, std::min(make_domain(0, 0, 0, p.nx, p.ny, p.nz, 1).ntiles, 2 * sms));
     }
     cf.ids = reinterpret_cast<const int32_t *>(base + o_ids);
-    cf.spatial = reinterpret_cast<const double *>(base + o_sp);
+    cf.nbeams = 1;
+    cf.cap = N;
+    cf.beams = reinterpret_cast<const BeamDev *>(base + o_bm);
+    cf.tile_off = reinterpret_cast<int *>(base + o_to);
+    cf.summary = reinterpret_cast<MarchSummary *>(base + o_sm);
+    BeamDev bm{};
+    bm.E_beam = p.beam_energy;
+    bm.sigma_E = p.energy_spread;
+    bm.rf = dd_exp(-(p.angular_spread * p.angular_spread));
+    bm.spatial = reinterpret_cast<const double *>(base + o_sp);
+    bm.init_box = make_domain(0, 0, 0, p.nx, p.ny, p.nz, 1);
     for (int m = 0; m < p.n_materials; ++m) {
         const pdm1_material &mt = p.materials[m];
         const pdm1_table *tabs[3] = {&mt.stopping_power, &mt.transport, &mt.nuclear};
@@ -1458,6 +1690,7 @@ extern "C" int pdm1_march_noalloc(const pdm1_problem *problem, double *U, double
     CUDA_TRY(cudaMemcpyAsync(base + o_ids, p.ids, N * sizeof(int32_t), cudaMemcpyHostToDevice, stream));
     CUDA_TRY(cudaMemcpyAsync(base + o_sp, p.inflow_spatial, (size_t)p.nx * p.ny * sizeof(double), cudaMemcpyHostToDevice, stream));
     CUDA_TRY(cudaMemcpyAsync(d_cf, &cf, sizeof cf, cudaMemcpyHostToDevice, stream));
+    CUDA_TRY(cudaMemcpyAsync(base + o_bm, &bm, sizeof bm, cudaMemcpyHostToDevice, stream));
     // the array keeps the previous call's contents: clear what must start at zero
     CUDA_TRY(cudaMemsetAsync(d_co, 0, sizeof(Coeffs), stream));
     CUDA_TRY(cudaMemsetAsync(d_st, 0, sizeof(MarchState), stream));
@@ -1474,8 +1707,9 @@ extern "C" int pdm1_march_noalloc(const pdm1_problem *problem, double *U, double
     a.dose = dose;
 
     (void)cudaGetLastError();
-    init_kernel<<<1, 32, 0, stream>>>(d_cf, d_co, d_st, energies, E0, U, 1);
-    cfl_kernel<<<cell_blocks(p), NT, 0, stream>>>(d_cf, d_co, d_st, 0);
+    init_kernel<<<1, 32, 0, stream>>>(d_cf, d_co, d_st, energies, E0, p.energy_window_sigma, U, 1);
+    const int cblocks = (int)std::max<size_t>(1, std::min<size_t>((N + NT - 1) / NT, 148 * 8));
+    cfl_kernel<<<dim3(cblocks, 1), NT, 0, stream>>>(d_cf, d_co, d_st, 0);
     CUDA_TRY(cudaGetLastError());
     int launches = 2 + 3 * p.n_materials, chunks = 0;
     const int per_step = p.energy_scheme == PDM1_SCHEME_FORWARD_EULER ? 3 : 4;

@@ -11,8 +11,6 @@ namespace pdm1 {
 template <typename T, int MODE>
 __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 3) stage_kernel(StageArgs a) {
     const ConfigDev &cf = *a.cf;
-    const Coeffs &co = *a.co;
-    if (MODE != MODE_RHS && !co.active) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *smem = reinterpret_cast<T *>(smem_raw);
     __shared__ double slab_buf[NT];   // moving box: phi of the tile's cells
@@ -21,17 +19,29 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 3) stage
     s.Y = s.X + 4 * SX;
     s.Z = s.Y + 4 * SY;
     s.F = s.Z + 4 * SZ;
-    const DomainDev d = a.st->dom;
-    double *const Ua = a.st->Ua;
-    const int nx = d.nx, ny = d.ny, nz = d.nz;
-    const size_t N = (size_t)nx * ny * nz;
     const int tid = threadIdx.x;
-    const double *src = (MODE == MODE_B) ? a.U1 : (MODE == MODE_C ? a.U2 : Ua);
     const bool unit = cf.unit_speeds != 0;
     const bool all_axes[3] = {true, true, true};
     double cta_inv = 0.0;
+    // tiles of all marching beams, back to back (one beam: its domain's tiles)
+    const int total = MODE == MODE_RHS ? a.st[0].dom.ntiles : cf.tile_off[cf.nbeams];
 
-    for (int tile = blockIdx.x; tile < d.ntiles; tile += gridDim.x) {
+    for (int gt = blockIdx.x; gt < total; gt += gridDim.x) {
+        const int b = (MODE == MODE_RHS || cf.nbeams == 1) ? 0 : beam_of_tile(cf.tile_off, cf.nbeams, gt);
+        const int tile = MODE == MODE_RHS ? gt : gt - cf.tile_off[b];
+        const Coeffs &co = a.co[b];
+        MarchState &stb = a.st[b];
+        const BeamDev &bm = cf.beams[b];
+        const DomainDev d = stb.dom;
+        double *const Ua = stb.Ua;
+        const int nx = d.nx, ny = d.ny, nz = d.nz;
+        const size_t N = (size_t)nx * ny * nz;
+        const size_t boff = (size_t)b * cf.cap;
+        double *const U1 = a.U1 + 4 * boff;
+        double *const U2 = a.U2 + 4 * boff;
+        double *const Vb = a.V + 4 * boff;
+        double *const qb = a.qpart + boff;
+        const double *src = (MODE == MODE_B) ? U1 : (MODE == MODE_C ? U2 : Ua);
         const int tz = tile % d.tiles_z, ty = (tile / d.tiles_z) % d.tiles_y, tx = tile / (d.tiles_z * d.tiles_y);
         const int i0 = tx * TX, j0 = ty * TY, k0 = tz * TZ;
 
@@ -67,7 +77,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 3) stage
                 int j = e % TY, i = (e / TY) % TX, c = e / (TX * TY);
                 int li = i0 + i, lj = j0 + j;
                 if (li >= nx || lj >= ny) continue;
-                T ui = T(boundary_value<MODE>(a, cf, co, d, c, li, lj));
+                T ui = T(boundary_value<MODE>(a, cf, bm, co, d, c, li, lj));
                 const T *col = &s.X[((c * (TX + 6) + (i + 3)) * TY + j) * TZ];
                 T u0 = col[0], u1 = col[1], u2 = col[2], u3 = col[3];
                 T *z = &s.Z[((c * TX + i) * TY + j) * 6];
@@ -160,25 +170,25 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 3) stage
                     project(u1[0], u1[1], u1[2], u1[3]);
 #pragma unroll
                     for (int c = 0; c < 4; ++c) {
-                        a.U1[c * N + o] = u1[c];
-                        a.V[c * N + o] = v1[c];
+                        U1[c * N + o] = u1[c];
+                        Vb[c * N + o] = v1[c];
                     }
                     double q0 = un[0] * s0, q1 = u1[0] * co.S1[m];
-                    a.qpart[o] = 1.0 / 6.0 * q0 + 1.0 / 6.0 * q1;
+                    qb[o] = 1.0 / 6.0 * q0 + 1.0 / 6.0 * q1;
                 } else if (MODE == MODE_B) {
                     double u2[4];
 #pragma unroll
                     for (int c = 0; c < 4; ++c) {
                         double r = L[c] * (c == 0 ? co.c1ip[m] : co.c1ic[m]);
-                        r = (r * dE + a.V[c * N + o]) * 0.25;
+                        r = (r * dE + Vb[c * N + o]) * 0.25;
                         double v = 0.75 * (s0 * un[c]) + r;
-                        a.V[c * N + o] = v;
+                        Vb[c * N + o] = v;
                         double w = v * (c == 0 ? co.c2p[m] : co.c2c[m]);
                         u2[c] = w / co.S2[m];
                     }
                     project(u2[0], u2[1], u2[2], u2[3]);
 #pragma unroll
-                    for (int c = 0; c < 4; ++c) a.U2[c * N + o] = u2[c];
+                    for (int c = 0; c < 4; ++c) U2[c * N + o] = u2[c];
                 } else {
                     double unew[4];
                     double ed;
@@ -186,7 +196,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 3) stage
 #pragma unroll
                         for (int c = 0; c < 4; ++c) {
                             double r = L[c] * (c == 0 ? co.c2ip[m] : co.c2ic[m]);
-                            r = (r * dE + a.V[c * N + o]) * (2.0 / 3.0);
+                            r = (r * dE + Vb[c * N + o]) * (2.0 / 3.0);
                             double v = 1.0 / 3.0 * (s0 * un[c]) + r;
                             double w = v * (c == 0 ? co.c1p[m] : co.c1c[m]);
                             unew[c] = w / co.S1[m];
@@ -194,9 +204,9 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 3) stage
                         project(unew[0], unew[1], unew[2], unew[3]);
                         double u2c = sizeof(T) == sizeof(double)
                                          ? double(s.X[((0 * (TX + 6) + (i + 3)) * TY + j) * TZ + k])
-                                         : a.U2[o];
+                                         : U2[o];
                         double q2 = u2c * co.S2[m];
-                        ed = dE * (a.qpart[o] + 2.0 / 3.0 * q2);
+                        ed = dE * (qb[o] + 2.0 / 3.0 * q2);
                     } else {   // forward Euler, numerics/energy.py:663-722
 #pragma unroll
                         for (int c = 0; c < 4; ++c) {
@@ -214,7 +224,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 3) stage
 #pragma unroll
                             for (int c = 1; c < 4; ++c) unew[c] *= co.hs[m];
                     }
-                    double *dst = MODE == MODE_C ? Ua : a.U1;
+                    double *dst = MODE == MODE_C ? Ua : U1;
                     bool finite = true;
 #pragma unroll
                     for (int c = 0; c < 4; ++c) {
@@ -222,9 +232,9 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 3) stage
                         finite = finite && isfinite(unew[c]);
                     }
                     // a non-finite state ends the march with PDM1_ERR_NONFINITE
-                    if (!finite) atomicOr(&a.st->error, ERR_DEV_NONFINITE);
+                    if (!finite) atomicOr(&stb.error, ERR_DEV_NONFINITE);
                     if (a.edep) a.edep[o] = ed;
-                    else a.dose[go] += ed * kMevToJoule / cf.mats[m].density;
+                    else atomicAdd(&a.dose[go], ed * kMevToJoule / cf.mats[m].density);
                     if (MODE == MODE_C) {
                         if (co.snap_slot >= 0 && a.snap) {
                             const size_t NG = (size_t)cf.nx * cf.ny * cf.nz;
@@ -235,8 +245,8 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 3) stage
                         if (!cf.moving) {
                             double phi_in = 0.0;
                             if (lk == 0 && d.inflow)
-                                phi_in = cf.spatial[(size_t)(d.i0 + li) * cf.ny + (d.j0 + lj)] * co.ed_next;
-                            double v = cfl_term(cf, unew, co.S1[m], lk == 0, phi_in, all_axes);
+                                phi_in = bm.spatial[(size_t)(d.i0 + li) * cf.ny + (d.j0 + lj)] * co.ed_next;
+                            double v = cfl_term<T>(cf, bm.rf, unew, co.S1[m], lk == 0, phi_in, all_axes);
                             cta_inv = fmax(cta_inv, v);
                         }
                         phi_new = unew[0];
@@ -247,11 +257,11 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 3) stage
         if (MODE == MODE_C && cf.moving) {
             slab_buf[tid] = phi_new;
             __syncthreads();
-            tile_slab_max(cf, d, slab_buf, i0, j0, k0);
+            tile_slab_max(cf, beam_slab(cf, b), d, slab_buf, i0, j0, k0);
         }
         __syncthreads();   // shared memory is reused by the next tile
     }
-    if (MODE == MODE_C && !cf.moving) block_max_atomic(cta_inv, &a.st->inv_bits);
+    if (MODE == MODE_C && !cf.moving) block_max_atomic(cta_inv, &a.st[0].inv_bits);
 }
 
 }  // namespace pdm1

@@ -56,55 +56,64 @@ def _check_supported(config) -> None:
         raise ValueError("Zero energy spread is not supported by the Gaussian inflow.")
 
 
+def _problem_struct(config, material_map, grid, spatial, precision=None):
+    """The pdm1_problem of a configuration, and the host arrays it points into."""
+    _check_supported(config)
+    num, phys, beam = config.numerics, config.physics, config.beam
+    shape = tuple(int(n) for n in grid.shape)
+    ids = np.ascontiguousarray(_to_numpy(material_map.ids), dtype=np.int32)
+    if ids.shape != shape:
+        raise ValueError(f"material ids have shape {ids.shape}, expected {shape}")
+    spatial = np.ascontiguousarray(_to_numpy(spatial), dtype=np.float64)
+    materials = tuple(material_map.materials)
+    keep = [ids, spatial]
+    mats = (_native.Material * len(materials))()
+    for k, m in enumerate(materials):
+        t = material_tables(m.value)
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in
+                (t.sp_energy, t.sp_value, t.tr_energy, t.tr_value, t.nuc_energy, t.nuc_value)]
+        keep += arrs
+        ptr = [a.ctypes.data_as(C.POINTER(C.c_double)) for a in arrs]
+        mats[k] = _native.Material(_native.Table(len(arrs[0]), ptr[0], ptr[1]),
+                                   _native.Table(len(arrs[2]), ptr[2], ptr[3]),
+                                   _native.Table(len(arrs[4]), ptr[4], ptr[5]),
+                                   t.density, t.radiation_length)
+    keep.append(mats)
+    if precision is None:
+        accel = getattr(config, "accel", None)
+        precision = accel.precision.name if accel is not None else "FP64"
+    p = _native.Problem()
+    p.nx, p.ny, p.nz = shape
+    p.dx, p.dy, p.dz = float(grid.dx), float(grid.dy), float(grid.dz)
+    p.n_materials = len(materials)
+    p.materials = mats
+    p.ids = ids.ctypes.data_as(C.POINTER(C.c_int32))
+    p.inflow_spatial = spatial.ctypes.data_as(C.POINTER(C.c_double))
+    p.beam_energy, p.energy_spread = beam.energy, beam.energy_spread
+    p.angular_spread = beam.angular_spread
+    p.scattering = _SCATTER[phys.scattering.name]
+    p.nuclear = int(bool(phys.nuclear))
+    p.interpolation = _INTERP[phys.coefficient_interpolation.name]
+    p.energy_scheme = _SCHEME[num.energy_scheme.name]
+    p.wave_speeds = _SPEEDS[num.wave_speeds.name]
+    p.max_energy_step, p.cfl = num.max_energy_step, num.cfl
+    p.energy_min, p.energy_window_sigma = num.energy_min, num.energy_window_sigma
+    p.moving_active_domain = int(bool(num.moving_active_domain))
+    p.vacuum_aware_cfl = int(bool(num.vacuum_aware_cfl))
+    p.active_guard_cells = int(num.active_guard_cells)
+    p.active_relative_tolerance = math.exp(-0.5 * num.active_truncation_sigma ** 2)
+    p.precision = _PRECISION[precision]
+    return p, keep, materials
+
+
 class M1Plan:
     """One beam on one phantom, resident on the GPU (a ``pdm1_plan``)."""
 
     def __init__(self, config, material_map, grid, inflow, precision: str | None = None):
-        _check_supported(config)
-        num, phys, beam = config.numerics, config.physics, config.beam
+        p, keep, materials = _problem_struct(config, material_map, grid, inflow.spatial, precision)
+        num, beam = config.numerics, config.beam
         self.shape = tuple(int(n) for n in grid.shape)
         self.config = config
-        ids = np.ascontiguousarray(_to_numpy(material_map.ids), dtype=np.int32)
-        if ids.shape != self.shape:
-            raise ValueError(f"material ids have shape {ids.shape}, expected {self.shape}")
-        spatial = np.ascontiguousarray(_to_numpy(inflow.spatial), dtype=np.float64)
-        materials = tuple(material_map.materials)
-        keep = [ids, spatial]
-        mats = (_native.Material * len(materials))()
-        for k, m in enumerate(materials):
-            t = material_tables(m.value)
-            arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in
-                    (t.sp_energy, t.sp_value, t.tr_energy, t.tr_value, t.nuc_energy, t.nuc_value)]
-            keep += arrs
-            ptr = [a.ctypes.data_as(C.POINTER(C.c_double)) for a in arrs]
-            mats[k] = _native.Material(_native.Table(len(arrs[0]), ptr[0], ptr[1]),
-                                       _native.Table(len(arrs[2]), ptr[2], ptr[3]),
-                                       _native.Table(len(arrs[4]), ptr[4], ptr[5]),
-                                       t.density, t.radiation_length)
-        if precision is None:
-            accel = getattr(config, "accel", None)
-            precision = accel.precision.name if accel is not None else "FP64"
-        p = _native.Problem()
-        p.nx, p.ny, p.nz = self.shape
-        p.dx, p.dy, p.dz = float(grid.dx), float(grid.dy), float(grid.dz)
-        p.n_materials = len(materials)
-        p.materials = mats
-        p.ids = ids.ctypes.data_as(C.POINTER(C.c_int32))
-        p.inflow_spatial = spatial.ctypes.data_as(C.POINTER(C.c_double))
-        p.beam_energy, p.energy_spread = beam.energy, beam.energy_spread
-        p.angular_spread = beam.angular_spread
-        p.scattering = _SCATTER[phys.scattering.name]
-        p.nuclear = int(bool(phys.nuclear))
-        p.interpolation = _INTERP[phys.coefficient_interpolation.name]
-        p.energy_scheme = _SCHEME[num.energy_scheme.name]
-        p.wave_speeds = _SPEEDS[num.wave_speeds.name]
-        p.max_energy_step, p.cfl = num.max_energy_step, num.cfl
-        p.energy_min, p.energy_window_sigma = num.energy_min, num.energy_window_sigma
-        p.moving_active_domain = int(bool(num.moving_active_domain))
-        p.vacuum_aware_cfl = int(bool(num.vacuum_aware_cfl))
-        p.active_guard_cells = int(num.active_guard_cells)
-        p.active_relative_tolerance = math.exp(-0.5 * num.active_truncation_sigma ** 2)
-        p.precision = _PRECISION[precision]
         self.materials = materials
         self.start_energy = beam.energy + num.energy_window_sigma * beam.energy_spread
         h = C.c_void_p()
@@ -220,6 +229,75 @@ class M1Plan:
             self._h, E.ctypes.data_as(C.POINTER(C.c_double)), len(E),
             out.ctypes.data_as(C.POINTER(C.c_double))))
         return out
+
+
+class FieldPlan:
+    """A spot-scanning field: many pencil beams on one phantom in one launch.
+
+    Every beam marches on its own moving active box with its own energy and
+    CFL step (``pdm1_field_plan_create`` / ``pdm1_field_march``); the field
+    dose is the sum of the beams' doses.  ``config`` gives the phantom,
+    physics, numerics and precision; ``beams`` are ``Beam`` objects.
+    """
+
+    def __init__(self, config, material_map, grid, beams, box_capacity_cells: int = 0):
+        from dataclasses import replace
+        from .boundary import transverse_profile
+        num = config.numerics
+        if not num.moving_active_domain:
+            config = type(config)(geometry=config.geometry, beam=config.beam, physics=config.physics,
+                                  numerics=replace(num, moving_active_domain=True),
+                                  accel=getattr(config, "accel", None) or type(config.accel)())
+        beams = list(beams)
+        if not beams:
+            raise ValueError("a field needs at least one beam")
+        profiles = [np.ascontiguousarray(b.n_protons * transverse_profile(b, grid), dtype=np.float64)
+                    for b in beams]
+        p, keep, materials = _problem_struct(config, material_map, grid, profiles[0])
+        descs = (_native.BeamDesc * len(beams))()
+        for k, (b, prof) in enumerate(zip(beams, profiles)):
+            if b.energy_spread == 0:
+                raise ValueError("Zero energy spread is not supported by the Gaussian inflow.")
+            descs[k] = _native.BeamDesc(b.energy, b.energy_spread, b.angular_spread,
+                                        prof.ctypes.data_as(C.POINTER(C.c_double)))
+        keep += profiles + [descs]
+        self.shape = tuple(int(n) for n in grid.shape)
+        self.n_beams = len(beams)
+        self.config = config
+        h = C.c_void_p()
+        _native.check(_native.lib().pdm1_field_plan_create(C.byref(p), descs, len(beams),
+                                                           int(box_capacity_cells), C.byref(h)))
+        self._h = h
+        self._keep = keep
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _native.lib().pdm1_plan_destroy(h)
+            self._h = None
+
+    __del__ = close
+
+    @property
+    def workspace_bytes(self) -> int:
+        return int(_native.lib().pdm1_plan_workspace_bytes(self._h))
+
+    def march_device(self, dose, max_steps=2_000_000):
+        """Field dose into the device tensor ``dose``; returns steps per beam."""
+        import torch
+        steps = (C.c_int * self.n_beams)()
+        info = _native.MarchInfo()
+        _native.check(_native.lib().pdm1_field_march(
+            self._h, C.c_void_p(dose.data_ptr()), int(max_steps), steps, C.byref(info),
+            C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        self.last_info = info
+        return list(steps)
+
+    def march(self, max_steps=2_000_000):
+        torch = _torch()
+        dose = torch.empty(self.shape, dtype=torch.float64, device="cuda")
+        steps = self.march_device(dose, max_steps)
+        return dose, steps
 
 
 def energy_march(U: Any, material_map, grid, inflow, config, xp=None,

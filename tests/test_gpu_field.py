@@ -1,0 +1,93 @@
+"""Batched spot-scanning fields: many beams in one launch per stage.
+
+Beams do not interact, so a field march must give, for every beam, the same
+energy steps as that beam marched alone on its moving box, and a field dose
+equal to the sum of the single-beam doses (the FP64 atomic accumulation
+across beams only changes the summation order).
+"""
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from dataclasses import replace
+
+from proton_dose_m1_b200 import Accel, Beam, Box, Geometry, Numerics, Physics, SolverConfig
+from proton_dose_m1_b200 import metrics
+from proton_dose_m1_b200.enums import EnergyScheme, Material, Precision, Scattering
+from proton_dose_m1_b200.numerics.boundary import BeamInflow
+from proton_dose_m1_b200.numerics.energy import FieldPlan, M1Plan
+from proton_dose_m1_b200.numerics.grid import Grid
+from proton_dose_m1_b200.physics.materials import MaterialMap
+
+pytestmark = pytest.mark.gpu
+
+
+def phantom(precision=Precision.FP64, moving=True):
+    geo = Geometry(size=(0.032, 0.032, 0.06), resolution=(32, 32, 60),
+                   objects=[Box(-0.016, 0.0, -0.016, 0.016, 0.02, 0.03, Material.BONE_COMPACT),
+                            Box(0.004, 0.016, -0.016, 0.0, 0.035, 0.05, Material.LUNG)])
+    return SolverConfig(geometry=geo, beam=Beam(energy=60.0),
+                        physics=Physics(scattering=Scattering.WENTZEL, nuclear=True),
+                        numerics=Numerics(energy_scheme=EnergyScheme.IF_SSPRK3, cfl=0.9, max_energy_step=0.5,
+                                          moving_active_domain=moving),
+                        accel=Accel(precision=precision))
+
+
+BEAMS = [Beam(n_protons=1e6, energy=55.0, energy_spread=1.0, sigma=(0.003, 0.003), center=(-0.006, -0.004)),
+         Beam(n_protons=2e6, energy=62.0, energy_spread=0.8, sigma=(0.002, 0.004), center=(0.005, 0.003)),
+         Beam(n_protons=1e6, energy=48.0, energy_spread=1.2, sigma=(0.004, 0.002), center=(0.0, 0.008),
+              angular_spread=0.03),
+         Beam(n_protons=5e5, energy=66.0, energy_spread=1.0, sigma=(0.0025, 0.0025), center=(0.008, -0.007))]
+
+
+def single(cfg, beam):
+    c = SolverConfig(geometry=cfg.geometry, beam=beam, physics=cfg.physics, numerics=cfg.numerics,
+                     accel=cfg.accel)
+    grid = Grid.from_geometry(c.geometry)
+    mm = MaterialMap.from_geometry(c.geometry, grid)
+    plan = M1Plan(c, mm, grid, BeamInflow.from_beam(beam, grid))
+    _, dose, E, _ = plan.march(None)
+    return dose.cpu().numpy(), len(E) - 1
+
+
+def field(cfg, beams, cap=0):
+    grid = Grid.from_geometry(cfg.geometry)
+    mm = MaterialMap.from_geometry(cfg.geometry, grid)
+    fp = FieldPlan(cfg, mm, grid, beams, box_capacity_cells=cap)
+    dose, steps = fp.march()
+    return dose.cpu().numpy(), steps, grid
+
+
+def test_field_equals_sum_of_single_beams():
+    cfg = phantom()
+    singles = [single(cfg, b) for b in BEAMS]
+    dose, steps, _ = field(cfg, BEAMS)
+    assert steps == [n for _, n in singles]
+    total = sum(d for d, _ in singles)
+    assert np.abs(dose - total).max() <= 1e-12 * total.max()
+
+
+def test_field_of_one_beam_is_the_moving_march():
+    cfg = phantom()
+    d1, n1 = single(cfg, BEAMS[1])
+    dose, steps, _ = field(cfg, BEAMS[1:2])
+    assert steps == [n1]
+    np.testing.assert_array_equal(dose, d1)
+
+
+def test_field_rejects_boxes_beyond_capacity():
+    cfg = phantom()
+    with pytest.raises(ValueError, match="capacity"):
+        field(cfg, BEAMS, cap=2000)
+
+
+def test_fp32_field_gate_against_plain_fp64():
+    """FP32 stencil + moving boxes + batching against the plain FP64 full-domain
+    march of every beam, summed."""
+    plain = sum(single(phantom(moving=False), b)[0] for b in BEAMS)
+    dose, steps, grid = field(phantom(Precision.FP32_FP64), BEAMS)
+    score = metrics.compare(dose, plain, grid)
+    assert score["gamma_1pct_1mm_pass_percent"] >= 99.5, score
+    assert abs(score["maximum_dose_relative_difference"]) <= 0.005, score
