@@ -9,9 +9,13 @@ region).  ``--impl reference`` times the CPU restatement of the reference
 algorithm (oracle/) on the host cores.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-       [--workload slab80]
+       [--workload slab80|water40|field256|pelvis1024]
 Under torchrun (N > 1) every rank marches its own spots (independent pencil
 beams, no data-path collective) and rank 0 prints one JSON line.
+
+Field workloads (field256: 256 spots on a 128x128x256 ellipsoid phantom;
+pelvis1024: 1024 spots on a 256x256x320 pelvis phantom): a "step" is one
+march of the whole field, batched; ``value`` is spots/s of the field.
 """
 
 from __future__ import annotations
@@ -33,10 +37,27 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "spots/s at gamma1%/1mm>=99.5% vs plain FP64 GPU path; stage-kernel HBM GB/s"
-# Algorithmic DRAM bytes per cell-step of the FP64 march: U^n read by each of
-# the three stages (96), three stage states written (96) and two read back
-# (64), dose read+write (16), material id per stage (3).
-ALG_BYTES_PER_CELL_STEP = {"FP64": 275.0, "FP32_FP64": 147.0}
+# Algorithmic DRAM bytes per cell-step of the march: U^n read by each of the
+# three stages (96), three stage states written (96) and two read back (64),
+# dose read+write (16), material id per stage (3).  The state and the stage
+# states are stored in double in both precision modes (the FP32 form converts
+# on load), so the count is the same for both.
+ALG_BYTES_PER_CELL_STEP = {"FP64": 275.0, "FP32_FP64": 275.0}
+FIELDS = {
+    "field256": dict(phantom="ellipsoid", seed=4, n_side=16, pitch=5e-3, energy=(70.0, 220.0),
+                     gate_beams=4,
+                     desc="256 spots (16x16 at 5 mm, E~U[70,220] MeV, sigma~U[2,6] mm, sigma_E 1 MeV, "
+                          "1e6 protons) on a 128x128x256 @1 mm water phantom with 6-12 seeded ellipsoids "
+                          "of water/lung/bone/muscle; Wentzel-VI + nuclear, WENO-Z/HLL/IF-SSPRK3, "
+                          "cfl 0.9, max dE 0.5"),
+    "pelvis1024": dict(phantom="pelvis", seed=5, n_side=32, pitch=3e-3, energy=(70.0, 230.0),
+                       gate_beams=3,
+                       desc="1024 spots (32x32 at 3 mm, E~U[70,230] MeV, sigma~U[2,6] mm, sigma_E 1 MeV, "
+                            "1e6 protons) on a 256x256x320 @1 mm synthetic pelvis (water/muscle body, "
+                            "ADIPOSE_SYNTH shell = water scaled to 950 kg/m3, bone ring, two bone femoral "
+                            "heads, water outside); Wentzel-VI + nuclear, WENO-Z/HLL/IF-SSPRK3, cfl 0.9, "
+                            "max dE 0.5"),
+}
 
 
 def workload(name: str):
@@ -62,6 +83,33 @@ def workload(name: str):
         desc = "40x40x200 @1 mm water, 150 MeV, sigma 3 mm, sigma_E 1 MeV, CSDA only"
         return cfg, desc
     raise SystemExit(f"unknown workload {name}")
+
+
+def field_workload(name: str):
+    """(config template, material map, grid, beams, description) of a field workload."""
+    from proton_dose_m1_b200 import Numerics, Physics, SolverConfig, phantoms
+    from proton_dose_m1_b200.enums import EnergyScheme, Scattering
+    from proton_dose_m1_b200.numerics.grid import Grid
+    from proton_dose_m1_b200.physics.materials import MaterialMap
+    w = FIELDS[name]
+    if w["phantom"] == "ellipsoid":
+        geo, _ = phantoms.ellipsoid_phantom(w["seed"])
+    else:
+        geo, _ = phantoms.pelvis_phantom(w["seed"])
+    beams = phantoms.spot_grid(w["seed"], w["n_side"], w["pitch"], energy_mev=w["energy"])
+    cfg = SolverConfig(geometry=geo, beam=beams[0],
+                       physics=Physics(scattering=Scattering.WENTZEL, nuclear=True),
+                       numerics=Numerics(energy_scheme=EnergyScheme.IF_SSPRK3, cfl=0.9, max_energy_step=0.5))
+    grid = Grid.from_geometry(geo)
+    return cfg, MaterialMap.from_geometry(geo, grid), grid, beams, w["desc"]
+
+
+def gate_sample(beams, n):
+    """``n`` spots spread over the field's energy range (quantiles of energy)."""
+    order = sorted(range(len(beams)), key=lambda k: beams[k].energy)
+    if n >= len(beams):
+        return order
+    return [order[int(round(q * (len(order) - 1)))] for q in np.linspace(0.1, 0.9, n)]
 
 
 def problem(cfg):
@@ -135,23 +183,41 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def cpu_baseline(cfg, n_steps_full: int, target_s: float = 12.0):
-    """Oracle (CPU restatement) on a bounded sample of the same workload."""
+def static_config(cfg, beam=None):
+    """``cfg`` on the full domain (no moving box), optionally with another beam."""
+    from dataclasses import replace
+    from proton_dose_m1_b200 import SolverConfig
+    return SolverConfig(geometry=cfg.geometry, beam=beam or cfg.beam, physics=cfg.physics,
+                        numerics=replace(cfg.numerics, moving_active_domain=False))
+
+
+def oracle_cell_rate(cfg, material_map=None, target_s: float = 10.0, min_steps: int = 1):
+    """Cell-steps per second of the oracle (CPU restatement, all host threads)
+    on full-domain energy steps of ``cfg``: a bounded timing sample."""
     from oracle.oracle import OracleProblem
-    threads = os.cpu_count() or 1
-    orc = OracleProblem(cfg)
+    orc = OracleProblem(static_config(cfg), material_map)
+    n_cells = float(np.prod(orc.shape))
     t0 = time.perf_counter()
     _, _, done = orc.march_steps(1)
-    t1 = time.perf_counter()
-    per_step = t1 - t0
-    k = max(1, min(50, int(target_s / max(per_step, 1e-3))))
+    first = time.perf_counter() - t0
+    k = max(min_steps, min(50, int(target_s / max(first, 1e-3))))
     t0 = time.perf_counter()
     _, _, done = orc.march_steps(k)
-    per_step = (time.perf_counter() - t0) / done
-    return {"value": 1.0 / (per_step * n_steps_full), "unit": "spots/s", "cores": threads,
+    dt = time.perf_counter() - t0
+    return done * n_cells / dt, done, dt
+
+
+def cpu_baseline(cfg, cell_steps_per_unit: float, units: int = 1, material_map=None,
+                 what: str = "one spot"):
+    """Oracle throughput on a bounded sample, expressed in spots/s of the
+    workload: the oracle's cell-step rate (measured on full-domain energy
+    steps) divided by the cell-steps the moving-box march of the workload
+    takes (the reference's fastest CPU mode marches the same boxes)."""
+    rate, done, dt = oracle_cell_rate(cfg, material_map)
+    return {"value": units * rate / cell_steps_per_unit, "unit": "spots/s", "cores": os.cpu_count() or 1,
             "kind": "port",
-            "sample": f"first {done} of {n_steps_full} energy steps of one spot, "
-                      f"{per_step:.3f} s/step, extrapolated to the full march"}
+            "sample": f"{done} full-domain energy steps in {dt:.1f} s -> {rate:.3e} cell-steps/s; "
+                      f"{what} = {cell_steps_per_unit:.4e} moving-box cell-steps"}
 
 
 def estimated_step_count(cfg) -> int:
@@ -173,32 +239,50 @@ def estimated_step_count(cfg) -> int:
     return n
 
 
-def run_reference(args, cfg, desc, rank, world):
+# Cell-steps of the moving-box march of each workload (per spot for single-spot
+# workloads, per field for fields): the work the reference's fastest CPU mode
+# (moving active box) does, measured by the GPU march.
+MOVING_CELL_STEPS = {}
+
+
+def run_reference(args, rank, world):
+    """The oracle (CPU restatement of the reference path) on the host cores."""
     if rank != 0:
         return
     from oracle.oracle import OracleProblem
     threads = os.cpu_count() or 1
-    n_full = estimated_step_count(cfg)
-    orc = OracleProblem(cfg)
-    sample_steps = 3
+    if args.workload in FIELDS:
+        cfg, mm, grid, beams, desc = field_workload(args.workload)
+        units = len(beams)
+        cfg = static_config(cfg, beams[gate_sample(beams, 1)[0]])
+    else:
+        (cfg, desc), mm, units = workload(args.workload), None, 1
+    cell_steps = MOVING_CELL_STEPS.get(args.workload)
+    orc = OracleProblem(static_config(cfg), mm)
+    n_cells = float(np.prod(orc.shape))
+    if cell_steps is None:   # no moving-box measurement: the full-domain march
+        cell_steps = units * n_cells * estimated_step_count(cfg)
+        basis = "full-domain march (estimated step count)"
+    else:
+        basis = "moving-box march (measured cell-steps)"
     for _ in range(args.warmup):
         orc.march_steps(1)
-    times = []
+    rates = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        _, _, done = orc.march_steps(sample_steps)
-        times.append((time.perf_counter() - t0) / done)
-    per_step = statistics.median(times)
-    value = 1.0 / (per_step * n_full)
+        _, _, done = orc.march_steps(2)
+        rates.append(done * n_cells / (time.perf_counter() - t0))
+    rate = statistics.median(rates)
+    value = units * rate / cell_steps
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "spots/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": per_step * n_full * 1e3, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": units / value * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded phantom, no dataset)",
         "config": {"workload": args.workload, "description": desc},
         "cpu_baseline": {"value": value, "unit": "spots/s", "cores": threads, "kind": "port",
-                         "sample": f"{sample_steps} of ~{n_full} energy steps per timed step, "
-                                   "extrapolated to one full spot"},
+                         "sample": f"2 full-domain energy steps per timed step ({rate:.3e} cell-steps/s), "
+                                   f"scaled to the {basis}: {cell_steps:.4e} cell-steps for {units} spot(s)"},
         "e2e": {"value": value, "unit": "spots/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -342,7 +426,148 @@ def run_ours(args, cfg, desc, rank, world, local_rank):
         "clocks": clocks.summary(),
     }
     if not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(cfg, n_steps)
+        line["cpu_baseline"] = cpu_baseline(cfg, cell_steps / max(args.steps, 1))
+    print(json.dumps(line), flush=True)
+
+
+def run_field(args, rank, world, local_rank):
+    """A batched spot-scanning field: all spots in one batched march."""
+    import torch
+    import torch.distributed as dist
+    from proton_dose_m1_b200 import metrics
+    from proton_dose_m1_b200.numerics.energy import FieldPlan, M1Plan, field_march
+    from proton_dose_m1_b200.numerics.boundary import BeamInflow
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    cfg, mm, grid, beams, desc = field_workload(args.workload)
+    # weak scaling: every rank marches the whole field's spot list on its own GPU
+    run_cfg = accelerated_config(cfg)
+    stream = torch.cuda.Stream(device=dev)
+    with torch.cuda.stream(stream):
+        plan = FieldPlan(run_cfg, mm, grid, beams)
+        dose = torch.empty(grid.shape, dtype=torch.float64, device=dev)
+        for _ in range(args.warmup):
+            plan.march_device(dose)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        stage_ms, stage_launches, launches, cell_steps, max_box = 0.0, 0, 0, 0.0, 0.0
+        with ClockSampler(local_rank) as clocks:
+            start.record(stream)
+            for _ in range(args.steps):
+                steps = plan.march_device(dose)
+                info = plan.last_info
+                stage_ms += info.stage_ms
+                stage_launches += info.stage_launches
+                cell_steps += info.cell_steps
+                launches += info.kernel_launches
+                max_box = max(max_box, info.max_box_cells)
+            end.record(stream)
+            torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        ms = start.elapsed_time(end)
+        if world > 1:
+            t = torch.tensor([ms], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        n_spots = len(beams)
+        value = world * n_spots * args.steps / (ms / 1e3)
+        workspace = plan.workspace_bytes
+        waves, cap = len(plan.waves), plan.cap
+        plan.close()
+
+        gate = None
+        plain_spots_per_s = None
+        if rank == 0:
+            # gate: a sample of the field's spots, accelerated (batched) vs the
+            # plain FP64 full-domain path one spot at a time
+            sample = gate_sample(beams, FIELDS[args.workload]["gate_beams"])
+            sub = [beams[k] for k in sample]
+            sp = FieldPlan(run_cfg, mm, grid, sub)
+            dose_acc = torch.empty_like(dose)
+            sp.march_device(dose_acc)
+            sp.close()
+            dose_plain = torch.zeros_like(dose)
+            d1 = torch.empty_like(dose)
+            U = torch.empty((4, *grid.shape), dtype=torch.float64, device=dev)
+            energies = torch.empty(200_001, dtype=torch.float64, device=dev)
+            plain_ms = 0.0
+            for b in sub:
+                pc = static_config(cfg, b)
+                pplan = M1Plan(pc, mm, grid, BeamInflow.from_beam(b, grid))
+                U.zero_()
+                s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                s0.record(stream)
+                pplan.march_device(U, d1, energies)
+                s1.record(stream)
+                torch.cuda.synchronize()
+                plain_ms += s0.elapsed_time(s1)
+                dose_plain += d1
+                pplan.close()
+            del U
+            plain_spots_per_s = len(sub) / (plain_ms / 1e3)
+            score = metrics.compare(dose_acc, dose_plain, grid)
+            gate = {"vs": f"plain FP64 GPU path (full domain, one spot at a time) on {len(sub)} spots "
+                          f"of the field (energy quantiles: {[round(b.energy, 1) for b in sub]} MeV)",
+                    "gamma_1pct_1mm_pass_percent": score["gamma_1pct_1mm_pass_percent"],
+                    "max_dose_relative_difference": score["maximum_dose_relative_difference"],
+                    "max_abs_difference_over_max": score["max_abs_difference_over_max"],
+                    "passed": bool(score["gamma_1pct_1mm_pass_percent"] >= 99.5
+                                   and abs(score["maximum_dose_relative_difference"]) <= 0.005)}
+            del dose_acc, dose_plain, d1
+
+    # end to end through the public API with host buffers
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    dose_h, _ = field_march(run_cfg, mm, grid, beams)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    h2d = (mm.ids.nbytes + len(beams) * grid.shape[0] * grid.shape[1] * 8)
+    d2h = dose_h.nbytes
+
+    if rank != 0:
+        return
+    peak, peak_kind = measured_peaks()
+    alg_total = cell_steps * ALG_BYTES_PER_CELL_STEP["FP32_FP64"]
+    achieved = alg_total / (stage_ms / 1e3) / 1e9 if stage_ms > 0 else 0.0
+    traffic = None
+    prof = ROOT / "profiles" / "stage_kernel_traffic.json"
+    if prof.exists():
+        traffic = json.loads(prof.read_text()).get(f"{args.workload}/accelerated")
+    line = {
+        "metric": METRIC, "value": value, "unit": "spots/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 stencil / f64 dose",
+        "data": "synthetic (seeded phantom and spots, no dataset)",
+        "config": {"workload": args.workload, "description": desc,
+                   "method": "batched field, moving active box per spot + FP32 stencil / FP64 dose",
+                   "spots": n_spots, "waves": waves, "box_capacity_cells": cap,
+                   "workspace_bytes": workspace, "max_box_cells": max_box,
+                   "energy_steps_max": max(steps), "energy_steps_min": min(steps),
+                   "cells_marched_per_field": cell_steps / max(args.steps, 1),
+                   "plain_fp64_spots_per_s": plain_spots_per_s,
+                   "l2": "per-spot state buffers (GBs) exceed the 126 MB L2"},
+        "gate": gate,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "kernel": "stage_kernel<float> (A/B/C), all spots per launch",
+                     "avg_launch_ms": stage_ms / max(stage_launches, 1),
+                     "algorithmic_bytes_per_launch": alg_total / max(stage_launches, 1),
+                     "algorithmic_bytes_per_cell_step": ALG_BYTES_PER_CELL_STEP["FP32_FP64"],
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"},
+        "e2e": {"value": n_spots / e2e_s, "unit": "spots/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": launches,
+        "clocks": clocks.summary(),
+    }
+    if not args.no_cpu_baseline:
+        mid = beams[gate_sample(beams, 1)[0]]
+        line["cpu_baseline"] = cpu_baseline(static_config(cfg, mid), cell_steps / max(args.steps, 1),
+                                            units=n_spots, material_map=mm, what=f"the {n_spots}-spot field")
     print(json.dumps(line), flush=True)
 
 
@@ -358,13 +583,28 @@ def main():
                     help="accelerated: moving box + FP32 stencil/FP64 dose; plain: FP64 full domain")
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="only run the first K energy steps of one spot (for ncu captures) and exit")
+    ap.add_argument("--profile-spots", type=int, default=0,
+                    help="field workloads: march K spots of the field once (for ncu captures) and exit")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-    cfg, desc = workload(args.workload)
+    cfg, desc = (None, None) if args.workload in FIELDS else workload(args.workload)
     if args.impl == "reference":
-        run_reference(args, cfg, desc, rank, world)
+        run_reference(args, rank, world)
+        return
+    if args.profile_spots > 0 and args.workload in FIELDS:
+        from proton_dose_m1_b200.numerics.energy import FieldPlan
+        import torch
+        fcfg, mm, grid, beams, _ = field_workload(args.workload)
+        sub = [beams[k] for k in gate_sample(beams, args.profile_spots)]
+        plan = FieldPlan(accelerated_config(fcfg), mm, grid, sub)
+        dose, steps = plan.march()
+        torch.cuda.synchronize()
+        info = plan.last_info
+        print(json.dumps({"profile_spots": len(sub), "steps": steps, "stage_launches": info.stage_launches,
+                          "stage_ms": info.stage_ms, "cell_steps": info.cell_steps,
+                          "max_box_cells": info.max_box_cells, "box_capacity_cells": plan.cap}))
         return
     if args.profile_steps > 0:
         from proton_dose_m1_b200.numerics.energy import M1Plan
@@ -384,7 +624,10 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     try:
-        run_ours(args, cfg, desc, rank, world, local_rank)
+        if args.workload in FIELDS:
+            run_field(args, rank, world, local_rank)
+        else:
+            run_ours(args, cfg, desc, rank, world, local_rank)
     finally:
         if world > 1:
             dist.destroy_process_group()

@@ -104,6 +104,7 @@ typedef struct {
     int stage_launches;       /* launches of the fused stage kernels */
     double stage_ms;          /* their summed device time (CUDA events on the march stream) */
     double cell_steps;        /* sum over energy steps of the cells marched */
+    double max_box_cells;     /* largest domain (cells) one beam marched in one step */
 } pdm1_march_info;
 
 /* Plan: copies the problem to the device and allocates the workspace.

@@ -53,7 +53,7 @@ class MarchInfo(C.Structure):
     _fields_ = [("n_steps", C.c_int), ("n_snapshots", C.c_int), ("final_state_valid", C.c_int),
                 ("graph_replays", C.c_int), ("kernel_launches", C.c_int),
                 ("stage_launches", C.c_int), ("stage_ms", C.c_double),
-                ("cell_steps", C.c_double)]
+                ("cell_steps", C.c_double), ("max_box_cells", C.c_double)]
 
 
 _lib = None

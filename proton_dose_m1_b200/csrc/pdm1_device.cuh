@@ -103,6 +103,7 @@ struct MarchState {
     unsigned long long newmax_bits;   // max phi over the new box (vacuum-aware CFL)
     double pin_max;                // max inflow phi over the new box
     double cell_steps;             // sum over steps of the cells marched (domain volume)
+    double max_cells;              // largest domain marched in one step
 };
 
 __host__ __device__ inline DomainDev make_domain(int i0, int j0, int k0, int nx, int ny, int nz, int inflow);

@@ -86,6 +86,7 @@ __global__ void init_kernel(const ConfigDev *cfp, Coeffs *cos, MarchState *sts, 
         st->newmax_bits = 0ull;
         st->pin_max = 0.0;
         st->cell_steps = 0.0;
+        st->max_cells = 0.0;
         const bool moving = cf.moving && !full_domain;
         st->dom = moving ? bm.init_box : make_domain(0, 0, 0, cf.nx, cf.ny, cf.nz, 1);
         st->prev = st->dom;
@@ -197,7 +198,9 @@ __global__ void __launch_bounds__(256) prologue_kernel(const ConfigDev *cfp, Coe
                     }
                     st->step = step;
                     st->E = En;
-                    st->cell_steps += (double)st->dom.nx * st->dom.ny * st->dom.nz;
+                    const double cells = (double)st->dom.nx * st->dom.ny * st->dom.nz;
+                    st->cell_steps += cells;
+                    st->max_cells = fmax(st->max_cells, cells);
                     st->inv_bits = 0ull;
                     if (st->forced_dE > 0.0) st->done = 1;
                 }
@@ -1252,11 +1255,12 @@ int march_impl(pdm1_plan *pl, double *U, double *dose, double *energies, int max
     CUDA_TRY(cudaMemcpyAsync(pl->h_st, pl->d_st, (size_t)B * sizeof(MarchState), cudaMemcpyDeviceToHost, stream));
     CUDA_TRY(cudaStreamSynchronize(stream));
     int err = 0, max_step = 0;
-    double cells = 0.0;
+    double cells = 0.0, max_cells = 0.0;
     for (int b = 0; b < B; ++b) {
         err |= pl->h_st[b].error;
         max_step = std::max(max_step, pl->h_st[b].step);
         cells += pl->h_st[b].cell_steps;
+        max_cells = std::max(max_cells, pl->h_st[b].max_cells);
         if (steps_per_beam) steps_per_beam[b] = pl->h_st[b].step;
     }
     rc = device_error_status(err);
@@ -1271,6 +1275,7 @@ int march_impl(pdm1_plan *pl, double *U, double *dose, double *energies, int max
         info->stage_launches = stage_launches;
         info->stage_ms = stage_ms;
         info->cell_steps = cells;
+        info->max_box_cells = max_cells;
     }
     if (snap_E_out && !field)
         for (int i = 0; i < pl->h_st[0].taken; ++i) snap_E_out[i] = tg[i];
@@ -1732,6 +1737,7 @@ extern "C" int pdm1_march_noalloc(const pdm1_problem *problem, double *U, double
         info->stage_launches = 0;
         info->stage_ms = 0.0;
         info->cell_steps = hs.cell_steps;
+        info->max_box_cells = hs.max_cells;
     }
     (void)chunks;
     return device_error_status(hs);

@@ -4,6 +4,8 @@ Member names and ``Material`` values match the reference so configurations
 written for it work unchanged.  ``Material`` additionally lists the two
 materials whose tables ship with the reference data but which its enum
 omits (AIR, MUSCLE_SKELETAL); the table loaders only use ``.value``.
+ADIPOSE_SYNTH is a density-scaled water (950 kg/m^3) for phantoms with an
+adipose layer, for which the reference data has no table.
 """
 
 from enum import Enum, auto
@@ -21,6 +23,7 @@ class Material(Enum):
     LUNG = "G4_LUNG_ICRP"
     AIR = "G4_AIR"
     MUSCLE_SKELETAL = "G4_MUSCLE_SKELETAL_ICRP"
+    ADIPOSE_SYNTH = "ADIPOSE_SYNTH"
 
 
 class SpatialScheme(Enum):

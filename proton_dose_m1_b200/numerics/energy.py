@@ -231,16 +231,72 @@ class M1Plan:
         return out
 
 
+# Device bytes per box cell of one beam in a field plan: U on the box (double
+# buffered), the two stage states, V (4 components each, double), the dose
+# quadrature part, and the activity mask byte.
+FIELD_BYTES_PER_BOX_CELL = 21 * 8 + 1
+
+
+def estimate_box_cells(config, grid, beam) -> int:
+    """An upper estimate of the largest moving box (cells) of one beam.
+
+    The box is the region where phi > exp(-s^2/2) max(phi) (s = the
+    truncation sigma) plus ``active_guard_cells`` on every face
+    (numerics/moving_active_domain.py:107-193).  Laterally the fluence is a
+    Gaussian of width sqrt(sigma^2 + sigma_mcs^2) with multiple scattering
+    bounded by 4% of the CSDA range; along z the band where protons carry
+    energy E is the energy window 2 s sigma_E / S plus range straggling
+    (bounded by 1.5% of the range on each side of s sigma).  The estimate is
+    clipped to the phantom; a box that outgrows it stops the march with a
+    capacity error and ``FieldPlan`` retries with more room.
+    """
+    from ..phantoms import csda_range_m
+    from ..enums import Material
+    num = config.numerics
+    s = num.active_truncation_sigma
+    g = int(num.active_guard_cells)
+    nx, ny, nz = (int(n) for n in grid.shape)
+    E0 = beam.energy + num.energy_window_sigma * beam.energy_spread
+    R = min(csda_range_m(Material.WATER, E0), nz * grid.dz)
+    sig = max(beam.sigma)
+    lat = math.sqrt(sig ** 2 + (0.04 * R) ** 2)
+    hx = int(math.ceil(s * lat / grid.dx)) + g + 3
+    hy = int(math.ceil(s * lat / grid.dy)) + g + 3
+    t = material_tables("G4_WATER")
+    S_min = float(np.min(t.sp_value[(t.sp_energy >= 1.0) & (t.sp_energy <= E0)]))   # MeV/m
+    window = 2.0 * s * beam.energy_spread / S_min + 2.0 * s * 0.015 * R
+    wz = int(math.ceil(window / grid.dz)) + 2 * g + 8
+    return int(min(2 * hx + 1, nx) * min(2 * hy + 1, ny) * min(wz, nz))
+
+
+def field_waves(energies, bytes_per_beam: int, budget_bytes: int):
+    """Split a field into waves whose beam buffers fit ``budget_bytes``.
+
+    Beams are ordered by decreasing energy, so the beams of one wave take
+    similar numbers of energy steps and finish together.  Returns lists of
+    beam indices."""
+    wave = max(1, int(budget_bytes // max(1, bytes_per_beam)))
+    order = sorted(range(len(energies)), key=lambda k: (-energies[k], k))
+    return [order[i:i + wave] for i in range(0, len(order), wave)]
+
+
 class FieldPlan:
-    """A spot-scanning field: many pencil beams on one phantom in one launch.
+    """A spot-scanning field: many pencil beams on one phantom, batched.
 
     Every beam marches on its own moving active box with its own energy and
     CFL step (``pdm1_field_plan_create`` / ``pdm1_field_march``); the field
     dose is the sum of the beams' doses.  ``config`` gives the phantom,
     physics, numerics and precision; ``beams`` are ``Beam`` objects.
+
+    Each beam's box buffers hold ``box_capacity_cells`` (0: the largest
+    ``estimate_box_cells`` over the beams).  When all beams do not fit in
+    ``max_workspace_bytes`` (0: 70% of the free device memory), the beams run
+    in waves of similar energy, each wave one batched march, and the waves'
+    doses are summed.
     """
 
-    def __init__(self, config, material_map, grid, beams, box_capacity_cells: int = 0):
+    def __init__(self, config, material_map, grid, beams, box_capacity_cells: int = 0,
+                 max_workspace_bytes: int = 0):
         from dataclasses import replace
         from .boundary import transverse_profile
         num = config.numerics
@@ -251,53 +307,135 @@ class FieldPlan:
         beams = list(beams)
         if not beams:
             raise ValueError("a field needs at least one beam")
-        profiles = [np.ascontiguousarray(b.n_protons * transverse_profile(b, grid), dtype=np.float64)
-                    for b in beams]
-        p, keep, materials = _problem_struct(config, material_map, grid, profiles[0])
-        descs = (_native.BeamDesc * len(beams))()
-        for k, (b, prof) in enumerate(zip(beams, profiles)):
+        for b in beams:
             if b.energy_spread == 0:
                 raise ValueError("Zero energy spread is not supported by the Gaussian inflow.")
-            descs[k] = _native.BeamDesc(b.energy, b.energy_spread, b.angular_spread,
-                                        prof.ctypes.data_as(C.POINTER(C.c_double)))
-        keep += profiles + [descs]
+        self.beams = beams
+        self.config = config
+        self.material_map = material_map
+        self.grid = grid
         self.shape = tuple(int(n) for n in grid.shape)
         self.n_beams = len(beams)
-        self.config = config
+        self.auto_capacity = not box_capacity_cells
+        self.capacity_retries = 0
+        self.profiles = [np.ascontiguousarray(b.n_protons * transverse_profile(b, grid), dtype=np.float64)
+                         for b in beams]
+        self._budget = max_workspace_bytes
+        self._plans = {}
+        self._layout(int(box_capacity_cells or max(estimate_box_cells(config, grid, b) for b in beams)))
+
+    def _layout(self, cap):
+        """Set the box capacity, split the beams into waves, create the plan of
+        a single wave."""
+        self.close()
+        N = int(np.prod(self.shape))
+        nxy = self.shape[0] * self.shape[1]
+        self.cap = int(min(N, cap))
+        per_beam = self.cap * FIELD_BYTES_PER_BOX_CELL + nxy * 8 + 4096
+        budget = self._budget
+        if not budget:
+            torch = _torch()
+            free, _ = torch.cuda.mem_get_info()
+            budget = int(0.7 * free)
+        self.waves = field_waves([b.energy for b in self.beams], per_beam, budget)
+        if len(self.waves) == 1:
+            self._plans[0] = self._create(self.waves[0])
+
+    def _create(self, members):
+        """A native field plan for the beams ``members`` (indices into ``beams``)."""
+        p, keep, _ = _problem_struct(self.config, self.material_map, self.grid, self.profiles[members[0]])
+        descs = (_native.BeamDesc * len(members))()
+        for k, i in enumerate(members):
+            b = self.beams[i]
+            descs[k] = _native.BeamDesc(b.energy, b.energy_spread, b.angular_spread,
+                                        self.profiles[i].ctypes.data_as(C.POINTER(C.c_double)))
         h = C.c_void_p()
-        _native.check(_native.lib().pdm1_field_plan_create(C.byref(p), descs, len(beams),
-                                                           int(box_capacity_cells), C.byref(h)))
-        self._h = h
-        self._keep = keep
+        _native.check(_native.lib().pdm1_field_plan_create(C.byref(p), descs, len(members),
+                                                           int(self.cap), C.byref(h)))
+        return h
 
     def close(self):
-        h = getattr(self, "_h", None)
-        if h:
-            _native.lib().pdm1_plan_destroy(h)
-            self._h = None
+        for h in getattr(self, "_plans", {}).values():
+            if h:
+                _native.lib().pdm1_plan_destroy(h)
+        self._plans = {}
 
     __del__ = close
 
     @property
     def workspace_bytes(self) -> int:
-        return int(_native.lib().pdm1_plan_workspace_bytes(self._h))
+        return sum(int(_native.lib().pdm1_plan_workspace_bytes(h)) for h in self._plans.values())
 
     def march_device(self, dose, max_steps=2_000_000):
-        """Field dose into the device tensor ``dose``; returns steps per beam."""
-        import torch
-        steps = (C.c_int * self.n_beams)()
-        info = _native.MarchInfo()
-        _native.check(_native.lib().pdm1_field_march(
-            self._h, C.c_void_p(dose.data_ptr()), int(max_steps), steps, C.byref(info),
-            C.c_void_p(torch.cuda.current_stream().cuda_stream)))
-        self.last_info = info
-        return list(steps)
+        """Field dose into the device tensor ``dose``; returns steps per beam.
+
+        ``last_info`` sums the march statistics over the waves.  With an
+        estimated capacity, a box that outgrows it doubles the capacity and
+        the field is marched again."""
+        N = int(np.prod(self.shape))
+        while True:
+            try:
+                return self._march_waves(dose, max_steps)
+            except ValueError as e:
+                if not (self.auto_capacity and "capacity" in str(e) and self.cap < N):
+                    raise
+                self.capacity_retries += 1
+                self._layout(2 * self.cap)
+
+    def _march_waves(self, dose, max_steps):
+        torch = _torch()
+        steps_all = [0] * self.n_beams
+        total = _native.MarchInfo()
+        partial = torch.empty_like(dose) if len(self.waves) > 1 else None
+        stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        for w, members in enumerate(self.waves):
+            h = self._plans.get(w)
+            transient = h is None
+            if transient:
+                h = self._create(members)
+            try:
+                steps = (C.c_int * len(members))()
+                info = _native.MarchInfo()
+                out = dose if w == 0 else partial
+                _native.check(_native.lib().pdm1_field_march(
+                    h, C.c_void_p(out.data_ptr()), int(max_steps), steps, C.byref(info), stream))
+            finally:
+                if transient:
+                    _native.lib().pdm1_plan_destroy(h)
+            if w > 0:
+                dose.add_(partial)
+            for k, i in enumerate(members):
+                steps_all[i] = steps[k]
+            total.n_steps = max(total.n_steps, info.n_steps)
+            total.graph_replays += info.graph_replays
+            total.kernel_launches += info.kernel_launches + (1 if w > 0 else 0)
+            total.stage_launches += info.stage_launches
+            total.stage_ms += info.stage_ms
+            total.cell_steps += info.cell_steps
+            total.max_box_cells = max(total.max_box_cells, info.max_box_cells)
+        self.last_info = total
+        return steps_all
 
     def march(self, max_steps=2_000_000):
         torch = _torch()
         dose = torch.empty(self.shape, dtype=torch.float64, device="cuda")
         steps = self.march_device(dose, max_steps)
         return dose, steps
+
+
+def field_march(config, material_map, grid, beams, box_capacity_cells: int = 0):
+    """Dose of a spot-scanning field (host NumPy in, host NumPy out).
+
+    The field counterpart of ``energy_march``: the reference marches one beam
+    per ``Solver.solve`` call (proton_solver/solver.py:34-218) and a field is
+    the sum of its beams' doses.  Returns ``(dose, steps_per_beam)``.
+    """
+    plan = FieldPlan(config, material_map, grid, beams, box_capacity_cells)
+    try:
+        dose, steps = plan.march()
+        return dose.cpu().numpy(), steps
+    finally:
+        plan.close()
 
 
 def energy_march(U: Any, material_map, grid, inflow, config, xp=None,

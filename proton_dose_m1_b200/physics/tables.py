@@ -4,6 +4,12 @@ The tables are the reference's Geant4 exports (data/stopping_power,
 data/wentzel_transport, data/nuclear_attenuation, data/materials.csv),
 packed into ``data/material_tables.npz`` by ``data/pack_tables.py``.
 Each table is 6000 log-spaced nodes from 1e-4 to 300 MeV.
+
+``ADIPOSE_SYNTH`` has no Geant4 export: it is water scaled to 950 kg/m^3.
+Every coefficient here is per unit length and proportional to density for a
+fixed composition, so S, Sigma_tr and Sigma_r are the water values x 0.95 and
+the radiation length (in metres) is water's / 0.95.  It stands in for the
+adipose shell of synthetic pelvis phantoms.
 """
 
 from __future__ import annotations
@@ -38,9 +44,20 @@ def _archive():
         return {k: z[k] for k in z.files}
 
 
+SYNTHETIC_SCALED = {"ADIPOSE_SYNTH": ("G4_WATER", 950.0)}
+
+
 @lru_cache
 def material_tables(material: Material | str) -> MaterialTables:
     name = material.value if isinstance(material, Material) else str(material)
+    if name in SYNTHETIC_SCALED:
+        base_name, rho = SYNTHETIC_SCALED[name]
+        base = material_tables(base_name)
+        f = rho / base.density
+        return MaterialTables(name=name, sp_energy=base.sp_energy, sp_value=base.sp_value * f,
+                              tr_energy=base.tr_energy, tr_value=base.tr_value * f,
+                              nuc_energy=base.nuc_energy, nuc_value=base.nuc_value * f,
+                              density=rho, radiation_length=base.radiation_length / f)
     a = _archive()
     if f"{name}/sp_energy" not in a:
         raise FileNotFoundError(f"No stopping-power data found for {name}.")

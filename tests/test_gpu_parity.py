@@ -93,7 +93,7 @@ def test_coefficients_match_reference(unit):
     E = unit["coef_energy"]
     for interp, tr_key, nuc_key in ((CoefficientInterpolation.LINEAR, "tr_linear", "nuc_linear"),
                                     (CoefficientInterpolation.PCHIP, "tr_pchip", "nuc_pchip")):
-        mats = list(Material)
+        mats = [m for m in Material if m.value.startswith("G4_")]
         ids = np.arange(len(mats), dtype=np.int32).repeat(4 * 4).reshape(len(mats), 4, 4)
         ids = np.ascontiguousarray(np.tile(ids, (1, 1, 1)))
         geo = Geometry.from_ids((0.01, 0.004, 0.004), np.ascontiguousarray(ids.reshape(len(mats), 4, 4)), mats)

@@ -46,7 +46,7 @@ def test_hll_flux(unit):
     assert np.max(np.abs(unit_speeds - unit["hll_unit"]) / scale) < 1e-14
 
 
-@pytest.mark.parametrize("material", list(Material))
+@pytest.mark.parametrize("material", [m for m in Material if m.value.startswith("G4_")])
 def test_coefficients_bit_exact(unit, material):
     E = unit["coef_energy"]
     mi = list(unit["coef_materials"]).index(material.value)
