@@ -175,6 +175,22 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def stage_traffic(key, cell_steps, stage_launches):
+    """DRAM bytes per stage launch from the committed ncu measurement of this
+    workload and method: either bytes per launch, or bytes per cell-step
+    (measured over every stage launch of a smaller run of the same kernels)
+    scaled by the cell-steps of this run."""
+    prof = ROOT / "profiles" / "stage_kernel_traffic.json"
+    if not prof.exists():
+        return None
+    entry = json.loads(prof.read_text()).get(key)
+    if entry is None:
+        return None
+    if "bytes_per_cell_step" in entry:
+        return entry["bytes_per_cell_step"] * cell_steps / max(stage_launches, 1)
+    return entry.get("bytes_per_launch")
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -395,10 +411,7 @@ def run_ours(args, cfg, desc, rank, world, local_rank):
     # a third per stage launch (cell_steps already sums the domain over steps)
     alg_total = cell_steps * ALG_BYTES_PER_CELL_STEP[precision]
     achieved = alg_total / (stage_ms / 1e3) / 1e9 if stage_ms > 0 else 0.0
-    traffic = None
-    prof = ROOT / "profiles" / "stage_kernel_traffic.json"
-    if prof.exists():
-        traffic = json.loads(prof.read_text()).get(f"{args.workload}/{args.method}")
+    traffic = stage_traffic(f"{args.workload}/{args.method}", cell_steps, stage_launches)
     line = {
         "metric": METRIC, "value": value, "unit": "spots/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -533,10 +546,7 @@ def run_field(args, rank, world, local_rank):
     peak, peak_kind = measured_peaks()
     alg_total = cell_steps * ALG_BYTES_PER_CELL_STEP["FP32_FP64"]
     achieved = alg_total / (stage_ms / 1e3) / 1e9 if stage_ms > 0 else 0.0
-    traffic = None
-    prof = ROOT / "profiles" / "stage_kernel_traffic.json"
-    if prof.exists():
-        traffic = json.loads(prof.read_text()).get(f"{args.workload}/accelerated")
+    traffic = stage_traffic(f"{args.workload}/accelerated", cell_steps, stage_launches)
     line = {
         "metric": METRIC, "value": value, "unit": "spots/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -615,7 +625,7 @@ def main():
         torch.cuda.synchronize()
         print(json.dumps({"profile_steps": len(E) - 1, "energy": float(E[-1]),
                           "stage_launches": plan.last_info.stage_launches,
-                          "stage_ms": plan.last_info.stage_ms}))
+                          "stage_ms": plan.last_info.stage_ms, "cell_steps": plan.last_info.cell_steps}))
         return
     import torch
     import torch.distributed as dist

@@ -105,6 +105,8 @@ typedef struct {
     double stage_ms;          /* their summed device time (CUDA events on the march stream) */
     double cell_steps;        /* sum over energy steps of the cells marched */
     double max_box_cells;     /* largest domain (cells) one beam marched in one step */
+    int box_grow_events;      /* learned box: faces grown by the outgoing-flux check */
+    int box_fallbacks;        /* learned box: beams that fell back (full domain or heuristic box) */
 } pdm1_march_info;
 
 /* Plan: copies the problem to the device and allocates the workspace.
@@ -205,6 +207,68 @@ int pdm1_gamma(const double *dose_ref, const double *dose_eval, int nx, int ny, 
                double distance_mm, double lower_cutoff_percent, int interp_fraction,
                double max_gamma, double global_normalisation, double *gamma_out,
                double *pass_rate_out, pdm1_stream_t stream);
+
+/* ---- Learned moving box -------------------------------------------------
+ * No reference counterpart: the reference's moving box is the fixed heuristic
+ * of numerics/moving_active_domain.py:107-193 (significant box plus
+ * active_guard_cells on every face).  With a box model, a plan instead extends
+ * the significant box on each face by a margin that a small network proposes
+ * from the beam's fluence moments at every energy step, and checks every step
+ * that the particle current through the box faces stays below
+ * leak_tolerance of the beam current; faces that leak more grow by grow_cells,
+ * and a beam whose growth passes extra_max falls back to the full domain when
+ * its buffers hold it, else to the heuristic box. */
+#define PDM1_BOX_FEATURES 16
+#define PDM1_BOX_OUTPUTS 6
+#define PDM1_BOX_PARAMS 5638      /* 64*16 + 64 + 64*64 + 64 + 6*64 + 6 */
+#define PDM1_RECORD_WIDTH 40      /* floats per recorded energy step */
+
+typedef struct {
+    const float *params;          /* host: W1 (64x16), b1 (64), W2 (64x64), b2 (64), W3 (6x64), b3 (6);
+                                     matrices row-major [out][in]; h = relu(W x + b) */
+    float x_mean[PDM1_BOX_FEATURES], x_inv_std[PDM1_BOX_FEATURES];   /* feature normalisation */
+    float y_scale[PDM1_BOX_OUTPUTS], y_offset[PDM1_BOX_OUTPUTS];     /* margin = ceil(y * scale + offset) cells;
+                                     faces x-, x+, y-, y+, z-, z+ */
+    int margin_min, margin_max;   /* clamp of the proposed margins (cells) */
+    int grow_cells;               /* growth of a leaking face (cells) */
+    int extra_max;                /* total growth of a face beyond which the beam falls back */
+    double leak_tolerance;        /* face current / beam current that triggers growth (e.g. 1e-6) */
+} pdm1_box_model;
+
+/* Attach (or, with NULL, detach) a box model to a moving-box plan or field plan. */
+int pdm1_plan_set_box_model(pdm1_plan *plan, const pdm1_box_model *model);
+
+/* Training data: a one-beam plan on the full domain (moving_active_domain
+ * off) with a recorder writes, after every energy step, one row of
+ * PDM1_RECORD_WIDTH floats to `rows` (device, max_rows rows):
+ *   0 the energy after the step, 1 its dE,
+ *   2..7 the significant box (i0, i1, j0, j1, k0, k1: global cells, half-open,
+ *        -1 when nothing is significant) at the plan's box tolerance,
+ *   8..23 the PDM1_BOX_FEATURES features of the state,
+ *   24 the summed fluence, 25 the largest z-plane current, 26 the threshold scale,
+ *   27..32 and 33..38 the boxes of the cells above tail_a * scale and
+ *        tail_b * scale (the fluence tail at two levels), 39 zero.
+ * NULL detaches.  Rows beyond max_rows are dropped; pdm1_march_info.n_steps
+ * tells how many steps ran. */
+int pdm1_plan_set_recorder(pdm1_plan *plan, float *rows, int max_rows, double tail_a, double tail_b);
+
+/* Training of the proposer network (FP32, on the device; X (n x 16) and Y
+ * (n x 6) device, normalised): one fused forward/backward kernel per chunk of
+ * 64 samples, Adam updates of theta (device, PDM1_BOX_PARAMS) over `epochs`
+ * passes in minibatches of `batch` shuffled with `seed`.  Loss: mean of
+ * w (y - target)^2 with w = alpha where the prediction is below the target.
+ * loss_per_epoch (host, epochs) may be NULL. */
+int pdm1_mlp_train(float *theta, const float *X, const float *Y, int n, int epochs, int batch, float lr,
+                   float alpha, unsigned seed, float *loss_per_epoch, pdm1_stream_t stream);
+/* Loss (device scalar, may be NULL) and its gradient (device, PDM1_BOX_PARAMS) over all n samples. */
+int pdm1_mlp_gradients(const float *theta, const float *X, const float *Y, int n, float alpha, float *grad,
+                       float *loss, pdm1_stream_t stream);
+/* FP32 forward pass (device arrays). */
+int pdm1_mlp_forward(const float *theta, const float *X, int n, float *Y, pdm1_stream_t stream);
+/* The march's inference: raw features (device, n x 16) normalised with the
+ * model, BF16 tensor-core MLP with FP32 accumulation; out (device, n x 6). */
+int pdm1_box_model_infer(const pdm1_box_model *model, const float *features, int n, float *out,
+                         pdm1_stream_t stream);
 
 const char *pdm1_last_error(void);
 const char *pdm1_version(void);

@@ -53,7 +53,20 @@ class MarchInfo(C.Structure):
     _fields_ = [("n_steps", C.c_int), ("n_snapshots", C.c_int), ("final_state_valid", C.c_int),
                 ("graph_replays", C.c_int), ("kernel_launches", C.c_int),
                 ("stage_launches", C.c_int), ("stage_ms", C.c_double),
-                ("cell_steps", C.c_double), ("max_box_cells", C.c_double)]
+                ("cell_steps", C.c_double), ("max_box_cells", C.c_double),
+                ("box_grow_events", C.c_int), ("box_fallbacks", C.c_int)]
+
+
+BOX_FEATURES, BOX_OUTPUTS, BOX_PARAMS, RECORD_WIDTH = 16, 6, 5638, 40
+
+
+class BoxModel(C.Structure):
+    _fields_ = [("params", C.POINTER(C.c_float)),
+                ("x_mean", C.c_float * BOX_FEATURES), ("x_inv_std", C.c_float * BOX_FEATURES),
+                ("y_scale", C.c_float * BOX_OUTPUTS), ("y_offset", C.c_float * BOX_OUTPUTS),
+                ("margin_min", C.c_int), ("margin_max", C.c_int),
+                ("grow_cells", C.c_int), ("extra_max", C.c_int),
+                ("leak_tolerance", C.c_double)]
 
 
 _lib = None
@@ -90,6 +103,13 @@ def lib():
         L.pdm1_eigen_batch.argtypes = [_vp, C.c_int, _vp, C.c_int, _vp]
         L.pdm1_hll_batch.argtypes = [_vp, _vp, C.c_int, C.c_int, _vp, C.c_int, _vp]
         L.pdm1_exp_batch.argtypes = [_vp, _vp, C.c_int, _vp]
+        L.pdm1_plan_set_box_model.argtypes = [_vp, C.POINTER(BoxModel)]
+        L.pdm1_plan_set_recorder.argtypes = [_vp, _vp, C.c_int, C.c_double, C.c_double]
+        L.pdm1_mlp_train.argtypes = [_vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
+                                     C.c_uint, C.POINTER(C.c_float), _vp]
+        L.pdm1_mlp_gradients.argtypes = [_vp, _vp, _vp, C.c_int, C.c_float, _vp, _vp, _vp]
+        L.pdm1_mlp_forward.argtypes = [_vp, _vp, C.c_int, _vp, _vp]
+        L.pdm1_box_model_infer.argtypes = [C.POINTER(BoxModel), _vp, C.c_int, _vp, _vp]
         L.pdm1_gamma.argtypes = [_vp, _vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                  C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
                                  C.c_double, C.c_double, _vp, _dp, _vp]
@@ -115,4 +135,6 @@ EXPORTED_SYMBOLS = (
     "pdm1_spatial_operator", "pdm1_energy_step", "pdm1_advance", "pdm1_coefficients",
     "pdm1_weno_batch", "pdm1_project_batch", "pdm1_eigen_batch", "pdm1_hll_batch",
     "pdm1_exp_batch", "pdm1_gamma", "pdm1_last_error", "pdm1_version",
+    "pdm1_march_noalloc", "pdm1_plan_set_box_model", "pdm1_plan_set_recorder", "pdm1_mlp_train",
+    "pdm1_mlp_gradients", "pdm1_mlp_forward", "pdm1_box_model_infer",
 )

@@ -28,6 +28,8 @@ UNITS = {
     CSRC / "pdm1_stage_fp32.cu": ["--use_fast_math"],
     # dose scoring (gamma index)
     CSRC / "pdm1_gamma.cu": [],
+    # learned moving box: proposer network training and BF16 inference, box kernels
+    CSRC / "pdm1_box.cu": [],
 }
 SOURCES = list(UNITS)
 

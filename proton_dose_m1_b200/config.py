@@ -115,6 +115,9 @@ class Accel:
     graph_chunk_steps: int = 32
     # (tile_x, tile_y, tile_z) override for the stage kernels; None = autotuned/default.
     tile: tuple[int, int, int] | None = None
+    # Learned moving box (learned_box.BoxModel); None = the fixed heuristic box.
+    # Needs numerics.moving_active_domain.
+    box_model: object | None = None
 
     def __post_init__(self):
         if not isinstance(self.precision, Precision):

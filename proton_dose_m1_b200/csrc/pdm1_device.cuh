@@ -6,11 +6,32 @@
 #include "../../include/pdm1.h"
 #include "pdm1_math.cuh"
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 namespace pdm1 {
 
 constexpr int kMaxMat = 16;
+
+// Learned moving box: proposer network 16 -> 64 -> 64 -> 6 (ReLU).
+constexpr int kFeat = 16, kHid = 64, kOut = 6, kOutPad = 8;
+constexpr int kParams = kHid * kFeat + kHid + kHid * kHid + kHid + kOut * kHid + kOut;
+
+// Device form of a box model: BF16 weights [out][in] (the column-major B
+// operand of mma.m16n8k16), FP32 biases, input normalisation and the map of
+// the network's outputs to margins in cells.
+struct BoxModelDev {
+    __nv_bfloat16 W1[kHid * kFeat];
+    __nv_bfloat16 W2[kHid * kHid];
+    __nv_bfloat16 W3[kOutPad * kHid];
+    float b1[kHid], b2[kHid], b3[kOutPad];
+    float x_mean[kFeat], x_inv_std[kFeat];
+    float y_scale[kOut], y_offset[kOut];
+    int margin_min, margin_max, grow_cells, extra_max;
+    double leak_tol;
+};
+
+int pack_box_model(const pdm1_box_model *m, BoxModelDev &out);
 
 enum { ERR_DEV_RANGE = 1, ERR_DEV_MAXSTEPS = 2, ERR_DEV_NONFINITE = 4, ERR_DEV_CAPACITY = 8 };
 // ---------------------------------------------------------------------------
@@ -71,8 +92,23 @@ struct ConfigDev {
     unsigned char *active;      // vacuum-aware activity mask on the box, cap per beam
     int grid_ctas;              // persistent grid of the stage kernels
     int fp32;                   // FP32-stencil form: float eigenvalues in the CFL bound
+    // learned moving box and training-data recorder
+    int learned;                // a box model proposes the margins
+    const BoxModelDev *model;
+    double *acc;                // per beam kAcc doubles: fluence moments and face currents of the box
+    double *plane;              // per beam nz doubles: current through each z plane of the box
+    float *rec;                 // recorder rows (one-beam full-domain plans), or NULL
+    int rec_max;
+    double rec_tail_tol[2];     // recorder: the two fluence-tail thresholds
     MatDev mats[kMaxMat];
 };
+
+// Layout of a beam's accumulator (cell coordinates are global cell centres,
+// in cells): sums over the box of phi, phi x, phi y, phi z, phi x^2, phi y^2,
+// phi z^2, Jx, Jy, Jz, |Jx|, |Jy|, then the current |J.n| summed over the
+// cells of the box faces x-, x+, y-, y+, z-, z+ that lie inside the phantom
+// (the entrance face excluded), then max phi.
+enum { ACC_M = 0, ACC_X = 1, ACC_X2 = 4, ACC_J = 7, ACC_JABS = 10, ACC_FACE = 12, ACC_MAX = 18, kAcc = 20 };
 
 struct Coeffs {
     double E, dE, E_next;
@@ -104,6 +140,13 @@ struct MarchState {
     double pin_max;                // max inflow phi over the new box
     double cell_steps;             // sum over steps of the cells marched (domain volume)
     double max_cells;              // largest domain marched in one step
+    // learned box
+    int sig[6];                    // significant box (global, half-open); sig[1] < 0: none
+    double sig_scale;              // max(phi, phi_in) the threshold was taken from
+    int extra[6];                  // growth per face from the outgoing-flux check
+    int fallback;                  // 0 learned, 1 full domain, 2 heuristic box
+    int grows;                     // faces grown by the check
+    int margin[6];                 // margins of the last box
 };
 
 __host__ __device__ inline DomainDev make_domain(int i0, int j0, int k0, int nx, int ny, int nz, int inflow);
@@ -366,6 +409,102 @@ __device__ __forceinline__ int beam_of_tile(const int *tile_off, int nbeams, int
 __device__ __forceinline__ unsigned long long *beam_slab(const ConfigDev &cf, int b) {
     return cf.slab + (size_t)b * (cf.nx + cf.ny + cf.nz);
 }
+
+// The significant box of desired_box (moving_active_domain.py:107-151):
+// scale = max(max phi, max phi_in) (phi_in only while the domain touches
+// z = 0), then the first and last x / y / z slab of `d` whose max phi exceeds
+// tol * scale (the plan's tolerance for the moving box), an inflow cell above
+// it joining the k = 0 layer.  Called by all
+// threads of a CTA of 256; results (local indices, hi < 0 when none) in the
+// caller's shared memory.
+__device__ inline void significant_box_cta(const ConfigDev &cf, const BeamDev &bm, const DomainDev &d,
+                                           const unsigned long long *slab, double ed, double *red, int *s_lo,
+                                           int *s_hi, double *s_scale, double tol) {
+    const int t = threadIdx.x;
+    const unsigned long long *sx = slab, *sy = slab + cf.nx, *sz = slab + cf.nx + cf.ny;
+    auto as_d = [](unsigned long long b) { return __longlong_as_double((long long)b); };
+    double m = 0.0;
+    for (int i = t; i < d.nx; i += 256) m = fmax(m, as_d(sx[i]));
+    if (d.inflow)
+        for (int e = t; e < d.nx * d.ny; e += 256) {
+            int i = e / d.ny, j = e % d.ny;
+            m = fmax(m, bm.spatial[(size_t)(d.i0 + i) * cf.ny + (d.j0 + j)] * ed);
+        }
+    red[t] = m;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (t < w) red[t] = fmax(red[t], red[t + w]);
+        __syncthreads();
+    }
+    if (t == 0) {
+        *s_scale = red[0];
+        for (int q = 0; q < 3; ++q) { s_lo[q] = 0x7fffffff; s_hi[q] = -1; }
+    }
+    __syncthreads();
+    const double scale = *s_scale;
+    const double thr = tol * scale;
+    if (scale != 0.0) {
+        for (int i = t; i < d.nx; i += 256) {
+            bool act = as_d(sx[i]) > thr;
+            if (!act && d.inflow)
+                for (int j = 0; j < d.ny && !act; ++j)
+                    act = bm.spatial[(size_t)(d.i0 + i) * cf.ny + (d.j0 + j)] * ed > thr;
+            if (act) { atomicMin(&s_lo[0], i); atomicMax(&s_hi[0], i); }
+        }
+        for (int j = t; j < d.ny; j += 256) {
+            bool act = as_d(sy[j]) > thr;
+            if (!act && d.inflow)
+                for (int i = 0; i < d.nx && !act; ++i)
+                    act = bm.spatial[(size_t)(d.i0 + i) * cf.ny + (d.j0 + j)] * ed > thr;
+            if (act) { atomicMin(&s_lo[1], j); atomicMax(&s_hi[1], j); }
+        }
+        for (int k = t; k < d.nz; k += 256) {
+            bool act = as_d(sz[k]) > thr;
+            if (!act && k == 0 && d.inflow)
+                for (int e = 0; e < d.nx * d.ny && !act; ++e)
+                    act = bm.spatial[(size_t)(d.i0 + e / d.ny) * cf.ny + (d.j0 + e % d.ny)] * ed > thr;
+            if (act) { atomicMin(&s_lo[2], k); atomicMax(&s_hi[2], k); }
+        }
+    }
+    __syncthreads();
+}
+
+// Switch a beam to the box `nb` (one thread): the capacity check, the
+// compact-state ping-pong, the spectrum for the CFL bound and, for the
+// vacuum-aware CFL (energy.py:496-537), the max inflow over the new box.
+__device__ inline void switch_box(const ConfigDev &cf, const BeamDev &bm, Coeffs *co, MarchState *st, int b,
+                                  DomainDev nb, double ed) {
+    const DomainDev d = st->dom;
+    bool same = nb.i0 == d.i0 && nb.j0 == d.j0 && nb.k0 == d.k0 && nb.nx == d.nx && nb.ny == d.ny && nb.nz == d.nz;
+    if (!same && (size_t)nb.nx * nb.ny * nb.nz > cf.cap) {
+        st->error |= ERR_DEV_CAPACITY;   // the box outgrew the beam's buffers
+        same = true;
+    }
+    st->reboxed = same ? 0 : 1;
+    if (!same) {
+        st->prev = d;
+        st->Uprev = st->Ua;
+        double *a_buf = cf.bufA + 4 * (size_t)b * cf.cap, *b_buf = cf.bufB + 4 * (size_t)b * cf.cap;
+        st->Ua = st->Ua == a_buf ? b_buf : a_buf;
+        st->dom = nb;
+    }
+    st->inv_bits = 0ull;
+    co->ed_cfl = ed;
+    st->newmax_bits = 0ull;
+    double pin = 0.0;
+    if (cf.vacuum_aware && nb.inflow)
+        for (int e = 0; e < nb.nx * nb.ny; ++e)
+            pin = fmax(pin, bm.spatial[(size_t)(nb.i0 + e / nb.ny) * cf.ny + (nb.j0 + e % nb.ny)] * ed);
+    st->pin_max = pin;
+}
+
+// Learned box and recorder kernels (pdm1_box.cu).
+void launch_box_moments(const ConfigDev *d_cf, const MarchState *d_st, int grid, int record, cudaStream_t stream);
+void launch_box_learn(const ConfigDev *d_cf, Coeffs *d_co, MarchState *d_st, int nbeams, cudaStream_t stream);
+void launch_record(const ConfigDev *d_cf, const Coeffs *d_co, MarchState *d_st, cudaStream_t stream);
+
+// Record an error message for pdm1_last_error() and return `code`.
+int report_error(int code, const char *msg);
 
 // Single-precision stencil kernels (pdm1_stage_fp32.cu, compiled with fast math).
 int stage_fp32_set_attributes();

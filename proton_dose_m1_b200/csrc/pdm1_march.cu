@@ -87,6 +87,10 @@ __global__ void init_kernel(const ConfigDev *cfp, Coeffs *cos, MarchState *sts, 
         st->pin_max = 0.0;
         st->cell_steps = 0.0;
         st->max_cells = 0.0;
+        for (int q = 0; q < 6; ++q) { st->sig[q] = -1; st->extra[q] = 0; st->margin[q] = 0; }
+        st->sig_scale = 0.0;
+        st->fallback = 0;
+        st->grows = 0;
         const bool moving = cf.moving && !full_domain;
         st->dom = moving ? bm.init_box : make_domain(0, 0, 0, cf.nx, cf.ny, cf.nz, 1);
         st->prev = st->dom;
@@ -448,7 +452,8 @@ __global__ void __launch_bounds__(NT) box_init_kernel(const ConfigDev *cfp, Marc
 // One CTA at the start of every step: desired_box (moving_active_domain.py:
 // 107-193) from the slab maxima of the current state and the inflow at the
 // step's energy; the switch to the new box; S and spectrum for the CFL.
-// One CTA per beam.
+// One CTA per beam.  With a box model the significant box is kept for
+// box_learn_kernel, which chooses the margins and switches the box.
 __global__ void __launch_bounds__(256) box_kernel(const ConfigDev *cfp, Coeffs *cos, MarchState *sts) {
     const ConfigDev &cf = *cfp;
     const int b = blockIdx.x;
@@ -474,60 +479,24 @@ __global__ void __launch_bounds__(256) box_kernel(const ConfigDev *cfp, Coeffs *
     }
     __syncthreads();
     const double ed = s_ed;
-    const unsigned long long *sx = slab, *sy = slab + cf.nx, *sz = slab + cf.nx + cf.ny;
-    auto as_d = [](unsigned long long b) { return __longlong_as_double((long long)b); };
-    // scale = max(max phi, max phi_in)   (phi_in only while the box touches z = 0)
-    double m = 0.0;
-    for (int i = t; i < d.nx; i += 256) m = fmax(m, as_d(sx[i]));
-    if (d.inflow)
-        for (int e = t; e < d.nx * d.ny; e += 256) {
-            int i = e / d.ny, j = e % d.ny;
-            m = fmax(m, bm.spatial[(size_t)(d.i0 + i) * cf.ny + (d.j0 + j)] * ed);
-        }
-    red[t] = m;
-    __syncthreads();
-    for (int w = 128; w > 0; w >>= 1) {
-        if (t < w) red[t] = fmax(red[t], red[t + w]);
-        __syncthreads();
-    }
-    if (t == 0) {
-        s_scale = red[0];
-        for (int q = 0; q < 3; ++q) { s_lo[q] = INT_MAX; s_hi[q] = -1; }
-    }
-    __syncthreads();
-    const double scale = s_scale;
-    const double thr = cf.tol * scale;
-    if (scale != 0.0) {
-        // active x / y indices: slab max above the threshold, or an inflow cell
-        // of that row above it (the inflow joins the k = 0 layer)
-        for (int i = t; i < d.nx; i += 256) {
-            bool act = as_d(sx[i]) > thr;
-            if (!act && d.inflow)
-                for (int j = 0; j < d.ny && !act; ++j)
-                    act = bm.spatial[(size_t)(d.i0 + i) * cf.ny + (d.j0 + j)] * ed > thr;
-            if (act) { atomicMin(&s_lo[0], i); atomicMax(&s_hi[0], i); }
-        }
-        for (int j = t; j < d.ny; j += 256) {
-            bool act = as_d(sy[j]) > thr;
-            if (!act && d.inflow)
-                for (int i = 0; i < d.nx && !act; ++i)
-                    act = bm.spatial[(size_t)(d.i0 + i) * cf.ny + (d.j0 + j)] * ed > thr;
-            if (act) { atomicMin(&s_lo[1], j); atomicMax(&s_hi[1], j); }
-        }
-        for (int k = t; k < d.nz; k += 256) {
-            bool act = as_d(sz[k]) > thr;
-            if (!act && k == 0 && d.inflow)
-                for (int e = 0; e < d.nx * d.ny && !act; ++e)
-                    act = bm.spatial[(size_t)(d.i0 + e / d.ny) * cf.ny + (d.j0 + e % d.ny)] * ed > thr;
-            if (act) { atomicMin(&s_lo[2], k); atomicMax(&s_hi[2], k); }
-        }
-    }
-    __syncthreads();
+    significant_box_cta(cf, bm, d, slab, ed, red, s_lo, s_hi, &s_scale, cf.tol);
     // reset the slab maxima for this step's stage C
     for (int e = t; e < cf.nx + cf.ny + cf.nz; e += 256) slab[e] = 0ull;
     if (t == 0) {
+        const double scale = s_scale;
+        const bool none = scale == 0.0 || s_hi[0] < 0 || s_hi[1] < 0 || s_hi[2] < 0;
+        if (cf.learned) {
+            st->sig[0] = none ? -1 : d.i0 + s_lo[0];
+            st->sig[1] = none ? -1 : d.i0 + s_hi[0] + 1;
+            st->sig[2] = none ? -1 : d.j0 + s_lo[1];
+            st->sig[3] = none ? -1 : d.j0 + s_hi[1] + 1;
+            st->sig[4] = none ? -1 : d.k0 + s_lo[2];
+            st->sig[5] = none ? -1 : d.k0 + s_hi[2] + 1;
+            st->sig_scale = scale;
+            return;
+        }
         DomainDev nb;
-        if (scale == 0.0 || s_hi[0] < 0 || s_hi[1] < 0 || s_hi[2] < 0) {
+        if (none) {
             nb = bm.init_box;
         } else {
             const int g = cf.guard;
@@ -539,28 +508,7 @@ __global__ void __launch_bounds__(256) box_kernel(const ConfigDev *cfp, Coeffs *
             int bk0 = ak0 - g > 0 ? ak0 - g : 0, bk1 = ak1 + g < cf.nz ? ak1 + g : cf.nz;
             nb = make_domain(bi0, bj0, bk0, bi1 - bi0, bj1 - bj0, bk1 - bk0, bk0 == 0);
         }
-        bool same = nb.i0 == d.i0 && nb.j0 == d.j0 && nb.k0 == d.k0 && nb.nx == d.nx && nb.ny == d.ny && nb.nz == d.nz;
-        if (!same && (size_t)nb.nx * nb.ny * nb.nz > cf.cap) {
-            st->error |= ERR_DEV_CAPACITY;   // the box outgrew the beam's buffers
-            same = true;
-        }
-        st->reboxed = same ? 0 : 1;
-        if (!same) {
-            st->prev = d;
-            st->Uprev = st->Ua;
-            double *a_buf = cf.bufA + 4 * (size_t)b * cf.cap, *b_buf = cf.bufB + 4 * (size_t)b * cf.cap;
-            st->Ua = st->Ua == a_buf ? b_buf : a_buf;
-            st->dom = nb;
-        }
-        st->inv_bits = 0ull;
-        co->ed_cfl = ed;
-        // vacuum-aware masks (energy.py:496-537) use the inflow of the new box
-        st->newmax_bits = 0ull;
-        double pin = 0.0;
-        if (cf.vacuum_aware && nb.inflow)
-            for (int e = 0; e < nb.nx * nb.ny; ++e)
-                pin = fmax(pin, bm.spatial[(size_t)(nb.i0 + e / nb.ny) * cf.ny + (nb.j0 + e % nb.ny)] * ed);
-        st->pin_max = pin;
+        switch_box(cf, bm, co, st, b, nb, ed);
     }
 }
 
@@ -721,6 +669,10 @@ std::vector<double> pchip_slopes(const double *E, const double *v, int n) {
 
 }  // namespace
 
+namespace pdm1 {
+int report_error(int code, const char *msg) { return set_error(code, msg); }
+}  // namespace pdm1
+
 struct pdm1_plan {
     pdm1_problem p{};
     ConfigDev cf{};
@@ -743,6 +695,9 @@ struct pdm1_plan {
     double *d_bufA = nullptr, *d_bufB = nullptr;   // moving box: compact-state ping-pong
     unsigned long long *d_slab = nullptr;
     unsigned char *d_active = nullptr;
+    BoxModelDev *d_model = nullptr;  // learned box
+    double *d_acc = nullptr;         // nbeams x kAcc
+    double *d_plane = nullptr;       // nbeams x nz
     size_t workspace = 0;
     std::vector<BeamDev> h_beams;   // host copy (device spatial pointers)
     // per material: [lo, hi] of the stopping-power, transport, nuclear tables
@@ -886,8 +841,13 @@ int launch_box_step(pdm1_plan *pl, cudaStream_t stream) {
     const pdm1_problem &p = pl->p;
     const dim3 cells(cell_blocks(pl), pl->nbeams);
     box_kernel<<<pl->nbeams, 256, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st);
-    rebox_kernel<<<cells, NT, 0, stream>>>(pl->d_cf, pl->d_st);
     int n = 3;
+    if (pl->cf.learned) {
+        launch_box_moments(pl->d_cf, pl->d_st, pl->cf.grid_ctas, 0, stream);
+        launch_box_learn(pl->d_cf, pl->d_co, pl->d_st, pl->nbeams, stream);
+        n += 2;
+    }
+    rebox_kernel<<<cells, NT, 0, stream>>>(pl->d_cf, pl->d_st);
     if (p.vacuum_aware_cfl) {
         mask_kernel<<<cells, NT, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st);
         ++n;
@@ -925,6 +885,11 @@ int launch_step(pdm1_plan *pl, const StageArgs &a, double *energies, cudaStream_
     if (p.energy_scheme == PDM1_SCHEME_FORWARD_EULER) {
         euler_finish_kernel<<<cell_blocks(pl), NT, 0, stream>>>(a);
         ++launched;
+    }
+    if (pl->cf.rec) {
+        launch_box_moments(pl->d_cf, pl->d_st, grid, 1, stream);
+        launch_record(pl->d_cf, pl->d_co, pl->d_st, stream);
+        launched += 2;
     }
     return launched;
 }
@@ -995,6 +960,9 @@ void destroy_plan(pdm1_plan *pl) {
     cudaFree(pl->d_bufB);
     cudaFree(pl->d_slab);
     cudaFree(pl->d_active);
+    cudaFree(pl->d_model);
+    cudaFree(pl->d_acc);
+    cudaFree(pl->d_plane);
     if (pl->ready) cudaEventDestroy(pl->ready);
     for (cudaEvent_t e : pl->ev)
         if (e) cudaEventDestroy(e);
@@ -1084,10 +1052,12 @@ int create_plan(const pdm1_problem *problem, const pdm1_beam *beams, int nbeams,
     ALLOC(pl->d_U2, B * 4 * cap * sizeof(double));
     ALLOC(pl->d_V, B * 4 * cap * sizeof(double));
     ALLOC(pl->d_q, B * cap * sizeof(double));
+    ALLOC(pl->d_slab, B * (size_t)(p.nx + p.ny + p.nz) * sizeof(unsigned long long));
+    ALLOC(pl->d_acc, B * kAcc * sizeof(double));
+    ALLOC(pl->d_plane, B * (size_t)p.nz * sizeof(double));
     if (p.moving_active_domain) {
         ALLOC(pl->d_bufA, B * 4 * cap * sizeof(double));
         ALLOC(pl->d_bufB, B * 4 * cap * sizeof(double));
-        ALLOC(pl->d_slab, B * (size_t)(p.nx + p.ny + p.nz) * sizeof(unsigned long long));
         ALLOC(pl->d_active, B * cap);
     }
 #undef ALLOC
@@ -1127,6 +1097,12 @@ int create_plan(const pdm1_problem *problem, const pdm1_beam *beams, int nbeams,
     cf.bufB = pl->d_bufB;
     cf.slab = pl->d_slab;
     cf.active = pl->d_active;
+    cf.learned = 0;
+    cf.model = nullptr;
+    cf.acc = pl->d_acc;
+    cf.plane = pl->d_plane;
+    cf.rec = nullptr;
+    cf.rec_max = 0;
     {
         int dev = 0, sms = 148;
         if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -1194,6 +1170,11 @@ int march_impl(pdm1_plan *pl, double *U, double *dose, double *energies, int max
     CUDA_TRY(cudaMemsetAsync(dose, 0, N * sizeof(double), stream));
     if (p.moving_active_domain && !tg.empty())
         CUDA_TRY(cudaMemsetAsync(snap_out, 0, tg.size() * 4 * N * sizeof(double), stream));
+    CUDA_TRY(cudaMemsetAsync(pl->d_acc, 0, (size_t)B * kAcc * sizeof(double), stream));
+    CUDA_TRY(cudaMemsetAsync(pl->d_plane, 0, (size_t)B * p.nz * sizeof(double), stream));
+    CUDA_TRY(cudaMemsetAsync(pl->d_tile_off, 0, (size_t)(B + 1) * sizeof(int), stream));
+    if (!p.moving_active_domain)
+        CUDA_TRY(cudaMemsetAsync(pl->d_slab, 0, (size_t)B * (p.nx + p.ny + p.nz) * sizeof(unsigned long long), stream));
     (void)cudaGetLastError();   // start from a clean launch-error state
     init_kernel<<<B, 32, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, field ? nullptr : energies, -1.0,
                                       p.energy_window_sigma, U, 0);
@@ -1256,7 +1237,10 @@ int march_impl(pdm1_plan *pl, double *U, double *dose, double *energies, int max
     CUDA_TRY(cudaStreamSynchronize(stream));
     int err = 0, max_step = 0;
     double cells = 0.0, max_cells = 0.0;
+    int grows = 0, fallbacks = 0;
     for (int b = 0; b < B; ++b) {
+        grows += pl->h_st[b].grows;
+        fallbacks += pl->h_st[b].fallback != 0;
         err |= pl->h_st[b].error;
         max_step = std::max(max_step, pl->h_st[b].step);
         cells += pl->h_st[b].cell_steps;
@@ -1276,6 +1260,8 @@ int march_impl(pdm1_plan *pl, double *U, double *dose, double *energies, int max
         info->stage_ms = stage_ms;
         info->cell_steps = cells;
         info->max_box_cells = max_cells;
+        info->box_grow_events = grows;
+        info->box_fallbacks = fallbacks;
     }
     if (snap_E_out && !field)
         for (int i = 0; i < pl->h_st[0].taken; ++i) snap_E_out[i] = tg[i];
@@ -1334,6 +1320,44 @@ int pdm1_field_march(pdm1_plan *pl, double *field_dose, int max_steps, int *step
 }
 
 size_t pdm1_plan_workspace_bytes(const pdm1_plan *pl) { return pl ? pl->workspace : 0; }
+
+int pdm1_plan_set_box_model(pdm1_plan *pl, const pdm1_box_model *model) {
+    if (!pl) return set_error(PDM1_ERR_ARGUMENT, "plan is NULL");
+    if (!model) {
+        pl->cf.learned = 0;
+        pl->cf.model = nullptr;
+        return PDM1_OK;
+    }
+    if (!pl->p.moving_active_domain)
+        return set_error(PDM1_ERR_UNSUPPORTED, "a box model needs a plan with moving_active_domain");
+    BoxModelDev h;
+    int rc = pack_box_model(model, h);
+    if (rc) return rc;
+    if (!pl->d_model) CUDA_TRY(cudaMalloc((void **)&pl->d_model, sizeof(BoxModelDev)));
+    CUDA_TRY(cudaMemcpy(pl->d_model, &h, sizeof h, cudaMemcpyHostToDevice));
+    pl->cf.learned = 1;
+    pl->cf.model = pl->d_model;
+    return PDM1_OK;
+}
+
+int pdm1_plan_set_recorder(pdm1_plan *pl, float *rows, int max_rows, double tail_a, double tail_b) {
+    if (!pl) return set_error(PDM1_ERR_ARGUMENT, "plan is NULL");
+    if (!rows) {
+        pl->cf.rec = nullptr;
+        pl->cf.rec_max = 0;
+        return PDM1_OK;
+    }
+    if (pl->p.moving_active_domain || pl->field || pl->nbeams != 1)
+        return set_error(PDM1_ERR_UNSUPPORTED, "the recorder runs on one-beam full-domain plans");
+    if (max_rows < 1) return set_error(PDM1_ERR_ARGUMENT, "max_rows must be positive");
+    if (!(tail_a > 0.0 && tail_a < 1.0 && tail_b > 0.0 && tail_b < 1.0))
+        return set_error(PDM1_ERR_ARGUMENT, "tail tolerances must lie in (0, 1)");
+    pl->cf.rec = rows;
+    pl->cf.rec_max = max_rows;
+    pl->cf.rec_tail_tol[0] = tail_a;
+    pl->cf.rec_tail_tol[1] = tail_b;
+    return PDM1_OK;
+}
 
 int pdm1_march(pdm1_plan *pl, double *U, double *dose, double *energies, int max_steps,
                const double *snap_targets, int n_snap, double *snap_out, double *snap_E_out,

@@ -106,6 +106,16 @@ def _problem_struct(config, material_map, grid, spatial, precision=None):
     return p, keep, materials
 
 
+def _attach_box_model(config, handle) -> None:
+    """Give a plan the configuration's learned box model, if any."""
+    model = getattr(getattr(config, "accel", None), "box_model", None)
+    if model is None:
+        return
+    if not config.numerics.moving_active_domain:
+        raise ValueError("a learned box model needs numerics.moving_active_domain")
+    model.attach(handle)
+
+
 class M1Plan:
     """One beam on one phantom, resident on the GPU (a ``pdm1_plan``)."""
 
@@ -120,6 +130,7 @@ class M1Plan:
         _native.check(_native.lib().pdm1_plan_create(C.byref(p), C.byref(h)))
         self._h = h
         self._keep = keep
+        _attach_box_model(config, h)
 
     def close(self):
         h = getattr(self, "_h", None)
@@ -352,6 +363,11 @@ class FieldPlan:
         h = C.c_void_p()
         _native.check(_native.lib().pdm1_field_plan_create(C.byref(p), descs, len(members),
                                                            int(self.cap), C.byref(h)))
+        try:
+            _attach_box_model(self.config, h)
+        except Exception:
+            _native.lib().pdm1_plan_destroy(h)
+            raise
         return h
 
     def close(self):
