@@ -16,5 +16,16 @@ __all__ = [
     "Beam", "Accel", "Numerics", "OutputConfig", "Physics", "References", "SolverConfig",
     "Backend", "CoefficientInterpolation", "EnergyScheme", "Material", "Precision",
     "Reference", "Scattering", "SpatialScheme", "WaveSpeeds",
-    "Box", "CTScan", "Geometry", "HUPartition",
+    "Box", "CTScan", "Geometry", "HUPartition", "Result", "Solver",
 ]
+
+
+def __getattr__(name):
+    # Solver and Result pull in the march shim; import them on first use
+    if name == "Solver":
+        from .solver import Solver
+        return Solver
+    if name == "Result":
+        from .result import Result
+        return Result
+    raise AttributeError(name)

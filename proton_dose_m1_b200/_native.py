@@ -104,6 +104,9 @@ def lib():
         L.pdm1_hll_batch.argtypes = [_vp, _vp, C.c_int, C.c_int, _vp, C.c_int, _vp]
         L.pdm1_exp_batch.argtypes = [_vp, _vp, C.c_int, _vp]
         L.pdm1_plan_set_box_model.argtypes = [_vp, C.POINTER(BoxModel)]
+        L.pdm1_tile_shape.argtypes = [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.pdm1_plan_set_tile.argtypes = [_vp, C.c_int]
+        L.pdm1_plan_autotune.argtypes = [_vp, C.c_int, C.POINTER(C.c_int), _dp, _vp]
         L.pdm1_plan_set_recorder.argtypes = [_vp, _vp, C.c_int, C.c_double, C.c_double]
         L.pdm1_mlp_train.argtypes = [_vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
                                      C.c_uint, C.POINTER(C.c_float), _vp]
@@ -137,4 +140,6 @@ EXPORTED_SYMBOLS = (
     "pdm1_exp_batch", "pdm1_gamma", "pdm1_last_error", "pdm1_version",
     "pdm1_march_noalloc", "pdm1_plan_set_box_model", "pdm1_plan_set_recorder", "pdm1_mlp_train",
     "pdm1_mlp_gradients", "pdm1_mlp_forward", "pdm1_box_model_infer",
+    "pdm1_tile_shape", "pdm1_plan_set_tile", "pdm1_plan_autotune",
 )
+NUM_TILES = 3

@@ -106,6 +106,9 @@ class OutputConfig:
     store_final_state: bool = True
 
 
+TILE_SHAPES = ((4, 8, 8), (8, 8, 4), (2, 8, 16))
+
+
 @dataclass(frozen=True)
 class Accel:
     """GPU-only knobs.  The defaults reproduce the plain FP64 method."""
@@ -113,8 +116,10 @@ class Accel:
     precision: Precision = Precision.FP64
     # Steps recorded per CUDA graph replay of the march (host syncs once per chunk).
     graph_chunk_steps: int = 32
-    # (tile_x, tile_y, tile_z) override for the stage kernels; None = autotuned/default.
-    tile: tuple[int, int, int] | None = None
+    # Tile shape of the stage kernels: None = 4x8x8, a shape (x, y, z) among
+    # TILE_SHAPES, or "auto" = the fastest shape measured on the plan's problem
+    # by the autotuner (cached per precision, grid and beam count).
+    tile: tuple[int, int, int] | str | None = None
     # Learned moving box (learned_box.BoxModel); None = the fixed heuristic box.
     # Needs numerics.moving_active_domain.
     box_model: object | None = None
@@ -124,6 +129,8 @@ class Accel:
             raise ValueError("precision must be a Precision value.")
         if type(self.graph_chunk_steps) is not int or self.graph_chunk_steps <= 0:
             raise ValueError("graph_chunk_steps must be a positive integer.")
+        if not (self.tile is None or self.tile == "auto" or tuple(self.tile) in TILE_SHAPES):
+            raise ValueError(f"tile must be None, 'auto' or one of {TILE_SHAPES}.")
 
 
 @dataclass

@@ -325,7 +325,7 @@ __global__ void __launch_bounds__(NT) box_moments_kernel(const ConfigDev *cfp, c
     const ConfigDev &cf = *cfp;
     constexpr int kSums = ACC_MAX;   // summed entries; max phi separately
     __shared__ double part[NT / 32][kSums + 1];
-    __shared__ double pl[TZ];
+    __shared__ double pl[kMaxTileZ];
     __shared__ double buf[NT];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int total = record ? sts[0].dom.ntiles : cf.tile_off[cf.nbeams];
@@ -335,6 +335,7 @@ __global__ void __launch_bounds__(NT) box_moments_kernel(const ConfigDev *cfp, c
         const MarchState &st = sts[b];
         const DomainDev d = st.dom;
         if (tile >= d.ntiles) continue;   // same for the whole CTA
+        const int TX = d.tx, TY = d.ty, TZ = d.tz;
         const int tz = tile % d.tiles_z, ty = (tile / d.tiles_z) % d.tiles_y, tx = tile / (d.tiles_z * d.tiles_y);
         const int i0 = tx * TX, j0 = ty * TY, k0 = tz * TZ;
         const int ii = tid / (TY * TZ), jj = (tid / TZ) % TY, kk = tid % TZ;
@@ -484,12 +485,12 @@ __global__ void __launch_bounds__(128) box_learn_kernel(const ConfigDev *cfp, Co
             st->margin[q] = m[q];
         }
         if (st->fallback == 1) {
-            nb = make_domain(0, 0, 0, cf.nx, cf.ny, cf.nz, 1);
+            nb = make_domain(0, 0, 0, cf.nx, cf.ny, cf.nz, 1, cf.tile);
         } else {
             int bi0 = max(st->sig[0] - m[0], 0), bi1 = min(st->sig[1] + m[1], cf.nx);
             int bj0 = max(st->sig[2] - m[2], 0), bj1 = min(st->sig[3] + m[3], cf.ny);
             int bk0 = max(st->sig[4] - m[4], 0), bk1 = min(st->sig[5] + m[5], cf.nz);
-            nb = make_domain(bi0, bj0, bk0, bi1 - bi0, bj1 - bj0, bk1 - bk0, bk0 == 0);
+            nb = make_domain(bi0, bj0, bk0, bi1 - bi0, bj1 - bj0, bk1 - bk0, bk0 == 0, cf.tile);
         }
     }
     for (int q = 0; q < kAcc; ++q) acc[q] = 0.0;

@@ -47,8 +47,15 @@ struct MatDev {
 struct DomainDev {
     int i0, j0, k0;          // origin in the full grid
     int nx, ny, nz;          // extent
+    int tx, ty, tz;          // tile shape of the stage kernels
     int tiles_y, tiles_z, ntiles;
     int inflow;              // the domain's z-min face is the beam entrance (k0 == 0)
+};
+
+// Tile shape (cells) of the stage kernels; every shape holds one cell per
+// thread of a 256-thread CTA.
+struct TileDims {
+    int x, y, z;
 };
 
 // One pencil beam of a march (numerics/boundary.py:63-114): spectrum, angular
@@ -91,6 +98,8 @@ struct ConfigDev {
     unsigned long long *slab;   // max phi per x | y | z slab of the box (double bits), per beam
     unsigned char *active;      // vacuum-aware activity mask on the box, cap per beam
     int grid_ctas;              // persistent grid of the stage kernels
+    TileDims tile;              // tile shape of the stage kernels (kTiles[tile_id])
+    int tile_id;
     int fp32;                   // FP32-stencil form: float eigenvalues in the CFL bound
     // learned moving box and training-data recorder
     int learned;                // a box model proposes the margins
@@ -149,7 +158,8 @@ struct MarchState {
     int margin[6];                 // margins of the last box
 };
 
-__host__ __device__ inline DomainDev make_domain(int i0, int j0, int k0, int nx, int ny, int nz, int inflow);
+__host__ __device__ inline DomainDev make_domain(int i0, int j0, int k0, int nx, int ny, int nz, int inflow,
+                                                 TileDims t);
 
 
 // ---------------------------------------------------------------------------
@@ -202,25 +212,46 @@ __device__ __forceinline__ void source_factor(double ts, double tn, bool inverse
 // ---------------------------------------------------------------------------
 // The fused stage kernel
 // ---------------------------------------------------------------------------
-constexpr int TX = 4, TY = 8, TZ = 8;
-constexpr int NT = TX * TY * TZ;
-constexpr int NFX = (TX + 1) * TY * TZ;
-constexpr int NFY = TX * (TY + 1) * TZ;
-constexpr int NFZ = TX * TY * (TZ + 1);
-constexpr int NF = NFX + NFY + NFZ;
-constexpr int SX = (TX + 6) * TY * TZ;   // x-arm including the core
-constexpr int SY = TX * 6 * TZ;          // y halo
-constexpr int SZ = TX * TY * 6;          // z halo
-template <typename T>
-constexpr size_t stage_smem_bytes() { return sizeof(T) * 4 * (SX + SY + SZ + NF); }
+constexpr int NT = 256;   // threads of a stage CTA = cells of a tile
 
-__host__ __device__ inline DomainDev make_domain(int i0, int j0, int k0, int nx, int ny, int nz, int inflow) {
+// A tile shape: the tile's cells, its cross-shaped 3-cell WENO halo (no
+// corners: WENO reads along one axis at a time) and its faces.  Shared memory
+// holds three arms per component, each the core plus the halo along one axis
+// (the core stored three times), so every 6-point stencil is a strided run in
+// one arm.
+template <int X, int Y, int Z>
+struct Tile {
+    static_assert(X * Y * Z == NT, "one cell per thread");
+    static constexpr int TX = X, TY = Y, TZ = Z;
+    static constexpr int NFX = (X + 1) * Y * Z, NFY = X * (Y + 1) * Z, NFZ = X * Y * (Z + 1);
+    static constexpr int NF = NFX + NFY + NFZ;
+    static constexpr int SX = (X + 6) * Y * Z;   // x-arm loads (core and x halo)
+    static constexpr int SY = X * 6 * Z;         // y halo loads
+    static constexpr int SZ = X * Y * 6;         // z halo loads
+    static constexpr int AX = (X + 6) * Y * Z;   // arm sizes per component
+    static constexpr int AY = X * (Y + 6) * Z;
+    static constexpr int AZ = X * Y * (Z + 6);
+    template <typename T>
+    static constexpr size_t smem_bytes() { return sizeof(T) * 4 * (AX + AY + AZ + NF); }
+};
+
+// The tile shapes the stage kernels are built for, the autotuner's candidates.
+constexpr int kNumTiles = 3;
+using Tile0 = Tile<4, 8, 8>;
+using Tile1 = Tile<8, 8, 4>;
+using Tile2 = Tile<2, 8, 16>;
+constexpr TileDims kTiles[kNumTiles] = {{4, 8, 8}, {8, 8, 4}, {2, 8, 16}};
+constexpr int kMaxTileZ = 16;
+
+__host__ __device__ inline DomainDev make_domain(int i0, int j0, int k0, int nx, int ny, int nz, int inflow,
+                                                 TileDims t) {
     DomainDev d;
     d.i0 = i0; d.j0 = j0; d.k0 = k0;
     d.nx = nx; d.ny = ny; d.nz = nz;
-    d.tiles_y = (ny + TY - 1) / TY;
-    d.tiles_z = (nz + TZ - 1) / TZ;
-    d.ntiles = ((nx + TX - 1) / TX) * d.tiles_y * d.tiles_z;
+    d.tx = t.x; d.ty = t.y; d.tz = t.z;
+    d.tiles_y = (ny + t.y - 1) / t.y;
+    d.tiles_z = (nz + t.z - 1) / t.z;
+    d.ntiles = ((nx + t.x - 1) / t.x) * d.tiles_y * d.tiles_z;
     d.inflow = inflow;
     return d;
 }
@@ -248,14 +279,6 @@ struct SmemT {
     T *X, *Y, *Z, *F;
 };
 
-template <typename T>
-__device__ __forceinline__ T sval(const SmemT<T> &s, int c, int i, int j, int k) {
-    if (j < 0) return s.Y[((c * TX + i) * 6 + (j + 3)) * TZ + k];
-    if (j >= TY) return s.Y[((c * TX + i) * 6 + (j - TY + 3)) * TZ + k];
-    if (k < 0) return s.Z[((c * TX + i) * TY + j) * 6 + (k + 3)];
-    if (k >= TZ) return s.Z[((c * TX + i) * TY + j) * 6 + (k - TZ + 3)];
-    return s.X[((c * (TX + 6) + (i + 3)) * TY + j) * TZ + k];
-}
 
 __device__ __forceinline__ size_t global_cell(const ConfigDev &cf, const DomainDev &d, int li, int lj, int lk) {
     return ((size_t)(d.i0 + li) * cf.ny + (d.j0 + lj)) * cf.nz + (d.k0 + lk);
@@ -371,10 +394,11 @@ __device__ __forceinline__ void atomic_max_double(unsigned long long *target, do
 }
 
 // Per-slab maxima of phi over one tile (moving box): cell values in `buf`
-// (TX*TY*TZ doubles, -1 for cells outside the box).
+// (one per cell of the tile, (i, j, k) with k fastest; -1 outside the box).
 __device__ __forceinline__ void tile_slab_max(const ConfigDev &cf, unsigned long long *slab, const DomainDev &d,
                                               const double *buf, int i0, int j0, int k0) {
     int t = threadIdx.x;
+    const int TX = d.tx, TY = d.ty, TZ = d.tz;
     unsigned long long *sx = slab, *sy = slab + cf.nx, *sz = slab + cf.nx + cf.ny;
     if (t < TX) {
         double m = 0.0;
@@ -508,6 +532,6 @@ int report_error(int code, const char *msg);
 
 // Single-precision stencil kernels (pdm1_stage_fp32.cu, compiled with fast math).
 int stage_fp32_set_attributes();
-void launch_stage_fp32(int mode, int grid, const StageArgs &a, cudaStream_t stream);
+void launch_stage_fp32(int mode, int tile_id, int grid, const StageArgs &a, cudaStream_t stream);
 
 }  // namespace pdm1

@@ -92,7 +92,7 @@ __global__ void init_kernel(const ConfigDev *cfp, Coeffs *cos, MarchState *sts, 
         st->fallback = 0;
         st->grows = 0;
         const bool moving = cf.moving && !full_domain;
-        st->dom = moving ? bm.init_box : make_domain(0, 0, 0, cf.nx, cf.ny, cf.nz, 1);
+        st->dom = moving ? bm.init_box : make_domain(0, 0, 0, cf.nx, cf.ny, cf.nz, 1, cf.tile);
         st->prev = st->dom;
         st->Ua = moving ? cf.bufA + 4 * (size_t)b * cf.cap : U;
         st->Uprev = st->Ua;
@@ -506,7 +506,7 @@ __global__ void __launch_bounds__(256) box_kernel(const ConfigDev *cfp, Coeffs *
             int bi0 = ai0 - g > 0 ? ai0 - g : 0, bi1 = ai1 + g < cf.nx ? ai1 + g : cf.nx;
             int bj0 = aj0 - g > 0 ? aj0 - g : 0, bj1 = aj1 + g < cf.ny ? aj1 + g : cf.ny;
             int bk0 = ak0 - g > 0 ? ak0 - g : 0, bk1 = ak1 + g < cf.nz ? ak1 + g : cf.nz;
-            nb = make_domain(bi0, bj0, bk0, bi1 - bi0, bj1 - bj0, bk1 - bk0, bk0 == 0);
+            nb = make_domain(bi0, bj0, bk0, bi1 - bi0, bj1 - bj0, bk1 - bk0, bk0 == 0, cf.tile);
         }
         switch_box(cf, bm, co, st, b, nb, ed);
     }
@@ -819,19 +819,28 @@ int cell_blocks(const pdm1_plan *pl) {
     return (int)std::max<size_t>(1, std::min<size_t>(b, pl->nbeams > 1 ? 64 : 148 * 8));
 }
 
-// One stage launch in the plan's precision.
+template <class Tl>
+void launch_stage64(int mode, int grid, const StageArgs &a, cudaStream_t stream) {
+    const size_t bytes = Tl::template smem_bytes<double>();
+    switch (mode) {
+    case MODE_A: stage_kernel<double, MODE_A, Tl><<<grid, NT, bytes, stream>>>(a); break;
+    case MODE_B: stage_kernel<double, MODE_B, Tl><<<grid, NT, bytes, stream>>>(a); break;
+    case MODE_C: stage_kernel<double, MODE_C, Tl><<<grid, NT, bytes, stream>>>(a); break;
+    case MODE_EULER: stage_kernel<double, MODE_EULER, Tl><<<grid, NT, bytes, stream>>>(a); break;
+    default: stage_kernel<double, MODE_RHS, Tl><<<grid, NT, bytes, stream>>>(a); break;
+    }
+}
+
+// One stage launch in the plan's precision and tile shape.
 void launch_stage(const pdm1_plan *pl, int mode, int grid, const StageArgs &a, cudaStream_t stream) {
     if (pl->p.precision == PDM1_FP32_FP64) {
-        launch_stage_fp32(mode, grid, a, stream);
+        launch_stage_fp32(mode, pl->cf.tile_id, grid, a, stream);
         return;
     }
-    const size_t bytes = stage_smem_bytes<double>();
-    switch (mode) {
-    case MODE_A: stage_kernel<double, MODE_A><<<grid, NT, bytes, stream>>>(a); break;
-    case MODE_B: stage_kernel<double, MODE_B><<<grid, NT, bytes, stream>>>(a); break;
-    case MODE_C: stage_kernel<double, MODE_C><<<grid, NT, bytes, stream>>>(a); break;
-    case MODE_EULER: stage_kernel<double, MODE_EULER><<<grid, NT, bytes, stream>>>(a); break;
-    default: stage_kernel<double, MODE_RHS><<<grid, NT, bytes, stream>>>(a); break;
+    switch (pl->cf.tile_id) {
+    case 1: launch_stage64<Tile1>(mode, grid, a, stream); break;
+    case 2: launch_stage64<Tile2>(mode, grid, a, stream); break;
+    default: launch_stage64<Tile0>(mode, grid, a, stream); break;
     }
 }
 
@@ -894,14 +903,24 @@ int launch_step(pdm1_plan *pl, const StageArgs &a, double *energies, cudaStream_
     return launched;
 }
 
+template <class Tl>
+cudaError_t set_attributes64() {
+    const int bytes = (int)Tl::template smem_bytes<double>();
+    const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    cudaError_t e = cudaFuncSetAttribute(stage_kernel<double, MODE_A, Tl>, attr, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<double, MODE_B, Tl>, attr, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<double, MODE_C, Tl>, attr, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<double, MODE_EULER, Tl>, attr, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<double, MODE_RHS, Tl>, attr, bytes);
+    return e;
+}
+
 int set_smem_attributes() {
     static bool done = false;
     if (done) return PDM1_OK;
-    CUDA_TRY(cudaFuncSetAttribute(stage_kernel<double, MODE_A>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem_bytes<double>()));
-    CUDA_TRY(cudaFuncSetAttribute(stage_kernel<double, MODE_B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem_bytes<double>()));
-    CUDA_TRY(cudaFuncSetAttribute(stage_kernel<double, MODE_C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem_bytes<double>()));
-    CUDA_TRY(cudaFuncSetAttribute(stage_kernel<double, MODE_EULER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem_bytes<double>()));
-    CUDA_TRY(cudaFuncSetAttribute(stage_kernel<double, MODE_RHS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem_bytes<double>()));
+    CUDA_TRY(set_attributes64<Tile0>());
+    CUDA_TRY(set_attributes64<Tile1>());
+    CUDA_TRY(set_attributes64<Tile2>());
     CUDA_TRY((cudaError_t)stage_fp32_set_attributes());
     done = true;
     return PDM1_OK;
@@ -918,7 +937,7 @@ int device_error_status(int error) {
 int device_error_status(const MarchState &st) { return device_error_status(st.error); }
 
 // Initial box of a beam from its inflow support (moving_active_domain.py:35-60).
-int initial_box(const pdm1_problem &p, const double *spatial, DomainDev &box) {
+int initial_box(const pdm1_problem &p, const double *spatial, TileDims tile, DomainDev &box) {
     int ilo = -1, ihi = -1, jlo = -1, jhi = -1;
     for (int i = 0; i < p.nx; ++i)
         for (int j = 0; j < p.ny; ++j)
@@ -933,7 +952,7 @@ int initial_box(const pdm1_problem &p, const double *spatial, DomainDev &box) {
     int i0 = std::max(0, ilo - g), i1 = std::min(p.nx, ihi + 1 + g);
     int j0 = std::max(0, jlo - g), j1 = std::min(p.ny, jhi + 1 + g);
     int k1 = std::min(p.nz, 1 + g);
-    box = make_domain(i0, j0, 0, i1 - i0, j1 - j0, k1, 1);
+    box = make_domain(i0, j0, 0, i1 - i0, j1 - j0, k1, 1, tile);
     if (k1 < 4) return set_error(PDM1_ERR_ARGUMENT, "WENO-Z inflow extrapolation requires at least four z cells.");
     return PDM1_OK;
 }
@@ -989,6 +1008,8 @@ int create_plan(const pdm1_problem *problem, const pdm1_beam *beams, int nbeams,
     std::vector<std::pair<size_t, int>> fix;
     ConfigDev &cf = pl->cf;
     cf.nx = p.nx; cf.ny = p.ny; cf.nz = p.nz;
+    cf.tile = kTiles[0];
+    cf.tile_id = 0;
     cf.dx = p.dx; cf.dy = p.dy; cf.dz = p.dz;
     cf.nm = p.n_materials;
     cf.scattering = p.scattering;
@@ -1023,9 +1044,9 @@ int create_plan(const pdm1_problem *problem, const pdm1_beam *beams, int nbeams,
         bd.E_beam = beams[b].energy;
         bd.sigma_E = beams[b].energy_spread;
         bd.rf = dd_exp(-(beams[b].angular_spread * beams[b].angular_spread));
-        bd.init_box = make_domain(0, 0, 0, p.nx, p.ny, p.nz, 1);
+        bd.init_box = make_domain(0, 0, 0, p.nx, p.ny, p.nz, 1, cf.tile);
         if (p.moving_active_domain) {
-            rc = initial_box(p, beams[b].inflow_spatial, bd.init_box);
+            rc = initial_box(p, beams[b].inflow_spatial, cf.tile, bd.init_box);
             if (rc) return fail(rc);
             if ((size_t)bd.init_box.nx * bd.init_box.ny * bd.init_box.nz > cap)
                 return fail(set_error(PDM1_ERR_ARGUMENT, "box capacity smaller than a beam's initial box"));
@@ -1108,7 +1129,7 @@ int create_plan(const pdm1_problem *problem, const pdm1_beam *beams, int nbeams,
         if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         // resident CTAs per SM of the stage kernel: 2 in double, 3 in float
         int per_sm = p.precision == PDM1_FP32_FP64 ? 3 : 2;
-        size_t tiles = (size_t)make_domain(0, 0, 0, p.nx, p.ny, p.nz, 1).ntiles * B;
+        size_t tiles = (size_t)make_domain(0, 0, 0, p.nx, p.ny, p.nz, 1, cf.tile).ntiles * B;
         cf.grid_ctas = (int)std::max<size_t>(1, std::min<size_t>(tiles, (size_t)per_sm * sms));
     }
     bool ok = cudaMemcpy(pl->d_tables, blob.data(), blob.size() * sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess &&
@@ -1321,6 +1342,67 @@ int pdm1_field_march(pdm1_plan *pl, double *field_dose, int max_steps, int *step
 
 size_t pdm1_plan_workspace_bytes(const pdm1_plan *pl) { return pl ? pl->workspace : 0; }
 
+int pdm1_tile_shape(int tile_id, int *tx, int *ty, int *tz) {
+    if (tile_id < 0 || tile_id >= kNumTiles) return set_error(PDM1_ERR_ARGUMENT, "unknown tile shape");
+    if (tx) *tx = kTiles[tile_id].x;
+    if (ty) *ty = kTiles[tile_id].y;
+    if (tz) *tz = kTiles[tile_id].z;
+    return PDM1_OK;
+}
+
+int pdm1_plan_set_tile(pdm1_plan *pl, int tile_id) {
+    if (!pl) return set_error(PDM1_ERR_ARGUMENT, "plan is NULL");
+    if (tile_id < 0 || tile_id >= kNumTiles) return set_error(PDM1_ERR_ARGUMENT, "unknown tile shape");
+    const TileDims t = kTiles[tile_id];
+    pl->cf.tile = t;
+    pl->cf.tile_id = tile_id;
+    for (BeamDev &bd : pl->h_beams) {
+        const DomainDev &o = bd.init_box;
+        bd.init_box = make_domain(o.i0, o.j0, o.k0, o.nx, o.ny, o.nz, o.inflow, t);
+    }
+    CUDA_TRY(cudaMemcpy(pl->d_beams, pl->h_beams.data(), pl->h_beams.size() * sizeof(BeamDev), cudaMemcpyHostToDevice));
+    return PDM1_OK;
+}
+
+int pdm1_plan_autotune(pdm1_plan *pl, int steps, int *best_tile, double *ns_per_cell_step, pdm1_stream_t stream) {
+    if (!pl) return set_error(PDM1_ERR_ARGUMENT, "plan is NULL");
+    if (steps < 1) return set_error(PDM1_ERR_ARGUMENT, "steps must be >= 1");
+    const size_t N = (size_t)pl->p.nx * pl->p.ny * pl->p.nz;
+    double *U = nullptr, *dose = nullptr, *energies = nullptr;
+    auto release = [&]() { cudaFree(U); cudaFree(dose); cudaFree(energies); };
+    if (cudaMalloc(&dose, N * sizeof(double)) != cudaSuccess ||
+        (!pl->field && (cudaMalloc(&U, 4 * N * sizeof(double)) != cudaSuccess ||
+                        cudaMalloc(&energies, (size_t)(steps + 2) * sizeof(double)) != cudaSuccess))) {
+        release();
+        return set_error(PDM1_ERR_CUDA, "pdm1_plan_autotune: cudaMalloc failed");
+    }
+    std::vector<int> per_beam(pl->nbeams);
+    double best = 0.0;
+    int best_id = 0, rc = PDM1_OK;
+    // one untimed pass first (clocks, caches), then every candidate
+    for (int pass = -1; pass < kNumTiles && rc == PDM1_OK; ++pass) {
+        const int id = pass < 0 ? 0 : pass;
+        rc = pdm1_plan_set_tile(pl, id);
+        if (rc) break;
+        if (U) {
+            cudaError_t e = cudaMemsetAsync(U, 0, 4 * N * sizeof(double), (cudaStream_t)stream);
+            if (e != cudaSuccess) { rc = set_error(PDM1_ERR_CUDA, cudaGetErrorString(e)); break; }
+        }
+        pdm1_march_info info{};
+        rc = march_impl(pl, U, dose, energies, steps + 1, nullptr, 0, nullptr, nullptr, &info, stream, steps,
+                        per_beam.data());
+        if (rc) break;
+        const double ns = info.cell_steps > 0.0 ? info.stage_ms * 1e6 / info.cell_steps : 0.0;
+        if (pass < 0) continue;
+        if (ns_per_cell_step) ns_per_cell_step[id] = ns;
+        if (pass == 0 || ns < best) { best = ns; best_id = id; }
+    }
+    release();
+    if (rc) return rc;
+    if (best_tile) *best_tile = best_id;
+    return pdm1_plan_set_tile(pl, best_id);
+}
+
 int pdm1_plan_set_box_model(pdm1_plan *pl, const pdm1_box_model *model) {
     if (!pl) return set_error(PDM1_ERR_ARGUMENT, "plan is NULL");
     if (!model) {
@@ -1381,7 +1463,7 @@ static int full_domain_state(pdm1_plan *pl, double *U, double energy, double for
     MarchState st{};
     st.E = energy;
     st.forced_dE = forced_dE;
-    st.dom = make_domain(0, 0, 0, pl->p.nx, pl->p.ny, pl->p.nz, 1);
+    st.dom = make_domain(0, 0, 0, pl->p.nx, pl->p.ny, pl->p.nz, 1, pl->cf.tile);
     st.prev = st.dom;
     st.Ua = U;
     st.Uprev = U;
@@ -1571,14 +1653,14 @@ void launch_step_plain(const pdm1_problem &p, ConfigDev *d_cf, Coeffs *d_co, Mar
                        const StageArgs &a, double *energies, int tiles, cudaStream_t stream) {
     prologue_kernel<<<1, 256, 0, stream>>>(d_cf, d_co, d_st, energies);
     if (p.energy_scheme == PDM1_SCHEME_FORWARD_EULER) {
-        stage_kernel<double, MODE_EULER><<<tiles, NT, stage_smem_bytes<double>(), stream>>>(a);
+        stage_kernel<double, MODE_EULER, Tile0><<<tiles, NT, Tile0::smem_bytes<double>(), stream>>>(a);
         const size_t N = (size_t)p.nx * p.ny * p.nz;
         euler_finish_kernel<<<(int)std::max<size_t>(1, std::min<size_t>((N + NT - 1) / NT, 148 * 8)), NT, 0, stream>>>(a);
         return;
     }
-    stage_kernel<double, MODE_A><<<tiles, NT, stage_smem_bytes<double>(), stream>>>(a);
-    stage_kernel<double, MODE_B><<<tiles, NT, stage_smem_bytes<double>(), stream>>>(a);
-    stage_kernel<double, MODE_C><<<tiles, NT, stage_smem_bytes<double>(), stream>>>(a);
+    stage_kernel<double, MODE_A, Tile0><<<tiles, NT, Tile0::smem_bytes<double>(), stream>>>(a);
+    stage_kernel<double, MODE_B, Tile0><<<tiles, NT, Tile0::smem_bytes<double>(), stream>>>(a);
+    stage_kernel<double, MODE_C, Tile0><<<tiles, NT, Tile0::smem_bytes<double>(), stream>>>(a);
 }
 
 }  // namespace
@@ -1649,10 +1731,10 @@ extern "C" int pdm1_march_noalloc(const pdm1_problem *problem, double *U, double
     if (!g_noalloc_base[dev]) {
         void *ptr = nullptr;
         CUDA_TRY(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
-        CUDA_TRY(cudaFuncSetAttribute(stage_kernel<double, MODE_A>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem_bytes<double>()));
-        CUDA_TRY(cudaFuncSetAttribute(stage_kernel<double, MODE_B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem_bytes<double>()));
-        CUDA_TRY(cudaFuncSetAttribute(stage_kernel<double, MODE_C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem_bytes<double>()));
-        CUDA_TRY(cudaFuncSetAttribute(stage_kernel<double, MODE_EULER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem_bytes<double>()));
+        CUDA_TRY(cudaFuncSetAttribute(stage_kernel<double, MODE_A, Tile0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Tile0::smem_bytes<double>()));
+        CUDA_TRY(cudaFuncSetAttribute(stage_kernel<double, MODE_B, Tile0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Tile0::smem_bytes<double>()));
+        CUDA_TRY(cudaFuncSetAttribute(stage_kernel<double, MODE_C, Tile0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Tile0::smem_bytes<double>()));
+        CUDA_TRY(cudaFuncSetAttribute(stage_kernel<double, MODE_EULER, Tile0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Tile0::smem_bytes<double>()));
         g_noalloc_base[dev] = ptr;
     }
     unsigned char *base = static_cast<unsigned char *>(g_noalloc_base[dev]);
@@ -1664,6 +1746,8 @@ extern "C" int pdm1_march_noalloc(const pdm1_problem *problem, double *U, double
     // the configuration, tables, ids and inflow profile go into the scratch array
     ConfigDev cf{};
     cf.nx = p.nx; cf.ny = p.ny; cf.nz = p.nz;
+    cf.tile = kTiles[0];
+    cf.tile_id = 0;
     cf.dx = p.dx; cf.dy = p.dy; cf.dz = p.dz;
     cf.nm = p.n_materials;
     cf.scattering = p.scattering;
@@ -1684,7 +1768,7 @@ extern "C" int pdm1_march_noalloc(const pdm1_problem *problem, double *U, double
     {
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cf.grid_ctas = std::max(1, std::min(make_domain(0, 0, 0, p.nx, p.ny, p.nz, 1).ntiles, 2 * sms));
+        cf.grid_ctas = std::max(1, std::min(make_domain(0, 0, 0, p.nx, p.ny, p.nz, 1, kTiles[0]).ntiles, 2 * sms));
     }
     cf.ids = reinterpret_cast<const int32_t *>(base + o_ids);
     cf.nbeams = 1;
@@ -1697,7 +1781,7 @@ extern "C" int pdm1_march_noalloc(const pdm1_problem *problem, double *U, double
     bm.sigma_E = p.energy_spread;
     bm.rf = dd_exp(-(p.angular_spread * p.angular_spread));
     bm.spatial = reinterpret_cast<const double *>(base + o_sp);
-    bm.init_box = make_domain(0, 0, 0, p.nx, p.ny, p.nz, 1);
+    bm.init_box = make_domain(0, 0, 0, p.nx, p.ny, p.nz, 1, kTiles[0]);
     for (int m = 0; m < p.n_materials; ++m) {
         const pdm1_material &mt = p.materials[m];
         const pdm1_table *tabs[3] = {&mt.stopping_power, &mt.transport, &mt.nuclear};

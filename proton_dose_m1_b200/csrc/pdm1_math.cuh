@@ -120,6 +120,7 @@ PDM1_HD T weno_left(T v0, T v1, T v2, T v3, T v4) {
         al2 = T(0.3) * (T(1) + r2 * r2);
     }
     T s = al0 + al1 + al2;
+    if (sizeof(T) < sizeof(double)) return (al0 * p0 + al1 * p1 + al2 * p2) / s;   // one division
     T w0 = al0 / s, w1 = al1 / s, w2 = al2 / s;
     return w0 * p0 + w1 * p1 + w2 * p2;
 }

@@ -8,17 +8,21 @@
 
 namespace pdm1 {
 
-template <typename T, int MODE>
+template <typename T, int MODE, class Tl>
 __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 3) stage_kernel(StageArgs a) {
+    constexpr int TX = Tl::TX, TY = Tl::TY, TZ = Tl::TZ;
+    constexpr int NF = Tl::NF, NFX = Tl::NFX, NFY = Tl::NFY;
+    constexpr int SX = Tl::SX, SY = Tl::SY, SZ = Tl::SZ;
+    constexpr int AX = Tl::AX, AY = Tl::AY, AZ = Tl::AZ;
     const ConfigDev &cf = *a.cf;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *smem = reinterpret_cast<T *>(smem_raw);
     __shared__ double slab_buf[NT];   // moving box: phi of the tile's cells
     SmemT<T> s;
-    s.X = smem;
-    s.Y = s.X + 4 * SX;
-    s.Z = s.Y + 4 * SY;
-    s.F = s.Z + 4 * SZ;
+    s.X = smem;            // [c][i + 3][j][k]
+    s.Y = s.X + 4 * AX;    // [c][i][j + 3][k]
+    s.Z = s.Y + 4 * AY;    // [c][i][j][k + 3]
+    s.F = s.Z + 4 * AZ;
     const int tid = threadIdx.x;
     const bool unit = cf.unit_speeds != 0;
     const bool all_axes[3] = {true, true, true};
@@ -45,30 +49,40 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 3) stage
         const int tz = tile % d.tiles_z, ty = (tile / d.tiles_z) % d.tiles_y, tx = tile / (d.tiles_z * d.tiles_y);
         const int i0 = tx * TX, j0 = ty * TY, k0 = tz * TZ;
 
-        // ---- 1. stage the stencil source + halo ----
+        // ---- 1. stage the stencil source + halo (the core into all three arms) ----
         for (int e = tid; e < SX; e += NT) {
             int k = e % TZ, j = (e / TZ) % TY, ii = e / (TZ * TY);
             double u[4];
             load_cell<MODE>(cf, co, d, src, i0 + ii - 3, j0 + j, k0 + k, u);
+            const bool core = ii >= 3 && ii < TX + 3;
 #pragma unroll
-            for (int c = 0; c < 4; ++c) s.X[((c * (TX + 6) + ii) * TY + j) * TZ + k] = T(u[c]);
+            for (int c = 0; c < 4; ++c) {
+                const T v = T(u[c]);
+                s.X[((c * (TX + 6) + ii) * TY + j) * TZ + k] = v;
+                if (core) {
+                    s.Y[((c * TX + ii - 3) * (TY + 6) + j + 3) * TZ + k] = v;
+                    s.Z[((c * TX + ii - 3) * TY + j) * (TZ + 6) + k + 3] = v;
+                }
+            }
         }
         for (int e = tid; e < SY; e += NT) {
             int k = e % TZ, jj = (e / TZ) % 6, i = e / (TZ * 6);
             int gj = jj < 3 ? j0 + jj - 3 : j0 + TY + jj - 3;
+            int aj = jj < 3 ? jj : TY + jj;   // arm index of local j = gj - j0
             double u[4];
             load_cell<MODE>(cf, co, d, src, i0 + i, gj, k0 + k, u);
 #pragma unroll
-            for (int c = 0; c < 4; ++c) s.Y[((c * TX + i) * 6 + jj) * TZ + k] = T(u[c]);
+            for (int c = 0; c < 4; ++c) s.Y[((c * TX + i) * (TY + 6) + aj) * TZ + k] = T(u[c]);
         }
         for (int e = tid; e < SZ; e += NT) {
             int kk = e % 6, j = (e / 6) % TY, i = e / (6 * TY);
             int gk = kk < 3 ? k0 + kk - 3 : k0 + TZ + kk - 3;
+            int ak = kk < 3 ? kk : TZ + kk;
             if (gk < 0) continue;   // z-min ghost, filled below
             double u[4];
             load_cell<MODE>(cf, co, d, src, i0 + i, j0 + j, gk, u);
 #pragma unroll
-            for (int c = 0; c < 4; ++c) s.Z[((c * TX + i) * TY + j) * 6 + kk] = T(u[c]);
+            for (int c = 0; c < 4; ++c) s.Z[((c * TX + i) * TY + j) * (TZ + 6) + ak] = T(u[c]);
         }
         __syncthreads();
         // ---- 2. z-min ghost cells: quartic extrapolation through the inflow ----
@@ -78,9 +92,8 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 3) stage
                 int li = i0 + i, lj = j0 + j;
                 if (li >= nx || lj >= ny) continue;
                 T ui = T(boundary_value<MODE>(a, cf, bm, co, d, c, li, lj));
-                const T *col = &s.X[((c * (TX + 6) + (i + 3)) * TY + j) * TZ];
-                T u0 = col[0], u1 = col[1], u2 = col[2], u3 = col[3];
-                T *z = &s.Z[((c * TX + i) * TY + j) * 6];
+                T *z = &s.Z[((c * TX + i) * TY + j) * (TZ + 6)];
+                T u0 = z[3], u1 = z[4], u2 = z[5], u3 = z[6];
                 z[2] = T(5.0) * ui - T(77.0 / 12.0) * u0 + T(43.0 / 12.0) * u1 - T(17.0 / 12.0) * u2 + T(0.25) * u3;
                 z[1] = T(25.0) * ui - T(505.0 / 12.0) * u0 + T(335.0 / 12.0) * u1 - T(145.0 / 12.0) * u2 + T(9.0 / 4.0) * u3;
                 z[0] = T(75.0) * ui - T(545.0 / 4.0) * u0 + T(395.0 / 4.0) * u1 - T(181.0 / 4.0) * u2 + T(35.0 / 4.0) * u3;
@@ -100,15 +113,22 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 3) stage
                 axis = 2; k = u % (TZ + 1); j = (u / (TZ + 1)) % TY; i = u / ((TZ + 1) * TY);
             }
             T L[4], R[4];
-            const int di = axis == 0, dj = axis == 1, dk = axis == 2;
+            // the six cells along the axis, i - 3 .. i + 2 (face between i - 1 and i),
+            // are arm indices i .. i + 5
+            const T *base;
+            int stride, cs;
+            if (axis == 0) {
+                base = s.X + (i * TY + j) * TZ + k; stride = TY * TZ; cs = AX;
+            } else if (axis == 1) {
+                base = s.Y + (i * (TY + 6) + j) * TZ + k; stride = TZ; cs = AY;
+            } else {
+                base = s.Z + (i * TY + j) * (TZ + 6) + k; stride = 1; cs = AZ;
+            }
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
                 T w[6];
 #pragma unroll
-                for (int q = 0; q < 6; ++q) {
-                    int o = q - 3;
-                    w[q] = sval(s, c, i + o * di, j + o * dj, k + o * dk);
-                }
+                for (int q = 0; q < 6; ++q) w[q] = base[c * cs + q * stride];
                 L[c] = weno_left(w[0], w[1], w[2], w[3], w[4]);
                 R[c] = weno_left(w[5], w[4], w[3], w[2], w[1]);
             }

@@ -106,6 +106,35 @@ def _problem_struct(config, material_map, grid, spatial, precision=None):
     return p, keep, materials
 
 
+_TILE_CACHE: dict = {}
+AUTOTUNE_STEPS = 96
+
+
+def _apply_tile(config, handle, shape, n_beams) -> None:
+    """Set the plan's stage-kernel tile shape from ``config.accel.tile``."""
+    from ..config import TILE_SHAPES
+    tile = getattr(getattr(config, "accel", None), "tile", None)
+    if tile is None:
+        return
+    if tile != "auto":
+        _native.check(_native.lib().pdm1_plan_set_tile(handle, TILE_SHAPES.index(tuple(tile))))
+        return
+    key = (config.accel.precision.name, tuple(shape), n_beams, bool(config.numerics.moving_active_domain))
+    if key not in _TILE_CACHE:
+        torch = _torch()
+        best = C.c_int()
+        ns = (C.c_double * _native.NUM_TILES)()
+        _native.check(_native.lib().pdm1_plan_autotune(handle, AUTOTUNE_STEPS, C.byref(best), ns,
+                                                       C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        _TILE_CACHE[key] = (int(best.value), [float(v) for v in ns])
+    _native.check(_native.lib().pdm1_plan_set_tile(handle, _TILE_CACHE[key][0]))
+
+
+def autotuned_tiles():
+    """The autotuner's choices so far: {(precision, grid, beams, moving): (tile id, ns per cell-step)}."""
+    return dict(_TILE_CACHE)
+
+
 def _attach_box_model(config, handle) -> None:
     """Give a plan the configuration's learned box model, if any."""
     model = getattr(getattr(config, "accel", None), "box_model", None)
@@ -131,6 +160,7 @@ class M1Plan:
         self._h = h
         self._keep = keep
         _attach_box_model(config, h)
+        _apply_tile(config, h, self.shape, 1)
 
     def close(self):
         h = getattr(self, "_h", None)
@@ -365,6 +395,7 @@ class FieldPlan:
                                                            int(self.cap), C.byref(h)))
         try:
             _attach_box_model(self.config, h)
+            _apply_tile(self.config, h, self.shape, len(members))
         except Exception:
             _native.lib().pdm1_plan_destroy(h)
             raise

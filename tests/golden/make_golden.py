@@ -260,11 +260,27 @@ def published(root: Path):
     (OUT / "published_kats.json").write_text(json.dumps(cases, indent=1))
 
 
+def published_configs(root: Path):
+    """The canonical configurations and their hashes from the reference's own
+    run directories (config.json, metadata.json of thesis_results/)."""
+    out = []
+    for meta in sorted((root / "thesis_results").rglob("metadata.json")):
+        d = meta.parent
+        out.append({"source": str(d.relative_to(root)),
+                    "config": json.loads((d / "config.json").read_text()),
+                    "config_hash": json.loads(meta.read_text())["config_hash"]})
+    (OUT / "published_configs.json").write_text(json.dumps(out, indent=1, sort_keys=True))
+
+
 if __name__ == "__main__":
     root = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) > 2 and sys.argv[2] == "configs":
+        published_configs(root)
+        sys.exit(0)
     ps = import_reference(root)
     rng = np.random.default_rng(20261203)
     published(root)
+    published_configs(root)
     unit_vectors(ps, rng)
     operators(ps, rng)
     marches(ps)
