@@ -41,6 +41,8 @@ enum { PDM1_INTERP_LINEAR = 0, PDM1_INTERP_PCHIP = 1 };
 enum { PDM1_SCHEME_FORWARD_EULER = 0, PDM1_SCHEME_SSPRK3 = 1, PDM1_SCHEME_IF_SSPRK3 = 2 };
 enum { PDM1_SPEEDS_EXACT = 0, PDM1_SPEEDS_UNIT = 1 };
 enum { PDM1_FP64 = 0, PDM1_FP32_FP64 = 1 };
+/* reconstruction (Numerics.spatial_scheme; reconstruction_methods/): ghost widths 3, 1, 2, 2 */
+enum { PDM1_SPATIAL_WENO_Z = 0, PDM1_SPATIAL_FIRST_ORDER = 1, PDM1_SPATIAL_MUSCL = 2, PDM1_SPATIAL_WENO3 = 3 };
 
 /* One tabulated coefficient, host memory, strictly increasing energies. */
 typedef struct {
@@ -82,6 +84,7 @@ typedef struct {
     int active_guard_cells;
     double active_relative_tolerance;  /* exp(-sigma_trunc^2 / 2), energy.py:1305 */
     int precision;                     /* PDM1_FP64 or PDM1_FP32_FP64 */
+    int spatial_scheme;                /* PDM1_SPATIAL_*, 0 (WENO-Z) when zero-initialised */
 } pdm1_problem;
 
 /* One pencil beam of a field (numerics/boundary.py:63-114): its spectrum and

@@ -127,6 +127,8 @@ typedef struct {
     double density, X0;
 } mat_t;
 
+enum { ORC_SCHEME_WENO_Z = 0, ORC_SCHEME_FIRST_ORDER = 1, ORC_SCHEME_MUSCL = 2, ORC_SCHEME_WENO3 = 3 };
+
 struct orc_problem {
     orc_problem_desc d;
     double dx, dy, dz;
@@ -680,25 +682,64 @@ void orc_inflow_state(const orc_problem *p, double E, double *st)
     inflow_state(p, &dm, E, st);
 }
 
-/* z-min ghost cells, numerics/boundary.py:247-320 (quartic extrapolation) */
-static void zmin_ghosts(const domain_t *dm, const double *U, const double *bc, double *G)
+/* z-min ghost cells, numerics/boundary.py:117-320: the inflow state itself for
+ * first order (ng = 1, 205-212); the quadratic through U_in and the first two
+ * cell averages for MUSCL / WENO3 (ng = 2, 214-245); the quartic through U_in
+ * and four cell averages for WENO-Z (ng = 3, 247-320).  Ghost g (0-based
+ * from the face) is G[g]; unused ghosts are zero. */
+static void zmin_ghosts(const domain_t *dm, int scheme, const double *U, const double *bc, double *G)
 {
     int nx = dm->nx, ny = dm->ny, nz = dm->nz;
     size_t n2 = (size_t)nx * ny;
+    memset(G, 0, sizeof(double) * 3 * 4 * n2);
     for (int c = 0; c < 4; ++c)
         for (int i = 0; i < nx; ++i)
             for (int j = 0; j < ny; ++j) {
                 double ui = bc[c * n2 + (size_t)i * ny + j];
-                double u0 = U[IDX(c, i, j, 0)], u1 = U[IDX(c, i, j, 1)];
-                double u2 = U[IDX(c, i, j, 2)], u3 = U[IDX(c, i, j, 3)];
                 size_t o = c * n2 + (size_t)i * ny + j;
-                G[0 * 4 * n2 + o] = 5.0 * ui - (77.0 / 12.0) * u0 + (43.0 / 12.0) * u1
-                                    - (17.0 / 12.0) * u2 + 0.25 * u3;
-                G[1 * 4 * n2 + o] = 25.0 * ui - (505.0 / 12.0) * u0 + (335.0 / 12.0) * u1
-                                    - (145.0 / 12.0) * u2 + (9.0 / 4.0) * u3;
-                G[2 * 4 * n2 + o] = 75.0 * ui - (545.0 / 4.0) * u0 + (395.0 / 4.0) * u1
-                                    - (181.0 / 4.0) * u2 + (35.0 / 4.0) * u3;
+                if (scheme == ORC_SCHEME_FIRST_ORDER) {
+                    G[o] = ui;
+                } else if (scheme == ORC_SCHEME_MUSCL || scheme == ORC_SCHEME_WENO3) {
+                    double u0 = U[IDX(c, i, j, 0)], u1 = U[IDX(c, i, j, 1)];
+                    G[0 * 4 * n2 + o] = 3.0 * ui - 2.5 * u0 + 0.5 * u1;
+                    G[1 * 4 * n2 + o] = 9.0 * ui - 10.5 * u0 + 2.5 * u1;
+                } else {
+                    double u0 = U[IDX(c, i, j, 0)], u1 = U[IDX(c, i, j, 1)];
+                    double u2 = U[IDX(c, i, j, 2)], u3 = U[IDX(c, i, j, 3)];
+                    G[0 * 4 * n2 + o] = 5.0 * ui - (77.0 / 12.0) * u0 + (43.0 / 12.0) * u1
+                                        - (17.0 / 12.0) * u2 + 0.25 * u3;
+                    G[1 * 4 * n2 + o] = 25.0 * ui - (505.0 / 12.0) * u0 + (335.0 / 12.0) * u1
+                                        - (145.0 / 12.0) * u2 + (9.0 / 4.0) * u3;
+                    G[2 * 4 * n2 + o] = 75.0 * ui - (545.0 / 4.0) * u0 + (395.0 / 4.0) * u1
+                                        - (181.0 / 4.0) * u2 + (35.0 / 4.0) * u3;
+                }
             }
+}
+
+/* reconstruction_methods/weno3.py:15-62 (WENO3-Z, p = 2) */
+double orc_weno3_left(const double v[3])
+{
+    double p0 = -0.5 * v[0] + 1.5 * v[1];
+    double p1 = 0.5 * v[1] + 0.5 * v[2];
+    double beta0 = (v[1] - v[0]) * (v[1] - v[0]);
+    double beta1 = (v[2] - v[1]) * (v[2] - v[1]);
+    double tau3 = fabs(beta1 - beta0);
+    double r0 = tau3 / (beta0 + 1.0e-12);
+    double r1 = tau3 / (beta1 + 1.0e-12);
+    double alpha0 = (1.0 / 3.0) * (1.0 + r0 * r0);
+    double alpha1 = (2.0 / 3.0) * (1.0 + r1 * r1);
+    double s = alpha0 + alpha1;
+    double w0 = alpha0 / s, w1 = alpha1 / s;
+    return w0 * p0 + w1 * p1;
+}
+
+/* reconstruction_methods/muscl.py:22-44: minmod-limited faces of the centre cell */
+void orc_muscl_faces(double vm, double v0, double vp, double *minus, double *plus)
+{
+    double a = v0 - vm, b = vp - v0, slope = 0.0;
+    if (a * b > 0.0) slope = (a > 0.0 ? 1.0 : -1.0) * (fabs(a) < fabs(b) ? fabs(a) : fabs(b));
+    *minus = v0 - 0.5 * slope;
+    *plus = v0 + 0.5 * slope;
 }
 
 /* Value of the ghost-extended state (numerics/boundary.py:117-399):
@@ -722,21 +763,38 @@ static inline double ext_value(const domain_t *dm, const double *U, const double
 /* Reconstructed, projected left/right states at one interface and the HLL
  * flux through it (weno_z.py:131-321 + flux.py:137-386).  (i,j,k) is the
  * cell on the + side of the interface. */
-static void face_flux(const domain_t *dm, const double *U, const double *G, int axis, int i, int j,
-                      int k, int wave_speeds, double F[4])
+static void face_flux(const domain_t *dm, int scheme, const double *U, const double *G, int axis, int i,
+                      int j, int k, int wave_speeds, double F[4])
 {
     double L[4], R[4];
     int di = axis == 0, dj = axis == 1, dk = axis == 2;
     for (int c = 0; c < 4; ++c) {
+        /* w[s]: cells i-3 .. i+2 along the axis (the face lies between w[2] and w[3]) */
         double w[6];
         for (int s = 0; s < 6; ++s) {
             int o = s - 3;
             w[s] = ext_value(dm, U, G, c, i + o * di, j + o * dj, k + o * dk);
         }
-        double vl[5] = {w[0], w[1], w[2], w[3], w[4]};
-        double vr[5] = {w[5], w[4], w[3], w[2], w[1]};
-        L[c] = orc_weno_left(vl);
-        R[c] = orc_weno_left(vr);
+        if (scheme == ORC_SCHEME_FIRST_ORDER) {          /* first_order.py:66-111 */
+            L[c] = w[2];
+            R[c] = w[3];
+        } else if (scheme == ORC_SCHEME_MUSCL) {         /* muscl.py:86-145 */
+            double lo, hi;
+            orc_muscl_faces(w[1], w[2], w[3], &lo, &hi);
+            L[c] = hi;
+            orc_muscl_faces(w[2], w[3], w[4], &lo, &hi);
+            R[c] = lo;
+        } else if (scheme == ORC_SCHEME_WENO3) {         /* weno3.py:108-171 */
+            double vl[3] = {w[1], w[2], w[3]};
+            double vr[3] = {w[4], w[3], w[2]};
+            L[c] = orc_weno3_left(vl);
+            R[c] = orc_weno3_left(vr);
+        } else {                                          /* weno_z.py:131-321 */
+            double vl[5] = {w[0], w[1], w[2], w[3], w[4]};
+            double vr[5] = {w[5], w[4], w[3], w[2], w[1]};
+            L[c] = orc_weno_left(vl);
+            R[c] = orc_weno_left(vr);
+        }
     }
     orc_project(L);
     orc_project(R);
@@ -748,14 +806,18 @@ static int spatial_operator(const orc_problem *p, const domain_t *dm, const doub
                             const double *bc, double *rhs)
 {
     int nx = dm->nx, ny = dm->ny, nz = dm->nz;
-    if (nz < 4) return fail(ORC_ERR_ARG, "WENO-Z inflow extrapolation requires at least four z cells.");
+    const int scheme = p->d.spatial_scheme;
+    if (scheme == ORC_SCHEME_WENO_Z && nz < 4)
+        return fail(ORC_ERR_ARG, "WENO-Z inflow extrapolation requires at least four z cells.");
+    if ((scheme == ORC_SCHEME_MUSCL || scheme == ORC_SCHEME_WENO3) && nz < 2)
+        return fail(ORC_ERR_ARG, "WENO3 inflow extrapolation requires at least two z cells.");
     size_t n2 = (size_t)nx * ny;
     double *G = malloc(sizeof(double) * 3 * 4 * n2);
     double *Fx = malloc(sizeof(double) * 4 * (size_t)(nx + 1) * ny * nz);
     double *Fy = malloc(sizeof(double) * 4 * (size_t)nx * (ny + 1) * nz);
     double *Fz = malloc(sizeof(double) * 4 * n2 * (nz + 1));
     if (!G || !Fx || !Fy || !Fz) { free(G); free(Fx); free(Fy); free(Fz); return fail(ORC_ERR_ALLOC, "oom"); }
-    zmin_ghosts(dm, U, bc, G);
+    zmin_ghosts(dm, scheme, U, bc, G);
     int ws = p->d.wave_speeds;
     size_t sx = (size_t)(nx + 1) * ny * nz, sy = (size_t)nx * (ny + 1) * nz, sz = n2 * (nz + 1);
 #pragma omp parallel for schedule(static)
@@ -763,7 +825,7 @@ static int spatial_operator(const orc_problem *p, const domain_t *dm, const doub
         for (int j = 0; j < ny; ++j)
             for (int k = 0; k < nz; ++k) {
                 double F[4];
-                face_flux(dm, U, G, 0, i, j, k, ws, F);
+                face_flux(dm, scheme, U, G, 0, i, j, k, ws, F);
                 size_t o = ((size_t)i * ny + j) * nz + k;
                 for (int c = 0; c < 4; ++c) Fx[c * sx + o] = F[c];
             }
@@ -772,7 +834,7 @@ static int spatial_operator(const orc_problem *p, const domain_t *dm, const doub
         for (int j = 0; j <= ny; ++j)
             for (int k = 0; k < nz; ++k) {
                 double F[4];
-                face_flux(dm, U, G, 1, i, j, k, ws, F);
+                face_flux(dm, scheme, U, G, 1, i, j, k, ws, F);
                 size_t o = ((size_t)i * (ny + 1) + j) * nz + k;
                 for (int c = 0; c < 4; ++c) Fy[c * sy + o] = F[c];
             }
@@ -781,7 +843,7 @@ static int spatial_operator(const orc_problem *p, const domain_t *dm, const doub
         for (int j = 0; j < ny; ++j)
             for (int k = 0; k <= nz; ++k) {
                 double F[4];
-                face_flux(dm, U, G, 2, i, j, k, ws, F);
+                face_flux(dm, scheme, U, G, 2, i, j, k, ws, F);
                 size_t o = ((size_t)i * ny + j) * (nz + 1) + k;
                 for (int c = 0; c < 4; ++c) Fz[c * sz + o] = F[c];
             }
@@ -892,7 +954,10 @@ static int energy_step(const orc_problem *p, const domain_t *dm, const double *U
                 for (int i = 0; i < nx; ++i)
                     for (int j = 0; j < ny; ++j)
                         act[IDX(0, i, j, 0)] |= st[(size_t)i * ny + j] > thr;
-                int radius = 3;   /* WENO-Z ghost width, energy.py:614-622 */
+                /* the reconstruction's ghost width, energy.py:611-622 */
+                int sch = p->d.spatial_scheme;
+                int radius = sch == ORC_SCHEME_FIRST_ORDER ? 1
+                             : (sch == ORC_SCHEME_MUSCL || sch == ORC_SCHEME_WENO3) ? 2 : 3;
                 for (int a = 0; a < 3; ++a) {
                     mask[a] = malloc(n);
                     memcpy(mask[a], act, n);

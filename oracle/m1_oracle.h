@@ -67,6 +67,9 @@ typedef struct {
     int moving_active_domain, vacuum_aware_cfl, active_guard_cells;
     double active_truncation_sigma;
     int store_final_state;
+    /* reconstruction (config.py Numerics.spatial_scheme):
+     * 0 WENO_Z, 1 FIRST_ORDER, 2 MUSCL, 3 WENO3 */
+    int spatial_scheme;
 } orc_problem_desc;
 
 typedef struct orc_problem orc_problem;
@@ -78,6 +81,8 @@ const char *orc_last_error(void);
 /* ---- scalar kernels (unit parity) ---------------------------------- */
 double orc_exp(double x);   /* the double-double exp used by the march */
 double orc_weno_left(const double v[5]);
+double orc_weno3_left(const double v[3]);
+void orc_muscl_faces(double vm, double v0, double vp, double *minus, double *plus);
 void   orc_project(double u[4]);
 void   orc_eigenvalues(const double u[4], int axis, double *lmin, double *lmax);
 void   orc_hll_flux(const double left[4], const double right[4], int axis,

@@ -46,7 +46,9 @@ class _ProbDesc(C.Structure):
                 ("energy_min", C.c_double), ("energy_window_sigma", C.c_double),
                 ("moving_active_domain", C.c_int), ("vacuum_aware_cfl", C.c_int),
                 ("active_guard_cells", C.c_int), ("active_truncation_sigma", C.c_double),
-                ("store_final_state", C.c_int)]
+                ("store_final_state", C.c_int), ("spatial_scheme", C.c_int)]
+
+_SPATIAL = {"WENO_Z": 0, "FIRST_ORDER": 1, "MUSCL": 2, "WENO3": 3}
 
 
 def build(force: bool = False) -> Path:
@@ -145,8 +147,8 @@ class OracleProblem:
         from proton_dose_m1_b200.physics.tables import material_tables
 
         geo, beam, phys, num = config.geometry, config.beam, config.physics, config.numerics
-        if num.spatial_scheme.name != "WENO_Z":
-            raise NotImplementedError("the oracle restates the WENO-Z path only")
+        if num.spatial_scheme.name not in _SPATIAL:
+            raise NotImplementedError(f"spatial scheme {num.spatial_scheme.name}")
         if num.energy_scheme.name not in _SCHEME:
             raise NotImplementedError(f"Energy scheme {num.energy_scheme} has not been migrated yet.")
         if material_map is None:
@@ -190,6 +192,7 @@ class OracleProblem:
         d.active_guard_cells = int(num.active_guard_cells)
         d.active_truncation_sigma = num.active_truncation_sigma
         d.store_final_state = int(bool(getattr(config.output, "store_final_state", True)))
+        d.spatial_scheme = _SPATIAL[num.spatial_scheme.name]
         if beam.energy_spread == 0:
             raise ValueError("Zero energy spread is not supported by the Gaussian inflow.")
         self._desc = d

@@ -77,6 +77,8 @@ struct ConfigDev {
     double dx, dy, dz;
     int nm;
     int scattering, nuclear, interp, scheme, unit_speeds;
+    int spatial;         // PDM1_SPATIAL_*: the reconstruction
+    int stencil_radius;  // its ghost width (vacuum-aware CFL masks)
     int use_if;          // integrating factors active (IF_SSPRK3 with sources)
     int strang;          // Strang-split sources around an SSPRK3 / Euler step
     double cfl, max_dE, Emin;

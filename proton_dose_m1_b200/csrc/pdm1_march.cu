@@ -402,9 +402,10 @@ __global__ void __launch_bounds__(NT) cfl_kernel(const ConfigDev *cfp, const Coe
             for (int ax = 0; ax < 3; ++ax) {
                 int lo, hi, pos;
                 size_t stride;
-                if (ax == 0) { pos = li; lo = max(0, li - 3); hi = min(d.nx - 1, li + 3); stride = (size_t)d.ny * d.nz; }
-                else if (ax == 1) { pos = lj; lo = max(0, lj - 3); hi = min(d.ny - 1, lj + 3); stride = d.nz; }
-                else { pos = lk; lo = max(0, lk - 3); hi = min(d.nz - 1, lk + 3); stride = 1; }
+                const int r = cf.stencil_radius;   // the reconstruction's ghost width, energy.py:611-622
+                if (ax == 0) { pos = li; lo = max(0, li - r); hi = min(d.nx - 1, li + r); stride = (size_t)d.ny * d.nz; }
+                else if (ax == 1) { pos = lj; lo = max(0, lj - r); hi = min(d.ny - 1, lj + r); stride = d.nz; }
+                else { pos = lk; lo = max(0, lk - r); hi = min(d.nz - 1, lk + r); stride = 1; }
                 bool any = false;
                 for (int q = lo; q <= hi && !any; ++q) any = act[o + (long long)(q - pos) * (long long)stride] != 0;
                 use[ax] = any;
@@ -738,10 +739,25 @@ TableView add_table(std::vector<double> &blob, std::vector<std::pair<size_t, int
     return v;
 }
 
+// Ghost width of a reconstruction (reconstruction_methods/*.py GHOST_WIDTH)
+// and the z cells its inflow extrapolation needs (boundary.py:214-320).
+int ghost_width(int scheme) {
+    return scheme == PDM1_SPATIAL_FIRST_ORDER ? 1 : (scheme == PDM1_SPATIAL_WENO_Z ? 3 : 2);
+}
+int min_z_cells(int scheme) {
+    return scheme == PDM1_SPATIAL_WENO_Z ? 4 : (scheme == PDM1_SPATIAL_FIRST_ORDER ? 1 : 2);
+}
+const char *z_cells_message(int scheme) {
+    return scheme == PDM1_SPATIAL_WENO_Z ? "WENO-Z inflow extrapolation requires at least four z cells."
+                                         : "WENO3 inflow extrapolation requires at least two z cells.";
+}
+
 int validate_problem(const pdm1_problem *p) {
     if (!p) return set_error(PDM1_ERR_ARGUMENT, "problem is NULL");
     if (p->nx <= 0 || p->ny <= 0 || p->nz <= 0) return set_error(PDM1_ERR_ARGUMENT, "grid dimensions must be positive");
-    if (p->nz < 4) return set_error(PDM1_ERR_ARGUMENT, "WENO-Z inflow extrapolation requires at least four z cells.");
+    if (p->spatial_scheme < PDM1_SPATIAL_WENO_Z || p->spatial_scheme > PDM1_SPATIAL_WENO3)
+        return set_error(PDM1_ERR_UNSUPPORTED, "unknown spatial scheme");
+    if (p->nz < min_z_cells(p->spatial_scheme)) return set_error(PDM1_ERR_ARGUMENT, z_cells_message(p->spatial_scheme));
     if (p->n_materials < 1 || p->n_materials > kMaxMat) return set_error(PDM1_ERR_ARGUMENT, "n_materials must be in 1..16");
     if (!p->materials || !p->ids) return set_error(PDM1_ERR_ARGUMENT, "NULL materials/ids");
     if (!(p->dx > 0 && p->dy > 0 && p->dz > 0)) return set_error(PDM1_ERR_ARGUMENT, "spacings must be positive");
@@ -953,7 +969,7 @@ int initial_box(const pdm1_problem &p, const double *spatial, TileDims tile, Dom
     int j0 = std::max(0, jlo - g), j1 = std::min(p.ny, jhi + 1 + g);
     int k1 = std::min(p.nz, 1 + g);
     box = make_domain(i0, j0, 0, i1 - i0, j1 - j0, k1, 1, tile);
-    if (k1 < 4) return set_error(PDM1_ERR_ARGUMENT, "WENO-Z inflow extrapolation requires at least four z cells.");
+    if (k1 < min_z_cells(p.spatial_scheme)) return set_error(PDM1_ERR_ARGUMENT, z_cells_message(p.spatial_scheme));
     return PDM1_OK;
 }
 
@@ -1012,6 +1028,8 @@ int create_plan(const pdm1_problem *problem, const pdm1_beam *beams, int nbeams,
     cf.tile_id = 0;
     cf.dx = p.dx; cf.dy = p.dy; cf.dz = p.dz;
     cf.nm = p.n_materials;
+    cf.spatial = p.spatial_scheme;
+    cf.stencil_radius = ghost_width(p.spatial_scheme);
     cf.scattering = p.scattering;
     cf.nuclear = p.nuclear ? 1 : 0;
     cf.interp = p.interpolation;
@@ -1750,6 +1768,8 @@ extern "C" int pdm1_march_noalloc(const pdm1_problem *problem, double *U, double
     cf.tile_id = 0;
     cf.dx = p.dx; cf.dy = p.dy; cf.dz = p.dz;
     cf.nm = p.n_materials;
+    cf.spatial = p.spatial_scheme;
+    cf.stencil_radius = ghost_width(p.spatial_scheme);
     cf.scattering = p.scattering;
     cf.nuclear = p.nuclear ? 1 : 0;
     cf.interp = p.interpolation;

@@ -126,6 +126,40 @@ PDM1_HD T weno_left(T v0, T v1, T v2, T v3, T v4) {
 }
 
 // ---------------------------------------------------------------------------
+// WENO3-Z left reconstruction (p = 2), reconstruction_methods/weno3.py:15-62
+// ---------------------------------------------------------------------------
+template <typename T>
+PDM1_HD T weno3_left(T v0, T v1, T v2) {
+    T p0 = T(-0.5) * v0 + T(1.5) * v1;
+    T p1 = T(0.5) * v1 + T(0.5) * v2;
+    T beta0 = (v1 - v0) * (v1 - v0);
+    T beta1 = (v2 - v1) * (v2 - v1);
+    T tau3 = fabs(beta1 - beta0);
+    T r0 = tau3 / (beta0 + T(kWenoEps));
+    T r1 = tau3 / (beta1 + T(kWenoEps));
+    T alpha0 = T(1.0 / 3.0) * (T(1) + r0 * r0);
+    T alpha1 = T(2.0 / 3.0) * (T(1) + r1 * r1);
+    if (sizeof(T) < sizeof(double) && !(alpha0 < T(1e30) && alpha1 < T(1e30))) {
+        // single precision: r^2 overflows; the weights are those of r0^2 : 2 r1^2
+        T m = fmax(r0, r1), q0 = r0 / m, q1 = r1 / m;
+        alpha0 = q0 * q0;
+        alpha1 = T(2) * q1 * q1;
+    }
+    T s = alpha0 + alpha1;
+    T w0 = alpha0 / s, w1 = alpha1 / s;
+    return w0 * p0 + w1 * p1;
+}
+
+// Minmod-limited faces of a cell, reconstruction_methods/muscl.py:22-44.
+template <typename T>
+PDM1_HD void muscl_faces(T vm, T v0, T vp, T &minus, T &plus) {
+    T a = v0 - vm, b = vp - v0, slope = T(0);
+    if (a * b > T(0)) slope = (a > T(0) ? T(1) : T(-1)) * fmin(fabs(a), fabs(b));
+    minus = v0 - T(0.5) * slope;
+    plus = v0 + T(0.5) * slope;
+}
+
+// ---------------------------------------------------------------------------
 // Realizability projection, numerics/realizability.py:132-176
 // ---------------------------------------------------------------------------
 template <typename T>

@@ -94,9 +94,16 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 3) stage
                 T ui = T(boundary_value<MODE>(a, cf, bm, co, d, c, li, lj));
                 T *z = &s.Z[((c * TX + i) * TY + j) * (TZ + 6)];
                 T u0 = z[3], u1 = z[4], u2 = z[5], u3 = z[6];
-                z[2] = T(5.0) * ui - T(77.0 / 12.0) * u0 + T(43.0 / 12.0) * u1 - T(17.0 / 12.0) * u2 + T(0.25) * u3;
-                z[1] = T(25.0) * ui - T(505.0 / 12.0) * u0 + T(335.0 / 12.0) * u1 - T(145.0 / 12.0) * u2 + T(9.0 / 4.0) * u3;
-                z[0] = T(75.0) * ui - T(545.0 / 4.0) * u0 + T(395.0 / 4.0) * u1 - T(181.0 / 4.0) * u2 + T(35.0 / 4.0) * u3;
+                if (cf.spatial == PDM1_SPATIAL_WENO_Z) {   // quartic, boundary.py:247-320
+                    z[2] = T(5.0) * ui - T(77.0 / 12.0) * u0 + T(43.0 / 12.0) * u1 - T(17.0 / 12.0) * u2 + T(0.25) * u3;
+                    z[1] = T(25.0) * ui - T(505.0 / 12.0) * u0 + T(335.0 / 12.0) * u1 - T(145.0 / 12.0) * u2 + T(9.0 / 4.0) * u3;
+                    z[0] = T(75.0) * ui - T(545.0 / 4.0) * u0 + T(395.0 / 4.0) * u1 - T(181.0 / 4.0) * u2 + T(35.0 / 4.0) * u3;
+                } else if (cf.spatial == PDM1_SPATIAL_FIRST_ORDER) {   // boundary.py:205-212
+                    z[2] = ui;
+                } else {   // MUSCL / WENO3: quadratic, boundary.py:214-245
+                    z[2] = T(3.0) * ui - T(2.5) * u0 + T(0.5) * u1;
+                    z[1] = T(9.0) * ui - T(10.5) * u0 + T(2.5) * u1;
+                }
             }
             __syncthreads();
         }
@@ -124,13 +131,34 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 3) stage
             } else {
                 base = s.Z + (i * TY + j) * (TZ + 6) + k; stride = 1; cs = AZ;
             }
+            if (cf.spatial == PDM1_SPATIAL_WENO_Z) {
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                T w[6];
+                for (int c = 0; c < 4; ++c) {
+                    T w[6];
 #pragma unroll
-                for (int q = 0; q < 6; ++q) w[q] = base[c * cs + q * stride];
-                L[c] = weno_left(w[0], w[1], w[2], w[3], w[4]);
-                R[c] = weno_left(w[5], w[4], w[3], w[2], w[1]);
+                    for (int q = 0; q < 6; ++q) w[q] = base[c * cs + q * stride];
+                    L[c] = weno_left(w[0], w[1], w[2], w[3], w[4]);
+                    R[c] = weno_left(w[5], w[4], w[3], w[2], w[1]);
+                }
+            } else {
+                // the narrower stencils read cells i-2 .. i+1 (arm indices i+1 .. i+4)
+                for (int c = 0; c < 4; ++c) {
+                    const T *p = base + c * cs;
+                    const T wm = p[stride], w0 = p[2 * stride], w1 = p[3 * stride], wp = p[4 * stride];
+                    if (cf.spatial == PDM1_SPATIAL_FIRST_ORDER) {   // first_order.py:66-111
+                        L[c] = w0;
+                        R[c] = w1;
+                    } else if (cf.spatial == PDM1_SPATIAL_MUSCL) {   // muscl.py:86-145
+                        T lo, hi;
+                        muscl_faces(wm, w0, w1, lo, hi);
+                        L[c] = hi;
+                        muscl_faces(w0, w1, wp, lo, hi);
+                        R[c] = lo;
+                    } else {   // WENO3, weno3.py:108-171
+                        L[c] = weno3_left(wm, w0, w1);
+                        R[c] = weno3_left(wp, w1, w0);
+                    }
+                }
             }
             project(L[0], L[1], L[2], L[3]);
             project(R[0], R[1], R[2], R[3]);

@@ -26,6 +26,7 @@ _INTERP = {"LINEAR": 0, "PCHIP": 1}
 _SCHEME = {"FORWARD_EULER": 0, "SSPRK3": 1, "IF_SSPRK3": 2}
 _SPEEDS = {"EXACT": 0, "UNIT": 1}
 _PRECISION = {"FP64": 0, "FP32_FP64": 1}
+_SPATIAL = {"WENO_Z": 0, "FIRST_ORDER": 1, "MUSCL": 2, "WENO3": 3}
 
 
 def _to_numpy(a):
@@ -45,9 +46,8 @@ def _torch():
 
 def _check_supported(config) -> None:
     num, phys = config.numerics, config.physics
-    if num.spatial_scheme.name != "WENO_Z":
-        raise NotImplementedError(
-            f"spatial scheme {num.spatial_scheme.name} has no GPU kernel; only WENO_Z is built")
+    if num.spatial_scheme.name not in _SPATIAL:
+        raise NotImplementedError(f"spatial scheme {num.spatial_scheme.name} has no GPU kernel")
     if getattr(num, "active_domain", False):
         raise NotImplementedError("the legacy per-operator active_domain crop has no GPU kernel")
     if num.energy_scheme.name not in _SCHEME:
@@ -103,6 +103,7 @@ def _problem_struct(config, material_map, grid, spatial, precision=None):
     p.active_guard_cells = int(num.active_guard_cells)
     p.active_relative_tolerance = math.exp(-0.5 * num.active_truncation_sigma ** 2)
     p.precision = _PRECISION[precision]
+    p.spatial_scheme = _SPATIAL[num.spatial_scheme.name]
     return p, keep, materials
 
 

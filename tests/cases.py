@@ -30,13 +30,21 @@ def march_specs() -> dict:
     return json.loads((GOLDEN / "marches.json").read_text())
 
 
+def scheme_march_specs() -> dict:
+    """Marches with the first-order, MUSCL and WENO3 reconstructions."""
+    return json.loads((GOLDEN / "scheme_marches.json").read_text())
+
+
+SCHEMES = (SpatialScheme.FIRST_ORDER, SpatialScheme.MUSCL, SpatialScheme.WENO3)
+
+
 def march_config(spec: dict) -> SolverConfig:
     objects = [Box(*o[:6], Material[o[6]]) for o in spec["objects"]]
     beam_kw = {"n_protons": 1e6, "energy": 150.0, "energy_spread": 1.0, "sigma": (0.002, 0.002)}
     beam_kw.update({k: tuple(v) if isinstance(v, list) else v for k, v in spec["beam"].items()})
     phys = Physics(**{k: Scattering[v] if k == "scattering" else v for k, v in spec["physics"].items()})
     num_kw = {"energy_scheme": EnergyScheme.IF_SSPRK3, "cfl": 0.9, "max_energy_step": 0.25}
-    num_kw.update(spec["numerics"])
+    num_kw.update({k: SpatialScheme[v] if k == "spatial_scheme" else v for k, v in spec["numerics"].items()})
     geo = Geometry(size=tuple(spec["size"]), resolution=tuple(spec["resolution"]), objects=objects)
     return SolverConfig(geometry=geo, beam=Beam(**beam_kw), physics=phys, numerics=Numerics(**num_kw))
 

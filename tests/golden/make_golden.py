@@ -214,15 +214,27 @@ MARCHES = {
                                "max_energy_step": 0.5}, ()),
 }
 
+# the other reconstructions of reconstruction_methods/ (ghost widths 1 and 2)
+_HETERO = MARCHES["hetero_snapshots"]
+SCHEME_MARCHES = {
+    f"scheme_{s.lower()}": (*_HETERO[:5], {**_HETERO[5], "spatial_scheme": s}, _HETERO[6])
+    for s in ("FIRST_ORDER", "MUSCL", "WENO3")
+}
+SCHEME_MARCHES["scheme_muscl_moving_vacuum"] = (
+    *MARCHES["moving_box_vacuum_cfl"][:5],
+    {**MARCHES["moving_box_vacuum_cfl"][5], "spatial_scheme": "MUSCL"}, ())
 
-def marches(ps):
+
+def marches(ps, table=None, spec_file="marches.json"):
     from proton_solver import (Box, Beam, Material, Physics, Numerics, Scattering, EnergyScheme,
-                               Solver)
-    for name, (size, res, objs, bk, pk, nk, snaps) in MARCHES.items():
+                               Solver, SpatialScheme)
+    table = MARCHES if table is None else table
+    for name, (size, res, objs, bk, pk, nk, snaps) in table.items():
         objects = [Box(*o[:6], Material[o[6]]) for o in objs]
         beam = Beam(**{"n_protons": 1e6, "energy": 150.0, "energy_spread": 1.0,
                        "sigma": (0.002, 0.002), **bk})
         phys = Physics(**{k: (Scattering[v] if k == "scattering" else v) for k, v in pk.items()})
+        nk = {k: (SpatialScheme[v] if k == "spatial_scheme" else v) for k, v in nk.items()}
         num = Numerics(**{"energy_scheme": EnergyScheme.IF_SSPRK3, "cfl": 0.9,
                           "max_energy_step": 0.25, **nk})
         cfg = _config(ps, size=size, resolution=res, objects=objects, beam=beam, physics=phys,
@@ -236,8 +248,44 @@ def marches(ps):
             out[f"snap{k}"] = s
         np.savez_compressed(OUT / f"march_{name}.npz", **out)
     spec = {n: {"size": v[0], "resolution": v[1], "objects": v[2], "beam": v[3], "physics": v[4],
-                "numerics": v[5], "snapshots": v[6]} for n, v in MARCHES.items()}
-    (OUT / "marches.json").write_text(json.dumps(spec, indent=1))
+                "numerics": v[5], "snapshots": v[6]} for n, v in table.items()}
+    (OUT / spec_file).write_text(json.dumps(spec, indent=1))
+
+
+def schemes(ps):
+    """First-order, MUSCL and WENO3 operators on the state of operators.npz,
+    and marches (scheme_marches.json)."""
+    from proton_solver import Physics, Numerics, Scattering, EnergyScheme, WaveSpeeds, SpatialScheme
+    from proton_solver.numerics.grid import Grid
+    from proton_solver.numerics.boundary import BeamInflow
+    from proton_solver.physics.materials import MaterialMap
+    from proton_solver.numerics.spatial import spatial_operator
+    from proton_solver.numerics import energy as en
+    from proton_solver import Box, Beam, Material
+    g = np.load(OUT / "operators.npz")
+    U, E, dE, bc = g["U"], float(g["E"]), float(g["dE"]), g["bc_custom"]
+    size, res = tuple(g["size"]), tuple(int(n) for n in g["res"])
+    objects = [Box(-0.009, 0.0, -0.01, 0.01, 0.008, 0.016, Material.BONE_COMPACT),
+               Box(0.002, 0.009, -0.01, 0.0, 0.0, 0.024, Material.LUNG)]
+    beam = Beam(n_protons=1e6, energy=100.0, energy_spread=1.5, sigma=(0.003, 0.0025),
+                center=(0.001, -0.0005), angular_spread=0.05)
+    out = {}
+    for s in (SpatialScheme.FIRST_ORDER, SpatialScheme.MUSCL, SpatialScheme.WENO3):
+        cfg = _config(ps, size=size, resolution=res, objects=objects, beam=beam,
+                      physics=Physics(scattering=Scattering.WENTZEL, nuclear=True),
+                      numerics=Numerics(energy_scheme=EnergyScheme.IF_SSPRK3, cfl=0.8, max_energy_step=0.5,
+                                        spatial_scheme=s))
+        grid = Grid.from_geometry(cfg.geometry, np)
+        mm = MaterialMap.from_geometry(cfg.geometry, grid, np)
+        inflow = BeamInflow.from_beam(beam, grid, np)
+        key = s.name.lower()
+        out[f"rhs_{key}"] = spatial_operator(U.copy(), E, grid, inflow, s, WaveSpeeds.EXACT, np)
+        out[f"rhs_bc_{key}"] = spatial_operator(U.copy(), E, grid, inflow, s, WaveSpeeds.EXACT, np,
+                                                boundary_state=bc)
+        Un, ed = en.if_ssprk3(U.copy(), E, dE, mm, grid, inflow, cfg, np)
+        out[f"step_{key}_U"], out[f"step_{key}_edep"] = Un, ed
+    np.savez_compressed(OUT / "schemes.npz", **out)
+    marches(ps, SCHEME_MARCHES, "scheme_marches.json")
 
 
 def published(root: Path):
@@ -278,9 +326,13 @@ if __name__ == "__main__":
         published_configs(root)
         sys.exit(0)
     ps = import_reference(root)
+    if len(sys.argv) > 2 and sys.argv[2] == "schemes":
+        schemes(ps)
+        sys.exit(0)
     rng = np.random.default_rng(20261203)
     published(root)
     published_configs(root)
     unit_vectors(ps, rng)
     operators(ps, rng)
     marches(ps)
+    schemes(ps)

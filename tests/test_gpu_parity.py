@@ -240,3 +240,37 @@ def test_moving_box_follows_the_beam_at_full_size():
     dm, ds = dm.cpu().numpy(), ds.cpu().numpy()
     assert abs(len(em) - len(es)) <= 2
     assert np.abs(dm - ds).max() <= 1e-3 * ds.max()
+
+
+@pytest.mark.parametrize("scheme", cases.SCHEMES, ids=lambda s: s.name)
+def test_other_reconstructions_match_oracle(scheme):
+    """First-order, MUSCL and WENO3 operators and one full step: bit for bit
+    against the oracle, which is pinned to the reference's fixtures."""
+    g = cases.load("operators.npz")
+    E, dE = float(g["E"]), float(g["dE"])
+    cfg = cases.operator_config(spatial_scheme=scheme)
+    plan, _ = make_plan(cfg)
+    orc = O.OracleProblem(cfg)
+    for bc in (None, g["bc_custom"]):
+        np.testing.assert_array_equal(plan.spatial_operator(g["U"], E, bc).cpu().numpy(),
+                                      orc.spatial_operator(g["U"], E, bc))
+    cfg = cases.operator_config("if_full", spatial_scheme=scheme)
+    plan, _ = make_plan(cfg)
+    U, edep = plan.advance(g["U"], E, dE)
+    U_o, edep_o = O.OracleProblem(cfg).advance(g["U"], E, dE)
+    np.testing.assert_array_equal(U.cpu().numpy(), U_o)
+    np.testing.assert_array_equal(edep.cpu().numpy(), edep_o)
+
+
+@pytest.mark.parametrize("name", list(cases.scheme_march_specs()))
+def test_other_reconstruction_marches_match_oracle(name):
+    spec = cases.scheme_march_specs()[name]
+    cfg = cases.march_config(spec)
+    plan, _ = make_plan(cfg)
+    U0 = np.zeros((4, *cfg.geometry.resolution))
+    U, dose, energies, snaps = plan.march(U0, snapshot_energies=tuple(spec["snapshots"]))
+    Uo, dose_o, energies_o, _ = O.OracleProblem(cfg).march(U0, tuple(spec["snapshots"]))
+    np.testing.assert_array_equal(energies, energies_o)
+    np.testing.assert_array_equal(dose.cpu().numpy(), dose_o)
+    g = cases.load(f"march_{name}.npz")
+    assert np.abs(dose.cpu().numpy() - g["dose"]).max() <= cases.REFERENCE_DOSE_RTOL * g["dose"].max()

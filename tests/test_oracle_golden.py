@@ -133,3 +133,33 @@ def test_published_maximum_dose(case):
     p = O.OracleProblem(cfg)
     _, dose, _, _ = p.march(np.zeros((4, *cfg.geometry.resolution)))
     assert abs(dose.max() - kat["maximum_dose_Gy"]) <= cases.REFERENCE_DOSE_RTOL * kat["maximum_dose_Gy"]
+
+
+@pytest.mark.parametrize("scheme", cases.SCHEMES, ids=lambda s: s.name)
+def test_other_reconstructions_operators(scheme):
+    g = cases.load("operators.npz")
+    ref = cases.load("schemes.npz")
+    key = scheme.name.lower()
+    E, dE = float(g["E"]), float(g["dE"])
+    p = O.OracleProblem(cases.operator_config(spatial_scheme=scheme))
+    for name, bc in ((f"rhs_{key}", None), (f"rhs_bc_{key}", g["bc_custom"])):
+        scale = np.abs(ref[name][0]).max()
+        assert np.abs(p.spatial_operator(g["U"], E, bc) - ref[name]).max() / scale < 1e-10, name
+    pf = O.OracleProblem(cases.operator_config("if_full", spatial_scheme=scheme))
+    U, edep = pf.advance(g["U"], E, dE)
+    ref_U, ref_e = ref[f"step_{key}_U"], ref[f"step_{key}_edep"]
+    assert np.abs(U - ref_U).max() / np.abs(ref_U[0]).max() < 1e-11
+    assert np.abs(edep - ref_e).max() / np.abs(ref_e).max() < 1e-11
+
+
+@pytest.mark.parametrize("name", list(cases.scheme_march_specs()))
+def test_other_reconstruction_marches(name):
+    spec = cases.scheme_march_specs()[name]
+    cfg = cases.march_config(spec)
+    p = O.OracleProblem(cfg)
+    U0 = None if cfg.numerics.moving_active_domain else np.zeros((4, *cfg.geometry.resolution))
+    _, dose, energies, snaps = p.march(U0, snapshot_energies=tuple(spec["snapshots"]))
+    g = cases.load(f"march_{name}.npz")
+    np.testing.assert_allclose(energies, g["energies"], rtol=0, atol=1e-12)
+    assert np.abs(dose - g["dose"]).max() <= cases.REFERENCE_DOSE_RTOL * g["dose"].max()
+    assert len(snaps) == len(spec["snapshots"])
