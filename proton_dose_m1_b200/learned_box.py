@@ -164,13 +164,17 @@ def record(config, max_rows: int = 200_000, tails=TAIL_LEVELS):
     return rows[:min(n, max_rows)].cpu().numpy(), dose
 
 
-def samples(rows, level: int = 0, horizon: int = 1):
+def samples(rows, level=0, horizon: int = 1):
     """(features (n, 16), targets (n, 6)) of a recorded march.  The target of
-    step r on each face is how many cells the fluence tail (tail level
-    ``level``) of the next ``horizon`` steps reaches beyond the significant
-    box of step r (negative: it lies inside)."""
+    step r on each face is how many cells the fluence tail of the next
+    ``horizon`` steps reaches beyond the significant box of step r (negative:
+    it lies inside).  ``level`` picks the tail (0: 1e-8, 1: 1e-10 of the
+    maximum; -1: the significant box itself), one for all faces or one per
+    face (x-, x+, y-, y+, z-, z+)."""
+    levels = [level] * 6 if isinstance(level, int) else list(level)
     sig = rows[:, 2:8]
-    tail = rows[:, 27 + 6 * level:33 + 6 * level]
+    col = lambda lv, f: 2 + f if lv < 0 else 27 + 6 * lv + f
+    tail = np.stack([rows[:, col(levels[f], f)] for f in range(6)], axis=1)
     ok = (sig[:, 1] >= 0) & (tail[:, 1] >= 0) & (rows[:, 24] > 0)
     X, T = [], []
     for r in range(len(rows) - horizon):

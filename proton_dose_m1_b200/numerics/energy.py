@@ -396,7 +396,6 @@ class FieldPlan:
                                                            int(self.cap), C.byref(h)))
         try:
             _attach_box_model(self.config, h)
-            _apply_tile(self.config, h, self.shape, len(members))
         except Exception:
             _native.lib().pdm1_plan_destroy(h)
             raise
@@ -442,6 +441,9 @@ class FieldPlan:
             if transient:
                 h = self._create(members)
             try:
+                # tile shape (autotuned on the first march; a box that outgrows
+                # the capacity there is retried like one in the march)
+                _apply_tile(self.config, h, self.shape, len(members))
                 steps = (C.c_int * len(members))()
                 info = _native.MarchInfo()
                 out = dose if w == 0 else partial

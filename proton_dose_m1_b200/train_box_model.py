@@ -89,7 +89,8 @@ def main(argv=None):
     ap.add_argument("--solves", type=int, default=200)
     ap.add_argument("--test-seeds", type=int, nargs="*", default=[1000, 1001, 1002])
     ap.add_argument("--epochs", type=int, default=60)
-    ap.add_argument("--level", type=int, nargs="*", default=[0], help="tail level(s) to train on (0: 1e-8, 1: 1e-10)")
+    ap.add_argument("--level", nargs="*", default=["0"],
+                    help="tail level per variant (0: 1e-8, 1: 1e-10), or six comma-separated per-face levels")
     ap.add_argument("--safety", type=float, nargs="*", default=[1.0])
     ap.add_argument("--margin-min", type=int, default=3)
     ap.add_argument("--out", default=str(learned_box.MODEL_FILE), help="model of the first variant")
@@ -108,7 +109,8 @@ def main(argv=None):
     t_rec = time.perf_counter() - t0
     report = {"record_seconds": t_rec, "solves": len(all_rows), "variants": []}
     first = True
-    for level in args.level:
+    for level_arg in args.level:
+        level = tuple(int(v) for v in level_arg.split(",")) if "," in level_arg else int(level_arg)
         parts = [learned_box.samples(r, level=level) for r in all_rows.values()]
         X = np.concatenate([p[0] for p in parts])
         T = np.concatenate([p[1] for p in parts])
@@ -116,16 +118,20 @@ def main(argv=None):
             t0 = time.perf_counter()
             model, losses = learned_box.train(X, T, epochs=args.epochs, safety=safety, margin_min=args.margin_min)
             t_train = time.perf_counter() - t0
-            model.meta.update({"training_solves": len(all_rows), "tail_level": learned_box.TAIL_LEVELS[level],
+            lv = [level] * 6 if isinstance(level, int) else list(level)
+            model.meta.update({"training_solves": len(all_rows),
+                               "tail_level_per_face": [learned_box.TAIL_LEVELS[v] if v >= 0 else "significant"
+                                                       for v in lv],
                                "record_seconds": t_rec, "train_seconds": t_train,
                                "target_mean": T.mean(0).tolist(), "target_max": T.max(0).tolist()})
-            out = args.out if first else str(Path(args.out).with_suffix("")) + f"_l{level}_s{safety:g}.npz"
+            tag = "".join("s" if v < 0 else str(v) for v in lv)
+            out = args.out if first else str(Path(args.out).with_suffix("")) + f"_l{tag}_s{safety:g}.npz"
             model.save(out)
             first = False
-            print(json.dumps({"level": level, "safety": safety, "samples": len(X), "train_s": t_train,
+            print(json.dumps({"level": lv, "safety": safety, "samples": len(X), "train_s": t_train,
                               "loss_first": float(losses[0]), "loss_last": float(losses[-1]), "out": out}),
                   flush=True)
-            report["variants"].append({"level": level, "safety": safety, "model": model.meta, "out": out,
+            report["variants"].append({"level": lv, "safety": safety, "model": model.meta, "out": out,
                                        "losses": losses.tolist(), "evaluation": evaluate(model, args.test_seeds)})
             if args.report:
                 with open(args.report, "w") as f:

@@ -170,3 +170,21 @@ def test_flux_check_grows_a_box_that_is_too_small():
     score = metrics.compare(d, full, grid)
     assert score["gamma_1pct_1mm_pass_percent"] >= 99.5, score
     assert abs(score["maximum_dose_relative_difference"]) <= 0.005, score
+
+
+@pytest.mark.parametrize("seed", [1003, 1004])
+def test_trained_model_gains_over_the_heuristic_box(seed):
+    """The committed model (trained on 200 full-domain solves, seeds 0-199) on
+    held-out interface phantoms: fewer cells marched than the fixed heuristic
+    box, and the dose within the gate of the full-domain march."""
+    from proton_dose_m1_b200.train_box_model import march
+    cfg = learned_box.training_config(seed)
+    full, _, _, _, _, _, grid = march(cfg, moving=False)
+    heur, _, cs_h, _, _, _, _ = march(cfg, box_model=None)
+    lrn, _, cs_l, grows, fallbacks, _, _ = march(cfg, box_model=learned_box.default_model())
+    assert cs_l <= 0.9 * cs_h, (cs_l, cs_h)
+    for d in (heur, lrn):
+        sc = metrics.compare(d, full, grid)
+        assert sc["gamma_1pct_1mm_pass_percent"] >= 99.5, sc
+        assert abs(sc["maximum_dose_relative_difference"]) <= 0.005, sc
+    assert fallbacks == 0

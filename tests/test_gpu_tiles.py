@@ -94,7 +94,8 @@ def test_auto_tile_field_equals_default_field():
     for tile in (None, "auto"):
         cfg = _cfg(True, tile=tile)
         grid = Grid.from_geometry(cfg.geometry)
-        fp = FieldPlan(cfg, MaterialMap.from_geometry(cfg.geometry, grid), grid, beams)
+        fp = FieldPlan(cfg, MaterialMap.from_geometry(cfg.geometry, grid), grid, beams,
+                       box_capacity_cells=int(np.prod(grid.shape)))
         d, steps = fp.march()
         fp.close()
         doses.append((d.cpu().numpy(), steps))
