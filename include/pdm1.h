@@ -288,6 +288,16 @@ int pdm1_mlp_forward(const float *theta, const float *X, int n, float *Y, pdm1_s
 int pdm1_box_model_infer(const pdm1_box_model *model, const float *features, int n, float *out,
                          pdm1_stream_t stream);
 
+/* Analytical CSDA + straight-streaming dose (proton_solver/analytical.py:173-338),
+ * the reference's reduced-model verifier: available without scattering,
+ * nuclear removal and angular spread (else PDM1_ERR_ARGUMENT).  Range tables of
+ * range_points geometric energies per material (the reference uses 200000),
+ * trapezoid rule over energy_points incident energies (128000); `problem` as
+ * for pdm1_plan_create; dose (device, (nx, ny, nz)) is overwritten.
+ * Synchronises `stream`. */
+int pdm1_analytical_csda_dose(const pdm1_problem *problem, int energy_points, int range_points, double *dose,
+                              pdm1_stream_t stream);
+
 const char *pdm1_last_error(void);
 const char *pdm1_version(void);
 

@@ -113,6 +113,7 @@ def lib():
         L.pdm1_mlp_gradients.argtypes = [_vp, _vp, _vp, C.c_int, C.c_float, _vp, _vp, _vp]
         L.pdm1_mlp_forward.argtypes = [_vp, _vp, C.c_int, _vp, _vp]
         L.pdm1_box_model_infer.argtypes = [C.POINTER(BoxModel), _vp, C.c_int, _vp, _vp]
+        L.pdm1_analytical_csda_dose.argtypes = [C.POINTER(Problem), C.c_int, C.c_int, _vp, _vp]
         L.pdm1_gamma.argtypes = [_vp, _vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                  C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
                                  C.c_double, C.c_double, _vp, _dp, _vp]
@@ -140,6 +141,6 @@ EXPORTED_SYMBOLS = (
     "pdm1_exp_batch", "pdm1_gamma", "pdm1_last_error", "pdm1_version",
     "pdm1_march_noalloc", "pdm1_plan_set_box_model", "pdm1_plan_set_recorder", "pdm1_mlp_train",
     "pdm1_mlp_gradients", "pdm1_mlp_forward", "pdm1_box_model_infer",
-    "pdm1_tile_shape", "pdm1_plan_set_tile", "pdm1_plan_autotune",
+    "pdm1_tile_shape", "pdm1_plan_set_tile", "pdm1_plan_autotune", "pdm1_analytical_csda_dose",
 )
 NUM_TILES = 3

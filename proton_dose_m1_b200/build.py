@@ -30,6 +30,8 @@ UNITS = {
     CSRC / "pdm1_gamma.cu": [],
     # learned moving box: proposer network training and BF16 inference, box kernels
     CSRC / "pdm1_box.cu": [],
+    # analytical CSDA + straight-streaming reference dose
+    CSRC / "pdm1_analytical.cu": [],
 }
 SOURCES = list(UNITS)
 

@@ -672,6 +672,7 @@ std::vector<double> pchip_slopes(const double *E, const double *v, int n) {
 
 namespace pdm1 {
 int report_error(int code, const char *msg) { return set_error(code, msg); }
+std::vector<double> host_pchip_slopes(const double *E, const double *v, int n) { return pchip_slopes(E, v, n); }
 }  // namespace pdm1
 
 struct pdm1_plan {

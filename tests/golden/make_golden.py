@@ -252,6 +252,31 @@ def marches(ps, table=None, spec_file="marches.json"):
     (OUT / spec_file).write_text(json.dumps(spec, indent=1))
 
 
+def analytical(ps):
+    """The reference's analytical CSDA dose on a small slab phantom (analytical.npz)."""
+    from proton_solver import Box, Beam, Material, Numerics, EnergyScheme
+    from proton_solver.numerics.grid import Grid
+    from proton_solver.numerics.boundary import BeamInflow
+    from proton_solver.physics.materials import MaterialMap
+    from proton_solver.analytical import analytical_csda_dose
+    spec = ANALYTICAL_CASE
+    objects = [Box(*o[:6], Material[o[6]]) for o in spec["objects"]]
+    cfg = _config(ps, size=spec["size"], resolution=spec["resolution"], objects=objects,
+                  beam=Beam(**spec["beam"]),
+                  numerics=Numerics(energy_scheme=EnergyScheme.IF_SSPRK3, max_energy_step=0.5))
+    grid = Grid.from_geometry(cfg.geometry, np)
+    mm = MaterialMap.from_geometry(cfg.geometry, grid, np)
+    dose = analytical_csda_dose(cfg, mm, grid, BeamInflow.from_beam(cfg.beam, grid, np))
+    np.savez_compressed(OUT / "analytical.npz", dose=dose, spec=json.dumps(spec))
+
+
+ANALYTICAL_CASE = {"size": (0.02, 0.016, 0.06), "resolution": (10, 8, 60),
+                   "objects": [(-0.01, 0.0, -0.008, 0.008, 0.02, 0.03, "BONE_COMPACT"),
+                               (0.0, 0.01, -0.008, 0.0, 0.035, 0.05, "LUNG")],
+                   "beam": {"n_protons": 1e6, "energy": 60.0, "energy_spread": 0.8, "sigma": (0.003, 0.002),
+                            "center": (0.0015, 0.0)}}
+
+
 def schemes(ps):
     """First-order, MUSCL and WENO3 operators on the state of operators.npz,
     and marches (scheme_marches.json)."""
@@ -329,6 +354,9 @@ if __name__ == "__main__":
     if len(sys.argv) > 2 and sys.argv[2] == "schemes":
         schemes(ps)
         sys.exit(0)
+    if len(sys.argv) > 2 and sys.argv[2] == "analytical":
+        analytical(ps)
+        sys.exit(0)
     rng = np.random.default_rng(20261203)
     published(root)
     published_configs(root)
@@ -336,3 +364,4 @@ if __name__ == "__main__":
     operators(ps, rng)
     marches(ps)
     schemes(ps)
+    analytical(ps)

@@ -69,9 +69,13 @@ def test_save_result_layout(tmp_path):
 
 
 def test_solver_refuses_reference_solutions_it_does_not_hold():
-    from proton_dose_m1_b200 import References, Solver
-    from proton_dose_m1_b200.enums import Reference
-    cfg = SolverConfig(geometry=Geometry(size=(0.01, 0.01, 0.02), resolution=(5, 5, 10)), beam=Beam(),
+    from proton_dose_m1_b200 import Physics, References, Solver
+    from proton_dose_m1_b200.enums import Reference, Scattering
+    geo = Geometry(size=(0.01, 0.01, 0.02), resolution=(5, 5, 10))
+    cfg = SolverConfig(geometry=geo, beam=Beam(), references=References(reference=Reference.BFP_MC))
+    with pytest.raises(NotImplementedError, match="BFP_MC"):
+        Solver(cfg).solve()
+    cfg = SolverConfig(geometry=geo, beam=Beam(), physics=Physics(scattering=Scattering.WENTZEL),
                        references=References(reference=Reference.ANALYTICAL))
-    with pytest.raises(NotImplementedError, match="ANALYTICAL"):
+    with pytest.raises(ValueError, match="Analytical reference is not available"):
         Solver(cfg).solve()
