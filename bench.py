@@ -45,13 +45,15 @@ METRIC = "spots/s at gamma1%/1mm>=99.5% vs plain FP64 GPU path; stage-kernel HBM
 ALG_BYTES_PER_CELL_STEP = {"FP64": 275.0, "FP32_FP64": 275.0}
 FIELDS = {
     "field256": dict(phantom="ellipsoid", seed=4, n_side=16, pitch=5e-3, energy=(70.0, 220.0),
-                     gate_beams=4,
+                     gate_beams=4, precision="fp32",
                      desc="256 spots (16x16 at 5 mm, E~U[70,220] MeV, sigma~U[2,6] mm, sigma_E 1 MeV, "
                           "1e6 protons) on a 128x128x256 @1 mm water phantom with 6-12 seeded ellipsoids "
                           "of water/lung/bone/muscle; Wentzel-VI + nuclear, WENO-Z/HLL/IF-SSPRK3, "
                           "cfl 0.9, max dE 0.5"),
+    # FP64 stencil: the FP32 form misses the 0.5 % maximum-dose bar on this
+    # phantom (0.4-0.9 % on a 150 MeV spot through the adipose shell and bone ring)
     "pelvis1024": dict(phantom="pelvis", seed=5, n_side=32, pitch=3e-3, energy=(70.0, 230.0),
-                       gate_beams=3,
+                       gate_beams=3, precision="fp64",
                        desc="1024 spots (32x32 at 3 mm, E~U[70,230] MeV, sigma~U[2,6] mm, sigma_E 1 MeV, "
                             "1e6 protons) on a 256x256x320 @1 mm synthetic pelvis (water/muscle body, "
                             "ADIPOSE_SYNTH shell = water scaled to 950 kg/m3, bone ring, two bone femoral "
@@ -257,8 +259,11 @@ def estimated_step_count(cfg) -> int:
 
 # Cell-steps of the moving-box march of each workload (per spot for single-spot
 # workloads, per field for fields): the work the reference's fastest CPU mode
-# (moving active box) does, measured by the GPU march.
-MOVING_CELL_STEPS = {}
+# (its moving active box) does.  Measured by this library's moving-box march of
+# the workload with the reference's box rule: slab80 in FP64 (the same boxes as
+# the reference, bit for bit), the fields in the FP32 form (boxes within 0.1 %
+# of the FP64 ones on slab80).
+MOVING_CELL_STEPS = {"slab80": 302_300_556.0, "field256": 3.2113e10, "pelvis1024": 1.1100e11}
 
 
 def run_reference(args, rank, world):
@@ -309,6 +314,10 @@ def run_reference(args, rank, world):
 # fewer cells on its training distribution, but its per-step kernels cost more
 # than the cells they save in the FP32 form; see the learned-box profile).
 BOX = "heuristic"
+# Stencil arithmetic of the accelerated form (--precision): "fp32" (FP32
+# stencil / FP64 dose) or "fp64".  Field workloads override the default with
+# their own (FIELDS[...]["precision"]).
+PRECISION = "fp32"
 
 
 def accelerated_config(cfg):
@@ -318,13 +327,15 @@ def accelerated_config(cfg):
     from proton_dose_m1_b200 import Accel, SolverConfig, learned_box
     from proton_dose_m1_b200.enums import Precision
     model = learned_box.default_model() if BOX == "learned" else None
+    precision = Precision.FP32_FP64 if PRECISION == "fp32" else Precision.FP64
     return SolverConfig(geometry=cfg.geometry, beam=cfg.beam, physics=cfg.physics,
                         numerics=replace(cfg.numerics, moving_active_domain=True),
-                        accel=Accel(precision=Precision.FP32_FP64, box_model=model, tile="auto"))
+                        accel=Accel(precision=precision, box_model=model, tile="auto", phantom_cfl=True))
 
 
 def accelerated_label():
-    return (f"moving active box ({BOX}) + FP32 stencil / FP64 dose + autotuned tile")
+    arith = "FP32 stencil / FP64 dose" if PRECISION == "fp32" else "FP64"
+    return f"moving active box ({BOX}, phantom-wide CFL bound) + {arith} + autotuned tile"
 
 
 def run_ours(args, cfg, desc, rank, world, local_rank):
@@ -601,7 +612,7 @@ def run_field(args, rank, world, local_rank):
         "metric": METRIC, "value": value, "unit": "spots/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
-        "dtype": "f32 stencil / f64 dose",
+        "dtype": "f32 stencil / f64 dose" if PRECISION == "fp32" else "f64",
         "data": "synthetic (seeded phantom and spots, no dataset)",
         "config": {"workload": args.workload, "description": desc,
                    "method": "batched field, " + accelerated_label(),
@@ -615,7 +626,8 @@ def run_field(args, rank, world, local_rank):
         "gate": gate,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
-                     "kernel": "stage_kernel<float> (A/B/C), all spots per launch",
+                     "kernel": f"stage_kernel<{'float' if PRECISION == 'fp32' else 'double'}> (A/B/C), "
+                               "all spots per launch",
                      "avg_launch_ms": stage_ms / max(stage_launches, 1),
                      "algorithmic_bytes_per_launch": alg_total / max(stage_launches, 1),
                      "algorithmic_bytes_per_cell_step": ALG_BYTES_PER_CELL_STEP["FP32_FP64"],
@@ -646,11 +658,14 @@ def main():
                     help="only run the first K energy steps of one spot (for ncu captures) and exit")
     ap.add_argument("--box", choices=("learned", "heuristic"), default="heuristic",
                     help="moving box of the accelerated form")
+    ap.add_argument("--precision", choices=("fp32", "fp64"), default=None,
+                    help="stencil arithmetic of the accelerated form (default: fp32; fields: their own)")
     ap.add_argument("--profile-spots", type=int, default=0,
                     help="field workloads: march K spots of the field once (for ncu captures) and exit")
     args = ap.parse_args()
-    global BOX
+    global BOX, PRECISION
     BOX = args.box
+    PRECISION = args.precision or (FIELDS[args.workload]["precision"] if args.workload in FIELDS else "fp32")
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -85,6 +85,9 @@ typedef struct {
     double active_relative_tolerance;  /* exp(-sigma_trunc^2 / 2), energy.py:1305 */
     int precision;                     /* PDM1_FP64 or PDM1_FP32_FP64 */
     int spatial_scheme;                /* PDM1_SPATIAL_*, 0 (WENO-Z) when zero-initialised */
+    int phantom_cfl_floor;             /* moving box: bound the CFL step by the vacuum cells of
+                                          the whole phantom, as a full-domain march is (no
+                                          reference counterpart; 0 = the reference's rule) */
 } pdm1_problem;
 
 /* One pencil beam of a field (numerics/boundary.py:63-114): its spectrum and

@@ -41,7 +41,7 @@ class Problem(C.Structure):
                 ("energy_min", C.c_double), ("energy_window_sigma", C.c_double),
                 ("moving_active_domain", C.c_int), ("vacuum_aware_cfl", C.c_int),
                 ("active_guard_cells", C.c_int), ("active_relative_tolerance", C.c_double),
-                ("precision", C.c_int), ("spatial_scheme", C.c_int)]
+                ("precision", C.c_int), ("spatial_scheme", C.c_int), ("phantom_cfl_floor", C.c_int)]
 
 
 class BeamDesc(C.Structure):

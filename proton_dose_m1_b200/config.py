@@ -123,6 +123,12 @@ class Accel:
     # Learned moving box (learned_box.BoxModel); None = the fixed heuristic box.
     # Needs numerics.moving_active_domain.
     box_model: object | None = None
+    # Moving box: bound every energy step by the vacuum speed in the phantom's
+    # material of least stopping power, as the full-domain march does (its
+    # cells outside the beam hold no fluence), so the moving box follows the
+    # plain method's step sequence.  False = the reference's rule (the bound
+    # over the box only).
+    phantom_cfl: bool = False
 
     def __post_init__(self):
         if not isinstance(self.precision, Precision):

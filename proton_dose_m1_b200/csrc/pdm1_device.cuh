@@ -77,6 +77,8 @@ struct ConfigDev {
     double dx, dy, dz;
     int nm;
     int scattering, nuclear, interp, scheme, unit_speeds;
+    int cfl_floor;       // moving box: CFL bound at least the phantom's vacuum bound
+    unsigned present;    // bit m: material m occurs in the phantom
     int spatial;         // PDM1_SPATIAL_*: the reconstruction
     int stencil_radius;  // its ghost width (vacuum-aware CFL masks)
     int use_if;          // integrating factors active (IF_SSPRK3 with sources)
@@ -102,7 +104,7 @@ struct ConfigDev {
     int grid_ctas;              // persistent grid of the stage kernels
     TileDims tile;              // tile shape of the stage kernels (kTiles[tile_id])
     int tile_id;
-    int fp32;                   // FP32-stencil form: float eigenvalues in the CFL bound
+    int fp32;                   // FP32-stencil form: float eigenvalues in the CFL bound (not with cfl_floor)
     // learned moving box and training-data recorder
     int learned;                // a box model proposes the margins
     const BoxModelDev *model;

@@ -414,8 +414,20 @@ __global__ void __launch_bounds__(NT) cfl_kernel(const ConfigDev *cfp, const Coe
         double phi_in = 0.0;
         if (lk == 0 && d.inflow) phi_in = bm.spatial[(size_t)(d.i0 + li) * cf.ny + (d.j0 + lj)] * ed;
         double s = S[cf.ids[global_cell(cf, d, li, lj, lk)]];
-        inv = fmax(inv, cf.fp32 ? cfl_term<float>(cf, bm.rf, u, s, lk == 0, phi_in, use)
-                                : cfl_term<double>(cf, bm.rf, u, s, lk == 0, phi_in, use));
+        // the FP32 form takes float speeds, except with the phantom-wide bound,
+        // whose purpose is the plain method's step sequence
+        inv = fmax(inv, cf.fp32 && !cf.cfl_floor ? cfl_term<float>(cf, bm.rf, u, s, lk == 0, phi_in, use)
+                                                 : cfl_term<double>(cf, bm.rf, u, s, lk == 0, phi_in, use));
+    }
+    if (cf.cfl_floor && use_box_coeffs && blockIdx.x == 0 && threadIdx.x == 0) {
+        // the cells outside the box hold no fluence; on the full grid they would
+        // bound the step with the vacuum speed (wave_speeds.py:36-103) in the
+        // material of least stopping power
+        double smin = INFINITY;
+        for (int m = 0; m < cf.nm; ++m)
+            if (cf.present >> m & 1u) smin = fmin(smin, S[m]);
+        const double a = cf.unit_speeds ? 1.0 : 1.0 / sqrt(3.0);
+        inv = fmax(inv, a / (smin * cf.dx) + a / (smin * cf.dy) + a / (smin * cf.dz));
     }
     block_max_atomic(inv, &st->inv_bits);
 }
@@ -1031,6 +1043,8 @@ int create_plan(const pdm1_problem *problem, const pdm1_beam *beams, int nbeams,
     cf.nm = p.n_materials;
     cf.spatial = p.spatial_scheme;
     cf.stencil_radius = ghost_width(p.spatial_scheme);
+    cf.cfl_floor = p.moving_active_domain && p.phantom_cfl_floor ? 1 : 0;
+    cf.present = 0u;
     cf.scattering = p.scattering;
     cf.nuclear = p.nuclear ? 1 : 0;
     cf.interp = p.interpolation;
@@ -1071,6 +1085,7 @@ int create_plan(const pdm1_problem *problem, const pdm1_beam *beams, int nbeams,
                 return fail(set_error(PDM1_ERR_ARGUMENT, "box capacity smaller than a beam's initial box"));
         }
     }
+    for (size_t c = 0; c < N; ++c) cf.present |= 1u << problem->ids[c];
     cudaError_t e;
 #define ALLOC(ptr, bytes)                                                      \
     e = cudaMalloc((void **)&(ptr), (bytes));                                  \
@@ -1771,6 +1786,8 @@ extern "C" int pdm1_march_noalloc(const pdm1_problem *problem, double *U, double
     cf.nm = p.n_materials;
     cf.spatial = p.spatial_scheme;
     cf.stencil_radius = ghost_width(p.spatial_scheme);
+    cf.cfl_floor = p.moving_active_domain && p.phantom_cfl_floor ? 1 : 0;
+    cf.present = 0u;
     cf.scattering = p.scattering;
     cf.nuclear = p.nuclear ? 1 : 0;
     cf.interp = p.interpolation;

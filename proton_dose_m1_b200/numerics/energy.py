@@ -104,6 +104,8 @@ def _problem_struct(config, material_map, grid, spatial, precision=None):
     p.active_relative_tolerance = math.exp(-0.5 * num.active_truncation_sigma ** 2)
     p.precision = _PRECISION[precision]
     p.spatial_scheme = _SPATIAL[num.spatial_scheme.name]
+    accel = getattr(config, "accel", None)
+    p.phantom_cfl_floor = int(bool(getattr(accel, "phantom_cfl", False)))
     return p, keep, materials
 
 
@@ -473,6 +475,15 @@ class FieldPlan:
         return dose, steps
 
 
+def _to_host(t):
+    """Device tensor -> NumPy through page-locked memory (the caching host
+    allocator reuses the buffer across calls); the array keeps it alive."""
+    torch = _torch()
+    out = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+    out.copy_(t)
+    return out.numpy()
+
+
 def field_march(config, material_map, grid, beams, box_capacity_cells: int = 0):
     """Dose of a spot-scanning field (host NumPy in, host NumPy out).
 
@@ -483,7 +494,7 @@ def field_march(config, material_map, grid, beams, box_capacity_cells: int = 0):
     plan = FieldPlan(config, material_map, grid, beams, box_capacity_cells)
     try:
         dose, steps = plan.march()
-        return dose.cpu().numpy(), steps
+        return _to_host(dose), steps
     finally:
         plan.close()
 
@@ -507,6 +518,6 @@ def energy_march(U: Any, material_map, grid, inflow, config, xp=None,
     if config.numerics.moving_active_domain and not store:
         Ud = None
     if host:
-        conv = lambda t: None if t is None else t.cpu().numpy()
+        conv = lambda t: None if t is None else _to_host(t)
         return conv(Ud), conv(dose), energies, {e: conv(s) for e, s in snaps.items()}
     return Ud, dose, energies, snaps

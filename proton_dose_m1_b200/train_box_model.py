@@ -26,8 +26,8 @@ import numpy as np
 from . import learned_box, metrics
 
 
-def march(config, box_model=None, moving=True):
-    """(dose (host), energy steps, cell-steps, grow events, fallbacks, seconds)."""
+def march(config, box_model=None, moving=True, phantom_cfl=False):
+    """(dose, energy steps, cell-steps, grow events, fallbacks, seconds, grid)."""
     import torch
     from .config import Accel, SolverConfig
     from .numerics.boundary import BeamInflow
@@ -36,7 +36,8 @@ def march(config, box_model=None, moving=True):
     from .physics.materials import MaterialMap
     cfg = SolverConfig(geometry=config.geometry, beam=config.beam, physics=config.physics,
                        numerics=replace(config.numerics, moving_active_domain=moving),
-                       accel=Accel(precision=config.accel.precision, box_model=box_model))
+                       accel=Accel(precision=config.accel.precision, box_model=box_model,
+                                   phantom_cfl=phantom_cfl))
     grid = Grid.from_geometry(cfg.geometry)
     mm = MaterialMap.from_geometry(cfg.geometry, grid)
     plan = M1Plan(cfg, mm, grid, BeamInflow.from_beam(cfg.beam, grid))
@@ -54,25 +55,29 @@ def march(config, box_model=None, moving=True):
 _REFERENCE = {}
 
 
-def _reference(seed):
+def _reference(seed, phantom_cfl=False):
     """Full-domain dose and the heuristic-box march of a seed (cached)."""
     if seed not in _REFERENCE:
         cfg = learned_box.training_config(seed)
         full, n_full, cs_full, _, _, t_full, grid = march(cfg, moving=False)
-        _REFERENCE[seed] = (cfg, full, grid, {"steps": n_full, "cell_steps": cs_full, "seconds": t_full},
-                            march(cfg, box_model=None))
-    return _REFERENCE[seed]
+        _REFERENCE[seed] = (cfg, full, grid, {"steps": n_full, "cell_steps": cs_full, "seconds": t_full})
+    if (seed, phantom_cfl) not in _REFERENCE:
+        cfg = _REFERENCE[seed][0]
+        _REFERENCE[seed, phantom_cfl] = march(cfg, box_model=None, phantom_cfl=phantom_cfl)
+    return (*_REFERENCE[seed], _REFERENCE[seed, phantom_cfl])
 
 
-def evaluate(model, seeds):
-    """Learned box vs heuristic box on held-out seeds (FP64 throughout)."""
+def evaluate(model, seeds, phantom_cfl=False):
+    """Learned box vs heuristic box on held-out seeds (FP64 throughout); with
+    ``phantom_cfl`` both boxes take the phantom-wide CFL bound."""
     rows = []
     for s in seeds:
-        cfg, full, grid, full_info, heuristic = _reference(s)
+        cfg, full, grid, full_info, heuristic = _reference(s, phantom_cfl)
         entry = {"seed": s, "energy_MeV": cfg.beam.energy, "sigma_mm": cfg.beam.sigma[0] * 1e3,
-                 "full": full_info}
+                 "full": full_info, "phantom_cfl": phantom_cfl}
         for name, bm in (("heuristic", None), ("learned", model)):
-            d, n, cs, grows, fb, t, _ = heuristic if bm is None else march(cfg, box_model=bm)
+            d, n, cs, grows, fb, t, _ = (heuristic if bm is None
+                                         else march(cfg, box_model=bm, phantom_cfl=phantom_cfl))
             sc = metrics.compare(d, full, grid)
             diff = (d - full)
             entry[name] = {"steps": n, "cell_steps": cs, "grow_events": grows, "fallbacks": fb, "seconds": t,
@@ -96,7 +101,17 @@ def main(argv=None):
     ap.add_argument("--out", default=str(learned_box.MODEL_FILE), help="model of the first variant")
     ap.add_argument("--report", default=None)
     ap.add_argument("--rows", default=None, help="recorded rows: load from this npz if it exists, else save to it")
+    ap.add_argument("--evaluate", default=None, help="only evaluate this model file on the test seeds")
+    ap.add_argument("--phantom-cfl", action="store_true", help="evaluate with the phantom-wide CFL bound")
     args = ap.parse_args(argv)
+    if args.evaluate:
+        report = {"model": args.evaluate, "phantom_cfl": args.phantom_cfl,
+                  "evaluation": evaluate(learned_box.BoxModel.load(args.evaluate), args.test_seeds,
+                                         args.phantom_cfl)}
+        if args.report:
+            with open(args.report, "w") as f:
+                json.dump(report, f, indent=1)
+        return report
     from pathlib import Path
     t0 = time.perf_counter()
     if args.rows and Path(args.rows).exists():
