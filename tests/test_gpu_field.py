@@ -91,3 +91,32 @@ def test_fp32_field_gate_against_plain_fp64():
     score = metrics.compare(dose, plain, grid)
     assert score["gamma_1pct_1mm_pass_percent"] >= 99.5, score
     assert abs(score["maximum_dose_relative_difference"]) <= 0.005, score
+
+
+def test_phantom_cfl_bound_follows_the_full_domain_steps():
+    """A low-stopping-power block (ADIPOSE_SYNTH, 0.95 x water) outside the
+    beam bounds every energy step of the full-domain march through its empty
+    cells; the reference's box rule ignores it, the phantom-wide bound
+    reproduces the full-domain energies exactly."""
+    geo = Geometry(size=(0.04, 0.04, 0.06), resolution=(40, 40, 60),
+                   objects=[Box(0.017, 0.02, -0.02, 0.02, 0.0, 0.06, Material.ADIPOSE_SYNTH)])
+    beam = Beam(n_protons=1e6, energy=60.0, energy_spread=1.0, sigma=(0.0015, 0.0015))
+    grid = Grid.from_geometry(geo)
+    mm = MaterialMap.from_geometry(geo, grid)
+    inflow = BeamInflow.from_beam(beam, grid)
+    out = {}
+    for name, moving, floor in (("full", False, False), ("box", True, False), ("floor", True, True)):
+        cfg = SolverConfig(geometry=geo, beam=beam, physics=Physics(scattering=Scattering.WENTZEL, nuclear=True),
+                           numerics=Numerics(energy_scheme=EnergyScheme.IF_SSPRK3, cfl=0.9, max_energy_step=0.5,
+                                             moving_active_domain=moving),
+                           accel=Accel(phantom_cfl=floor))
+        plan = M1Plan(cfg, mm, grid, inflow)
+        U = None if moving else torch.zeros((4, *grid.shape), dtype=torch.float64, device="cuda")
+        _, dose, E, _ = plan.march(U)
+        plan.close()
+        out[name] = (dose.cpu().numpy(), E)
+    np.testing.assert_array_equal(out["floor"][1], out["full"][1])
+    assert len(out["box"][1]) < len(out["full"][1])
+    full = out["full"][0]
+    err = {k: np.abs(out[k][0] - full).max() / full.max() for k in ("box", "floor")}
+    assert err["floor"] < err["box"], err
