@@ -43,6 +43,15 @@ METRIC = "spots/s at gamma1%/1mm>=99.5% vs plain FP64 GPU path; stage-kernel HBM
 # states are stored in double in both precision modes (the FP32 form converts
 # on load), so the count is the same for both.
 ALG_BYTES_PER_CELL_STEP = {"FP64": 275.0, "FP32_FP64": 275.0}
+# Algorithmic floating-point operations per cell-step of the WENO-Z march:
+# three stages x (three owned faces x (8 reconstructions, 2 projections, HLL
+# with both closures and wave-speed pairs) + divergence and stage update),
+# each +, -, *, / and sqrt counted once (oracle/flops.py tallies them; the
+# CPU test suite keeps the two equal).
+FLOPS_PER_CELL_STEP = 7479
+# Non-tensor peaks of the CUDA cores: 148 SMs x lanes per SM x 2 (FMA) x the
+# 1965 MHz maximum SM clock; nominal, no measured figure exists for them.
+CORE_PEAK_TFLOPS = {"FP32_FP64": 148 * 128 * 2 * 1.965e-3, "FP64": 148 * 64 * 2 * 1.965e-3}
 FIELDS = {
     "field256": dict(phantom="ellipsoid", seed=4, n_side=16, pitch=5e-3, energy=(70.0, 220.0),
                      gate_beams=4, precision="fp32",
@@ -191,6 +200,18 @@ def stage_traffic(key, cell_steps, stage_launches):
     if "bytes_per_cell_step" in entry:
         return entry["bytes_per_cell_step"] * cell_steps / max(stage_launches, 1)
     return entry.get("bytes_per_launch")
+
+
+def compute_roofline(cell_steps, stage_ms, precision):
+    """The stage kernels are issue-bound on the CUDA cores, not HBM-bound: the
+    algorithmic FLOP rate of the stage launches against the nominal core peak
+    of the stencil's precision."""
+    achieved = cell_steps * FLOPS_PER_CELL_STEP / (stage_ms / 1e3) / 1e12 if stage_ms > 0 else 0.0
+    peak = CORE_PEAK_TFLOPS[precision]
+    return {"unit": "TFLOP/s", "achieved": achieved, "peak": peak, "frac": achieved / peak,
+            "flops_per_cell_step": FLOPS_PER_CELL_STEP,
+            "peak_source": f"nominal {'FP32' if precision == 'FP32_FP64' else 'FP64'} CUDA-core peak "
+                           "(148 SMs x lanes x 2 x 1965 MHz), not measured"}
 
 
 def measured_peaks():
@@ -455,7 +476,8 @@ def run_ours(args, cfg, desc, rank, world, local_rank):
                      "avg_launch_ms": avg_launch_ms,
                      "algorithmic_bytes_per_launch": alg_total / max(stage_launches, 1),
                      "algorithmic_bytes_per_cell_step": ALG_BYTES_PER_CELL_STEP[precision],
-                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"},
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                     "compute": compute_roofline(cell_steps, stage_ms, precision)},
         "e2e": {"value": 1.0 / e2e_s, "unit": "spots/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": launches,
@@ -631,7 +653,9 @@ def run_field(args, rank, world, local_rank):
                      "avg_launch_ms": stage_ms / max(stage_launches, 1),
                      "algorithmic_bytes_per_launch": alg_total / max(stage_launches, 1),
                      "algorithmic_bytes_per_cell_step": ALG_BYTES_PER_CELL_STEP["FP32_FP64"],
-                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"},
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                     "compute": compute_roofline(cell_steps, stage_ms,
+                                                 "FP32_FP64" if PRECISION == "fp32" else "FP64")},
         "e2e": {"value": n_spots / e2e_s, "unit": "spots/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": launches,
