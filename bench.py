@@ -607,8 +607,9 @@ def run_field(args, rank, world, local_rank):
     if world > 1:
         dist.barrier()
     t0 = time.perf_counter()
+    e2e_stats = {}
     if mine:
-        dose_h, _ = field_march(run_cfg, mm, grid, mine)
+        dose_h, _ = field_march(run_cfg, mm, grid, mine, stats=e2e_stats)
     else:
         dose_h = np.zeros(grid.shape)
     if world > 1:
@@ -657,7 +658,7 @@ def run_field(args, rank, world, local_rank):
                      "compute": compute_roofline(cell_steps, stage_ms,
                                                  "FP32_FP64" if PRECISION == "fp32" else "FP64")},
         "e2e": {"value": n_spots / e2e_s, "unit": "spots/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h)},
+                "d2h_bytes_per_step": int(d2h), "rank0_breakdown": e2e_stats},
         "gpu_launches": launches,
         "clocks": clocks.summary(),
     }

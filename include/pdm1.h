@@ -301,6 +301,14 @@ int pdm1_box_model_infer(const pdm1_box_model *model, const float *features, int
 int pdm1_analytical_csda_dose(const pdm1_problem *problem, int energy_points, int range_points, double *dose,
                               pdm1_stream_t stream);
 
+/* The plans' caching allocator (no reference counterpart: the reference
+ * allocates NumPy/CuPy arrays per call).  A destroyed plan's device buffers
+ * and pinned blocks stay cached for the next plan of the same sizes;
+ * pdm1_pool_cached_bytes: bytes cached for the current device;
+ * pdm1_pool_release: synchronise the device and free them. */
+size_t pdm1_pool_cached_bytes(void);
+int pdm1_pool_release(void);
+
 const char *pdm1_last_error(void);
 const char *pdm1_version(void);
 

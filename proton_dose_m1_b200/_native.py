@@ -87,6 +87,10 @@ def lib():
         L.pdm1_plan_destroy.argtypes = [_vp]
         L.pdm1_plan_workspace_bytes.argtypes = [_vp]
         L.pdm1_plan_workspace_bytes.restype = C.c_size_t
+        L.pdm1_pool_cached_bytes.argtypes = []
+        L.pdm1_pool_cached_bytes.restype = C.c_size_t
+        L.pdm1_pool_release.argtypes = []
+        L.pdm1_pool_release.restype = C.c_int
         L.pdm1_march.argtypes = [_vp, _vp, _vp, _vp, C.c_int, _dp, C.c_int, _vp, _dp,
                                  C.POINTER(MarchInfo), _vp]
         L.pdm1_field_plan_create.argtypes = [C.POINTER(Problem), C.POINTER(BeamDesc), C.c_int,
@@ -142,5 +146,6 @@ EXPORTED_SYMBOLS = (
     "pdm1_march_noalloc", "pdm1_plan_set_box_model", "pdm1_plan_set_recorder", "pdm1_mlp_train",
     "pdm1_mlp_gradients", "pdm1_mlp_forward", "pdm1_box_model_infer",
     "pdm1_tile_shape", "pdm1_plan_set_tile", "pdm1_plan_autotune", "pdm1_analytical_csda_dose",
+    "pdm1_pool_cached_bytes", "pdm1_pool_release",
 )
 NUM_TILES = 3

@@ -32,6 +32,8 @@ UNITS = {
     CSRC / "pdm1_box.cu": [],
     # analytical CSDA + straight-streaming reference dose
     CSRC / "pdm1_analytical.cu": [],
+    # the plans' caching allocator
+    CSRC / "pdm1_pool.cu": [],
 }
 SOURCES = list(UNITS)
 

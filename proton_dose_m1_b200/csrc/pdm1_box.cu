@@ -506,7 +506,7 @@ __global__ void __launch_bounds__(256) record_kernel(const ConfigDev *cfp, const
     const Coeffs *co = cos;
     MarchState *st = sts;
     const BeamDev &bm = cf.beams[0];
-    __shared__ double red[256];
+    __shared__ double red[512];   // significant_box_cta: two reductions
     __shared__ double s_scale, s_scale2;
     __shared__ int s_lo[3], s_hi[3], s_lo2[2][3], s_hi2[2][3];
     const int t = threadIdx.x;

@@ -442,55 +442,63 @@ __device__ __forceinline__ unsigned long long *beam_slab(const ConfigDev &cf, in
 // scale = max(max phi, max phi_in) (phi_in only while the domain touches
 // z = 0), then the first and last x / y / z slab of `d` whose max phi exceeds
 // tol * scale (the plan's tolerance for the moving box), an inflow cell above
-// it joining the k = 0 layer.  Called by all
-// threads of a CTA of 256; results (local indices, hi < 0 when none) in the
-// caller's shared memory.
+// it joining the k = 0 layer.  Called by all threads of a CTA of 256 (8
+// warps) with `red` = 512 doubles of shared memory; results (local indices,
+// hi < 0 when none) in the caller's shared memory.
 __device__ inline void significant_box_cta(const ConfigDev &cf, const BeamDev &bm, const DomainDev &d,
                                            const unsigned long long *slab, double ed, double *red, int *s_lo,
                                            int *s_hi, double *s_scale, double tol) {
-    const int t = threadIdx.x;
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const unsigned long long *sx = slab, *sy = slab + cf.nx, *sz = slab + cf.nx + cf.ny;
     auto as_d = [](unsigned long long b) { return __longlong_as_double((long long)b); };
-    double m = 0.0;
+    auto inflow = [&](int i, int j) { return bm.spatial[(size_t)(d.i0 + i) * cf.ny + (d.j0 + j)] * ed; };
+    // the state's maximum (slab maxima) and the inflow's over the box's entrance
+    double m = 0.0, mi = 0.0;
     for (int i = t; i < d.nx; i += 256) m = fmax(m, as_d(sx[i]));
     if (d.inflow)
-        for (int e = t; e < d.nx * d.ny; e += 256) {
-            int i = e / d.ny, j = e % d.ny;
-            m = fmax(m, bm.spatial[(size_t)(d.i0 + i) * cf.ny + (d.j0 + j)] * ed);
-        }
+        for (int e = t; e < d.nx * d.ny; e += 256) mi = fmax(mi, inflow(e / d.ny, e % d.ny));
     red[t] = m;
+    red[256 + t] = mi;
     __syncthreads();
     for (int w = 128; w > 0; w >>= 1) {
-        if (t < w) red[t] = fmax(red[t], red[t + w]);
+        if (t < w) {
+            red[t] = fmax(red[t], red[t + w]);
+            red[256 + t] = fmax(red[256 + t], red[256 + t + w]);
+        }
         __syncthreads();
     }
     if (t == 0) {
-        *s_scale = red[0];
+        *s_scale = fmax(red[0], red[256]);
         for (int q = 0; q < 3; ++q) { s_lo[q] = 0x7fffffff; s_hi[q] = -1; }
     }
     __syncthreads();
     const double scale = *s_scale;
     const double thr = tol * scale;
+    // an inflow cell above the threshold exists iff the inflow's maximum is above it
+    const bool inflow_on = d.inflow && red[256] > thr;
     if (scale != 0.0) {
-        for (int i = t; i < d.nx; i += 256) {
+        // one warp per x slab (y slab): the slab maximum, or any inflow cell of
+        // the slab's entrance row above the threshold
+        for (int i = warp; i < d.nx; i += 8) {
             bool act = as_d(sx[i]) > thr;
-            if (!act && d.inflow)
-                for (int j = 0; j < d.ny && !act; ++j)
-                    act = bm.spatial[(size_t)(d.i0 + i) * cf.ny + (d.j0 + j)] * ed > thr;
-            if (act) { atomicMin(&s_lo[0], i); atomicMax(&s_hi[0], i); }
+            if (!act && inflow_on) {
+                bool any = false;
+                for (int j = lane; j < d.ny; j += 32) any = any || inflow(i, j) > thr;
+                act = __any_sync(0xffffffffu, any);
+            }
+            if (act && lane == 0) { atomicMin(&s_lo[0], i); atomicMax(&s_hi[0], i); }
         }
-        for (int j = t; j < d.ny; j += 256) {
+        for (int j = warp; j < d.ny; j += 8) {
             bool act = as_d(sy[j]) > thr;
-            if (!act && d.inflow)
-                for (int i = 0; i < d.nx && !act; ++i)
-                    act = bm.spatial[(size_t)(d.i0 + i) * cf.ny + (d.j0 + j)] * ed > thr;
-            if (act) { atomicMin(&s_lo[1], j); atomicMax(&s_hi[1], j); }
+            if (!act && inflow_on) {
+                bool any = false;
+                for (int i = lane; i < d.nx; i += 32) any = any || inflow(i, j) > thr;
+                act = __any_sync(0xffffffffu, any);
+            }
+            if (act && lane == 0) { atomicMin(&s_lo[1], j); atomicMax(&s_hi[1], j); }
         }
         for (int k = t; k < d.nz; k += 256) {
-            bool act = as_d(sz[k]) > thr;
-            if (!act && k == 0 && d.inflow)
-                for (int e = 0; e < d.nx * d.ny && !act; ++e)
-                    act = bm.spatial[(size_t)(d.i0 + e / d.ny) * cf.ny + (d.j0 + e % d.ny)] * ed > thr;
+            const bool act = as_d(sz[k]) > thr || (k == 0 && inflow_on);
             if (act) { atomicMin(&s_lo[2], k); atomicMax(&s_hi[2], k); }
         }
     }
@@ -533,6 +541,13 @@ void launch_record(const ConfigDev *d_cf, const Coeffs *d_co, MarchState *d_st, 
 
 // Record an error message for pdm1_last_error() and return `code`.
 int report_error(int code, const char *msg);
+
+// The plans' caching allocator (pdm1_pool.cu): device blocks of the current
+// device and pinned host blocks, reused by size; pool_free of a pointer the
+// pool did not hand out is ignored.
+cudaError_t pool_malloc(void **ptr, size_t bytes);
+cudaError_t pool_malloc_host(void **ptr, size_t bytes);
+void pool_free(void *ptr);
 
 // Single-precision stencil kernels (pdm1_stage_fp32.cu, compiled with fast math).
 int stage_fp32_set_attributes();

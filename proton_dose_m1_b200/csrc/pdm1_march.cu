@@ -474,7 +474,7 @@ __global__ void __launch_bounds__(256) box_kernel(const ConfigDev *cfp, Coeffs *
     Coeffs *co = cos + b;
     MarchState *st = sts + b;
     unsigned long long *slab = beam_slab(cf, b);
-    __shared__ double red[256];
+    __shared__ double red[512];   // significant_box_cta: two reductions
     __shared__ double s_ed, s_scale;
     __shared__ int s_lo[3], s_hi[3];
     __shared__ int s_done;
@@ -988,29 +988,31 @@ int initial_box(const pdm1_problem &p, const double *spatial, TileDims tile, Dom
 
 void destroy_plan(pdm1_plan *pl) {
     if (!pl) return;
-    cudaFree(pl->d_cf);
-    cudaFree(pl->d_co);
-    cudaFree(pl->d_st);
-    cudaFreeHost(pl->h_st);
-    cudaFree(pl->d_sum);
-    cudaFreeHost(pl->h_sum);
-    cudaFree(pl->d_beams);
-    cudaFree(pl->d_tile_off);
-    cudaFree(pl->d_tables);
-    cudaFree(pl->d_ids);
-    cudaFree(pl->d_spatial);
-    cudaFree(pl->d_targets);
-    cudaFree(pl->d_U1);
-    cudaFree(pl->d_U2);
-    cudaFree(pl->d_V);
-    cudaFree(pl->d_q);
-    cudaFree(pl->d_bufA);
-    cudaFree(pl->d_bufB);
-    cudaFree(pl->d_slab);
-    cudaFree(pl->d_active);
-    cudaFree(pl->d_model);
-    cudaFree(pl->d_acc);
-    cudaFree(pl->d_plane);
+    // the buffers go back to the pool; wait for the device as cudaFree would
+    cudaDeviceSynchronize();
+    pool_free(pl->d_cf);
+    pool_free(pl->d_co);
+    pool_free(pl->d_st);
+    pool_free(pl->h_st);
+    pool_free(pl->d_sum);
+    pool_free(pl->h_sum);
+    pool_free(pl->d_beams);
+    pool_free(pl->d_tile_off);
+    pool_free(pl->d_tables);
+    pool_free(pl->d_ids);
+    pool_free(pl->d_spatial);
+    pool_free(pl->d_targets);
+    pool_free(pl->d_U1);
+    pool_free(pl->d_U2);
+    pool_free(pl->d_V);
+    pool_free(pl->d_q);
+    pool_free(pl->d_bufA);
+    pool_free(pl->d_bufB);
+    pool_free(pl->d_slab);
+    pool_free(pl->d_active);
+    pool_free(pl->d_model);
+    pool_free(pl->d_acc);
+    pool_free(pl->d_plane);
     if (pl->ready) cudaEventDestroy(pl->ready);
     for (cudaEvent_t e : pl->ev)
         if (e) cudaEventDestroy(e);
@@ -1088,7 +1090,7 @@ int create_plan(const pdm1_problem *problem, const pdm1_beam *beams, int nbeams,
     for (size_t c = 0; c < N; ++c) cf.present |= 1u << problem->ids[c];
     cudaError_t e;
 #define ALLOC(ptr, bytes)                                                      \
-    e = cudaMalloc((void **)&(ptr), (bytes));                                  \
+    e = pool_malloc((void **)&(ptr), (bytes));                                 \
     if (e != cudaSuccess) {                                                    \
         set_error(PDM1_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e)); \
         return fail(PDM1_ERR_CUDA);                                            \
@@ -1117,8 +1119,8 @@ int create_plan(const pdm1_problem *problem, const pdm1_beam *beams, int nbeams,
     }
 #undef ALLOC
     pl->workspace = B * cap * ((p.moving_active_domain ? 21 : 13) * sizeof(double) + (p.moving_active_domain ? 1 : 0));
-    if (cudaMallocHost((void **)&pl->h_st, B * sizeof(MarchState)) != cudaSuccess ||
-        cudaMallocHost((void **)&pl->h_sum, sizeof(MarchSummary)) != cudaSuccess ||
+    if (pool_malloc_host((void **)&pl->h_st, B * sizeof(MarchState)) != cudaSuccess ||
+        pool_malloc_host((void **)&pl->h_sum, sizeof(MarchSummary)) != cudaSuccess ||
         cudaStreamCreateWithFlags(&pl->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&pl->ready, cudaEventDisableTiming) != cudaSuccess)
         return fail(set_error(PDM1_ERR_CUDA, "cudaMallocHost/stream/event creation failed"));
@@ -1449,7 +1451,7 @@ int pdm1_plan_set_box_model(pdm1_plan *pl, const pdm1_box_model *model) {
     BoxModelDev h;
     int rc = pack_box_model(model, h);
     if (rc) return rc;
-    if (!pl->d_model) CUDA_TRY(cudaMalloc((void **)&pl->d_model, sizeof(BoxModelDev)));
+    if (!pl->d_model) CUDA_TRY(pool_malloc((void **)&pl->d_model, sizeof(BoxModelDev)));
     CUDA_TRY(cudaMemcpy(pl->d_model, &h, sizeof h, cudaMemcpyHostToDevice));
     pl->cf.learned = 1;
     pl->cf.model = pl->d_model;

@@ -125,6 +125,40 @@ PDM1_HD T weno_left(T v0, T v1, T v2, T v3, T v4) {
     return w0 * p0 + w1 * p1 + w2 * p2;
 }
 
+// Single-precision WENO-Z5 with the arithmetic regrouped for fewer
+// instructions: the candidate polynomials as integer combinations times 1/6,
+// the 1/6 folded into the one division by the weight sum.  Same weights and
+// overflow guard as weno_left<float>.
+PDM1_HD float weno_left_f32(float v0, float v1, float v2, float v3, float v4) {
+    const float q0 = 2.0f * v0 - 7.0f * v1 + 11.0f * v2;   // 6 p0
+    const float q1 = -v1 + 5.0f * v2 + 2.0f * v3;          // 6 p1
+    const float q2 = 2.0f * v2 + 5.0f * v3 - v4;           // 6 p2
+    float a = v0 - 2.0f * v1 + v2, b = v0 - 4.0f * v1 + 3.0f * v2;
+    const float beta0 = float(13.0 / 12.0) * (a * a) + 0.25f * (b * b);
+    a = v1 - 2.0f * v2 + v3; b = v1 - v3;
+    const float beta1 = float(13.0 / 12.0) * (a * a) + 0.25f * (b * b);
+    a = v2 - 2.0f * v3 + v4; b = 3.0f * v2 - 4.0f * v3 + v4;
+    const float beta2 = float(13.0 / 12.0) * (a * a) + 0.25f * (b * b);
+    const float tau5 = fabsf(beta2 - beta0);
+    const float r0 = tau5 / (beta0 + float(kWenoEps));
+    const float r1 = tau5 / (beta1 + float(kWenoEps));
+    const float r2 = tau5 / (beta2 + float(kWenoEps));
+    float al0, al1, al2;
+    const float rmax = fmaxf(r0, fmaxf(r1, r2));
+    if (rmax > 1e15f) {   // r^2 would overflow: divide every alpha by rmax^2
+        const float inv = 1.0f / rmax, e = inv * inv;
+        const float t0 = r0 * inv, t1 = r1 * inv, t2 = r2 * inv;
+        al0 = 0.1f * (e + t0 * t0);
+        al1 = 0.6f * (e + t1 * t1);
+        al2 = 0.3f * (e + t2 * t2);
+    } else {
+        al0 = 0.1f * (1.0f + r0 * r0);
+        al1 = 0.6f * (1.0f + r1 * r1);
+        al2 = 0.3f * (1.0f + r2 * r2);
+    }
+    return (al0 * q0 + al1 * q1 + al2 * q2) / (6.0f * (al0 + al1 + al2));
+}
+
 // ---------------------------------------------------------------------------
 // WENO3-Z left reconstruction (p = 2), reconstruction_methods/weno3.py:15-62
 // ---------------------------------------------------------------------------
@@ -295,6 +329,116 @@ PDM1_HD void hll_flux(const T L[4], const T R[4], int axis, bool unit_speeds, T 
     }
 #pragma unroll
     for (int c = 0; c < 4; ++c) F[c] = (sr * FL[c] - sl * FR[c] + sp * (R[c] - L[c])) / den;
+}
+
+// ---------------------------------------------------------------------------
+// Single-precision interface flux: the two realizability projections, the two
+// closures, the exact wave speeds and the HLL combination of one face, with
+// each shared quantity formed once.  The algebra is that of project, closure,
+// eigen and hll_flux above; with q = (1 - f)(1 + f) and r = sqrt(1 + 3q)
+// (= sqrt(4 - 3f^2)):
+//   1 - chi = 2q / (r + 1) = 2 iso,   3 chi - 1 = 2 dir = 2 (2 - r),
+//   5 - 3 chi = 2 + 6 iso,
+// so the wave speeds reuse the closure's iso and dir, and |J| after the
+// projection is the closure's |J|.  No factor carries the cancellation of
+// 1 - chi as f -> 1.  One reciprocal serves each common denominator.
+// ---------------------------------------------------------------------------
+struct SideF32 { float phi, jx, jy, jz, jn, f, nx, ny, nz, iso, dir; };
+
+PDM1_HD void closure_f32(float phi, float jn, float &f, float &iso, float &dir) {
+    f = phi > 0.0f ? fminf(jn / phi, 1.0f) : 0.0f;
+    const float q = (1.0f - f) * (1.0f + f);
+    const float r = sqrtf(1.0f + 3.0f * q);
+    iso = q / (r + 1.0f);
+    dir = 2.0f - r;
+}
+
+PDM1_HD SideF32 side_f32(const float u[4]) {
+    SideF32 s;
+    s.phi = u[0] < 0.0f ? 0.0f : u[0];
+    s.jx = u[1]; s.jy = u[2]; s.jz = u[3];
+    s.jn = sqrtf(s.jx * s.jx + s.jy * s.jy + s.jz * s.jz);
+    const float jmax = float(1.0 - kRealEps) * s.phi;
+    if (s.jn > jmax) {   // realizability projection onto |J| = jmax
+        const float sc = jmax / s.jn;
+        s.jx *= sc; s.jy *= sc; s.jz *= sc;
+        s.jn = jmax;
+    }
+    closure_f32(s.phi, s.jn, s.f, s.iso, s.dir);
+    if (s.jn > 0.0f) {
+        const float inv = 1.0f / s.jn;
+        s.nx = s.jx * inv; s.ny = s.jy * inv; s.nz = s.jz * inv;
+    } else {
+        s.nx = s.ny = s.nz = 0.0f;
+    }
+    return s;
+}
+
+PDM1_HD void speeds_f32(const SideF32 &s, int axis, float &lmin, float &lmax) {
+    if (s.jn < float(kEigEps)) {
+        lmin = -0.57735026918962576f;   // -1/sqrt(3)
+        lmax = 0.57735026918962576f;
+        return;
+    }
+    float f = s.f, iso = s.iso, dir = s.dir;
+    if (s.phi < float(kEigEps)) closure_f32(float(kEigEps), s.jn, f, iso, dir);   // phi floored
+    f = fminf(f, float(1.0 - kEigEps));
+    const float mu = axis == 0 ? s.nx : (axis == 1 ? s.ny : s.nz);
+    const float den = 2.0f + 6.0f * iso;
+    float disc = 4.0f * f * f * mu * mu - den * (2.0f * dir * mu * mu - 4.0f * iso);
+    disc = fmaxf(disc, 0.0f);
+    const float root = sqrtf(disc), inv = 1.0f / den, c = 2.0f * f * mu;
+    lmin = (c - root) * inv;
+    lmax = (c + root) * inv;
+}
+
+PDM1_HD void side_flux_f32(const SideF32 &s, int axis, float F[4]) {
+    const float pd = s.phi * s.dir;
+    if (axis == 0) {
+        F[0] = s.jx;
+        F[1] = s.phi * s.iso + pd * s.nx * s.nx;
+        F[2] = pd * s.nx * s.ny;
+        F[3] = pd * s.nx * s.nz;
+    } else if (axis == 1) {
+        F[0] = s.jy;
+        F[1] = pd * s.nx * s.ny;
+        F[2] = s.phi * s.iso + pd * s.ny * s.ny;
+        F[3] = pd * s.ny * s.nz;
+    } else {
+        F[0] = s.jz;
+        F[1] = pd * s.nx * s.nz;
+        F[2] = pd * s.ny * s.nz;
+        F[3] = s.phi * s.iso + pd * s.nz * s.nz;
+    }
+}
+
+// L and R: the reconstructed (unprojected) face states; F: the HLL flux.
+PDM1_HD void face_flux_f32(const float L[4], const float R[4], int axis, bool unit_speeds,
+                                              float F[4]) {
+    const SideF32 a = side_f32(L), b = side_f32(R);
+    float FL[4], FR[4];
+    side_flux_f32(a, axis, FL);
+    side_flux_f32(b, axis, FR);
+    float sl = -1.0f, sr = 1.0f;
+    if (!unit_speeds) {
+        float lminl, lmaxl, lminr, lmaxr;
+        speeds_f32(a, axis, lminl, lmaxl);
+        speeds_f32(b, axis, lminr, lmaxr);
+        sl = fminf(fminf(lminl, lminr), 0.0f);
+        sr = fmaxf(fmaxf(lmaxl, lmaxr), 0.0f);
+    }
+    const float den = sr - sl;
+    if (!(den > 0.0f)) {
+        // |J|/phi rounds to 1 for an exactly directed state: both speeds normal
+        // to J are 0 and the fan collapses; the HLL flux tends to the central flux
+#pragma unroll
+        for (int c = 0; c < 4; ++c) F[c] = 0.5f * (FL[c] + FR[c]);
+        return;
+    }
+    const float inv = 1.0f / den, sp = sl * sr;
+    const float dl[4] = {b.phi - a.phi, b.jx - a.jx, b.jy - a.jy, b.jz - a.jz};
+#pragma unroll
+    for (int c = 0; c < 4; ++c) F[c] = (sr * FL[c] - sl * FR[c] + sp * dl[c]) * inv;
 }
 
 // ---------------------------------------------------------------------------

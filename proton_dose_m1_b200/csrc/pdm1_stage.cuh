@@ -137,8 +137,13 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 3) stage
                     T w[6];
 #pragma unroll
                     for (int q = 0; q < 6; ++q) w[q] = base[c * cs + q * stride];
-                    L[c] = weno_left(w[0], w[1], w[2], w[3], w[4]);
-                    R[c] = weno_left(w[5], w[4], w[3], w[2], w[1]);
+                    if constexpr (sizeof(T) == sizeof(float)) {
+                        L[c] = weno_left_f32(w[0], w[1], w[2], w[3], w[4]);
+                        R[c] = weno_left_f32(w[5], w[4], w[3], w[2], w[1]);
+                    } else {
+                        L[c] = weno_left(w[0], w[1], w[2], w[3], w[4]);
+                        R[c] = weno_left(w[5], w[4], w[3], w[2], w[1]);
+                    }
                 }
             } else {
                 // the narrower stencils read cells i-2 .. i+1 (arm indices i+1 .. i+4)
@@ -160,10 +165,14 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 3) stage
                     }
                 }
             }
-            project(L[0], L[1], L[2], L[3]);
-            project(R[0], R[1], R[2], R[3]);
             T F[4];
-            hll_flux(L, R, axis, unit, F);
+            if constexpr (sizeof(T) == sizeof(float)) {
+                face_flux_f32(L, R, axis, unit, F);
+            } else {
+                project(L[0], L[1], L[2], L[3]);
+                project(R[0], R[1], R[2], R[3]);
+                hll_flux(L, R, axis, unit, F);
+            }
 #pragma unroll
             for (int c = 0; c < 4; ++c) s.F[c * NF + f] = F[c];
         }

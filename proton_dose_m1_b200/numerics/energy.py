@@ -12,6 +12,8 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import os
+import threading
 from typing import Any
 
 import numpy as np
@@ -122,7 +124,10 @@ def _apply_tile(config, handle, shape, n_beams) -> None:
     if tile != "auto":
         _native.check(_native.lib().pdm1_plan_set_tile(handle, TILE_SHAPES.index(tuple(tile))))
         return
-    key = (config.accel.precision.name, tuple(shape), n_beams, bool(config.numerics.moving_active_domain))
+    # one choice per precision, grid and kind of plan (one beam, or a field of
+    # any size: the waves of one field differ only in their beam counts)
+    key = (config.accel.precision.name, tuple(shape), 1 if n_beams == 1 else "field",
+           bool(config.numerics.moving_active_domain))
     if key not in _TILE_CACHE:
         torch = _torch()
         best = C.c_int()
@@ -134,7 +139,7 @@ def _apply_tile(config, handle, shape, n_beams) -> None:
 
 
 def autotuned_tiles():
-    """The autotuner's choices so far: {(precision, grid, beams, moving): (tile id, ns per cell-step)}."""
+    """The autotuner's choices so far: {(precision, grid, 1 | "field", moving): (tile id, ns per cell-step)}."""
     return dict(_TILE_CACHE)
 
 
@@ -368,9 +373,10 @@ class FieldPlan:
         self._plans = {}
         self._layout(int(box_capacity_cells or max(estimate_box_cells(config, grid, b) for b in beams)))
 
-    def _layout(self, cap):
-        """Set the box capacity, split the beams into waves, create the plan of
-        a single wave."""
+    def _layout(self, cap, members=None):
+        """Set the box capacity and split the beams ``members`` (default: all)
+        into waves; returns the waves.  With every beam in a single wave its
+        plan is created once and kept."""
         self.close()
         N = int(np.prod(self.shape))
         nxy = self.shape[0] * self.shape[1]
@@ -379,11 +385,18 @@ class FieldPlan:
         budget = self._budget
         if not budget:
             torch = _torch()
+            torch.cuda.empty_cache()   # blocks the caching allocator holds are free for the plans
             free, _ = torch.cuda.mem_get_info()
-            budget = int(0.7 * free)
-        self.waves = field_waves([b.energy for b in self.beams], per_beam, budget)
-        if len(self.waves) == 1:
-            self._plans[0] = self._create(self.waves[0])
+            # blocks of destroyed plans that the plans' own pool keeps are free for these
+            budget = int(0.7 * (free + int(_native.lib().pdm1_pool_cached_bytes())))
+        idx = list(range(self.n_beams)) if members is None else list(members)
+        order = field_waves([self.beams[i].energy for i in idx], per_beam, budget)
+        waves = [[idx[k] for k in wave] for wave in order]
+        if members is None:
+            self.waves = waves
+            if len(waves) == 1:
+                self._plans[0] = self._create(waves[0])
+        return waves
 
     def _create(self, members):
         """A native field plan for the beams ``members`` (indices into ``beams``)."""
@@ -419,40 +432,48 @@ class FieldPlan:
         """Field dose into the device tensor ``dose``; returns steps per beam.
 
         ``last_info`` sums the march statistics over the waves.  With an
-        estimated capacity, a box that outgrows it doubles the capacity and
-        the field is marched again."""
-        N = int(np.prod(self.shape))
-        while True:
-            try:
-                return self._march_waves(dose, max_steps)
-            except ValueError as e:
-                if not (self.auto_capacity and "capacity" in str(e) and self.cap < N):
-                    raise
-                self.capacity_retries += 1
-                self._layout(2 * self.cap)
-
-    def _march_waves(self, dose, max_steps):
+        estimated capacity, a box that outgrows it doubles the capacity: the
+        beams of that wave and of the waves after it are split into new waves
+        and marched at the new capacity; the waves already marched stand."""
         torch = _torch()
+        N = int(np.prod(self.shape))
         steps_all = [0] * self.n_beams
         total = _native.MarchInfo()
-        partial = torch.empty_like(dose) if len(self.waves) > 1 else None
+        partial = None
         stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
-        for w, members in enumerate(self.waves):
-            h = self._plans.get(w)
+        waves = list(self.waves)
+        regrown = False
+        w = 0
+        while w < len(waves):
+            members = waves[w]
+            if w > 0 and partial is None:
+                partial = torch.empty_like(dose)
+            out = dose if w == 0 else partial
+            h = self._plans.get(w) if not regrown else None
             transient = h is None
-            if transient:
-                h = self._create(members)
             try:
+                if transient:   # a beam's initial box beyond the capacity fails here
+                    h = self._create(members)
                 # tile shape (autotuned on the first march; a box that outgrows
                 # the capacity there is retried like one in the march)
                 _apply_tile(self.config, h, self.shape, len(members))
                 steps = (C.c_int * len(members))()
                 info = _native.MarchInfo()
-                out = dose if w == 0 else partial
                 _native.check(_native.lib().pdm1_field_march(
                     h, C.c_void_p(out.data_ptr()), int(max_steps), steps, C.byref(info), stream))
+            except ValueError as e:
+                if not (self.auto_capacity and "capacity" in str(e) and self.cap < N):
+                    raise
+                if transient and h:
+                    _native.lib().pdm1_plan_destroy(h)
+                transient = False
+                self.capacity_retries += 1
+                rest = [i for wave in waves[w:] for i in wave]
+                waves = waves[:w] + self._layout(2 * self.cap, rest)
+                regrown = True
+                continue
             finally:
-                if transient:
+                if transient and h:
                     _native.lib().pdm1_plan_destroy(h)
             if w > 0:
                 dose.add_(partial)
@@ -465,6 +486,9 @@ class FieldPlan:
             total.stage_ms += info.stage_ms
             total.cell_steps += info.cell_steps
             total.max_box_cells = max(total.max_box_cells, info.max_box_cells)
+            w += 1
+        if regrown:   # the next march lays every beam out at the grown capacity
+            self._layout(self.cap)
         self.last_info = total
         return steps_all
 
@@ -475,26 +499,71 @@ class FieldPlan:
         return dose, steps
 
 
+_STAGING: dict = {}          # device index -> page-locked uint8 tensor
+_STAGING_LOCK = threading.Lock()
+_COPY_THREADS = max(1, min(8, os.cpu_count() or 1))
+_COPY_POOL = None
+
+
 def _to_host(t):
-    """Device tensor -> NumPy through page-locked memory (the caching host
-    allocator reuses the buffer across calls); the array keeps it alive."""
+    """Device tensor -> a new NumPy array.
+
+    One device->host copy into a page-locked staging buffer that is kept
+    across calls (page-locking fresh memory costs about 1 ms per MB, more
+    than the copy), then a host copy into the returned array in parallel
+    slices.  Small tensors take the plain path."""
+    global _COPY_POOL
     torch = _torch()
-    out = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
-    out.copy_(t)
-    return out.numpy()
+    nbytes = t.numel() * t.element_size()
+    if nbytes < (4 << 20):
+        return t.cpu().numpy()
+    src = t.contiguous().reshape(-1).view(torch.uint8)
+    out = np.empty(tuple(t.shape), dtype=torch.empty(0, dtype=t.dtype).numpy().dtype)
+    dst = out.reshape(-1).view(np.uint8)
+    with _STAGING_LOCK:
+        dev = t.device.index or 0
+        buf = _STAGING.get(dev)
+        if buf is None or buf.numel() < nbytes:
+            buf = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+            _STAGING[dev] = buf
+        stage = buf[:nbytes]
+        stage.copy_(src, non_blocking=True)
+        torch.cuda.current_stream(t.device).synchronize()
+        host = stage.numpy()
+        if _COPY_POOL is None:
+            from concurrent.futures import ThreadPoolExecutor
+            _COPY_POOL = ThreadPoolExecutor(_COPY_THREADS)
+        step = -(-nbytes // _COPY_THREADS)
+        parts = [(a, min(a + step, nbytes)) for a in range(0, nbytes, step)]
+        list(_COPY_POOL.map(lambda ab: np.copyto(dst[ab[0]:ab[1]], host[ab[0]:ab[1]]), parts))
+    return out
 
 
-def field_march(config, material_map, grid, beams, box_capacity_cells: int = 0):
+def field_march(config, material_map, grid, beams, box_capacity_cells: int = 0,
+                stats: dict | None = None):
     """Dose of a spot-scanning field (host NumPy in, host NumPy out).
 
     The field counterpart of ``energy_march``: the reference marches one beam
     per ``Solver.solve`` call (proton_solver/solver.py:34-218) and a field is
-    the sum of its beams' doses.  Returns ``(dose, steps_per_beam)``.
+    the sum of its beams' doses.  Returns ``(dose, steps_per_beam)``.  A dict
+    passed as ``stats`` receives the plan's layout (waves, box capacity,
+    capacity retries) and the host seconds of planning, march and copy-back.
     """
+    import time
+    torch = _torch()
+    t0 = time.perf_counter()
     plan = FieldPlan(config, material_map, grid, beams, box_capacity_cells)
     try:
+        t1 = time.perf_counter()
         dose, steps = plan.march()
-        return _to_host(dose), steps
+        torch.cuda.current_stream().synchronize()
+        t2 = time.perf_counter()
+        out = _to_host(dose)
+        if stats is not None:
+            stats.update(waves=len(plan.waves), box_capacity_cells=plan.cap,
+                         capacity_retries=plan.capacity_retries, plan_s=t1 - t0, march_s=t2 - t1,
+                         copy_s=time.perf_counter() - t2)
+        return out, steps
     finally:
         plan.close()
 

@@ -97,7 +97,10 @@ def test_phantom_cfl_bound_follows_the_full_domain_steps():
     """A low-stopping-power block (ADIPOSE_SYNTH, 0.95 x water) outside the
     beam bounds every energy step of the full-domain march through its empty
     cells; the reference's box rule ignores it, the phantom-wide bound
-    reproduces the full-domain energies exactly."""
+    reproduces the full-domain step count.  Not the energies bit for bit: the
+    full grid's cells in the block also hold the beam's far tail (~1e-26 of
+    the peak in double), whose speeds exceed the vacuum speed at some steps
+    (by 1e-7 relative early on; the sequences then part by up to 0.012 MeV)."""
     geo = Geometry(size=(0.04, 0.04, 0.06), resolution=(40, 40, 60),
                    objects=[Box(0.017, 0.02, -0.02, 0.02, 0.0, 0.06, Material.ADIPOSE_SYNTH)])
     beam = Beam(n_protons=1e6, energy=60.0, energy_spread=1.0, sigma=(0.0015, 0.0015))
@@ -115,8 +118,45 @@ def test_phantom_cfl_bound_follows_the_full_domain_steps():
         _, dose, E, _ = plan.march(U)
         plan.close()
         out[name] = (dose.cpu().numpy(), E)
-    np.testing.assert_array_equal(out["floor"][1], out["full"][1])
-    assert len(out["box"][1]) < len(out["full"][1])
+    assert len(out["floor"][1]) == len(out["full"][1])
+    assert np.abs(out["floor"][1] - out["full"][1]).max() < 0.02   # MeV
+    # the box alone takes larger steps (its own bound) from the second step on
+    assert out["box"][1][2] < out["full"][1][2]
     full = out["full"][0]
     err = {k: np.abs(out[k][0] - full).max() / full.max() for k in ("box", "floor")}
     assert err["floor"] < err["box"], err
+
+
+def test_capacity_growth_marches_each_beam_once(monkeypatch):
+    """An estimated capacity far below the boxes: the field grows it wave by
+    wave, the waves already marched stand, and the result is the sum of the
+    single-beam marches; the next march starts at the grown capacity."""
+    from proton_dose_m1_b200.numerics import energy as en
+    cfg = phantom()
+    grid = Grid.from_geometry(cfg.geometry)
+    mm = MaterialMap.from_geometry(cfg.geometry, grid)
+    cells, doses, counts = 0.0, [], []
+    for b in BEAMS:
+        c = SolverConfig(geometry=cfg.geometry, beam=b, physics=cfg.physics, numerics=cfg.numerics,
+                         accel=cfg.accel)
+        plan = M1Plan(c, mm, grid, BeamInflow.from_beam(b, grid))
+        _, d, E, _ = plan.march(None)
+        cells += plan.last_info.cell_steps
+        doses.append(d.cpu().numpy())
+        counts.append(len(E) - 1)
+        plan.close()
+    total = sum(doses)
+    monkeypatch.setattr(en, "estimate_box_cells", lambda config, grid, beam: 3000)
+    per_beam = 3000 * en.FIELD_BYTES_PER_BOX_CELL + grid.shape[0] * grid.shape[1] * 8 + 4096
+    fp = FieldPlan(cfg, mm, grid, BEAMS, max_workspace_bytes=2 * per_beam)
+    assert len(fp.waves) == 2 and fp.cap == 3000
+    dose, steps = fp.march()
+    assert fp.capacity_retries >= 1 and fp.cap > 3000
+    assert steps == counts
+    assert fp.last_info.cell_steps == cells
+    assert np.abs(dose.cpu().numpy() - total).max() <= 1e-12 * total.max()
+    retries = fp.capacity_retries
+    dose2, steps2 = fp.march()
+    assert fp.capacity_retries == retries and steps2 == counts
+    assert np.abs(dose2.cpu().numpy() - total).max() <= 1e-12 * total.max()
+    fp.close()
