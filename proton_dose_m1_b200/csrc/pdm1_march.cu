@@ -367,9 +367,36 @@ __global__ void __launch_bounds__(NT) euler_finish_kernel(StageArgs a) {
     if (!cf.moving) block_max_atomic(inv, &a.st->inv_bits);
 }
 
+// One cell's CFL term on the beam's domain `d` (energy.py:539-660): the
+// speeds of the state u and, on the entrance layer, of the inflow state at
+// the spectrum value `ed`, over S of the cell's material.  The FP32 form takes
+// float speeds, except with the phantom-wide bound, whose purpose is the
+// plain method's step sequence.
+__device__ __forceinline__ double cell_cfl(const ConfigDev &cf, const BeamDev &bm, const DomainDev &d,
+                                           const double *S, double ed, const double u[4], int li, int lj, int lk,
+                                           const bool use[3]) {
+    double phi_in = 0.0;
+    if (lk == 0 && d.inflow) phi_in = bm.spatial[(size_t)(d.i0 + li) * cf.ny + (d.j0 + lj)] * ed;
+    const double s = S[cf.ids[global_cell(cf, d, li, lj, lk)]];
+    return cf.fp32 && !cf.cfl_floor ? cfl_term<float>(cf, bm.rf, u, s, lk == 0, phi_in, use)
+                                    : cfl_term<double>(cf, bm.rf, u, s, lk == 0, phi_in, use);
+}
+
+// The phantom-wide bound: the cells outside the box hold no fluence; on the
+// full grid they would bound the step with the vacuum speed (wave_speeds.py:
+// 36-103) in the material of least stopping power present.
+__device__ __forceinline__ double phantom_cfl_floor(const ConfigDev &cf, const double *S) {
+    double smin = INFINITY;
+    for (int m = 0; m < cf.nm; ++m)
+        if (cf.present >> m & 1u) smin = fmin(smin, S[m]);
+    const double a = cf.unit_speeds ? 1.0 : 1.0 / sqrt(3.0);
+    return a / (smin * cf.dx) + a / (smin * cf.dy) + a / (smin * cf.dz);
+}
+
 // CFL bound of the state on the current domain (energy.py:539-660), with S and
 // the spectrum at the state's energy: co->S1 / ed_next (static domain, first
-// step) or co->S_cfl / ed_cfl (moving box, every step).  With vacuum-aware
+// step) or co->S_cfl / ed_cfl (moving box, every step; without vacuum-aware
+// masks rebox_kernel computes it while it moves the box).  With vacuum-aware
 // masks (energy.py:459-537) a direction counts only within 3 cells, along that
 // axis, of an active cell.
 __global__ void __launch_bounds__(NT) cfl_kernel(const ConfigDev *cfp, const Coeffs *cos, MarchState *sts,
@@ -411,24 +438,10 @@ __global__ void __launch_bounds__(NT) cfl_kernel(const ConfigDev *cfp, const Coe
                 use[ax] = any;
             }
         }
-        double phi_in = 0.0;
-        if (lk == 0 && d.inflow) phi_in = bm.spatial[(size_t)(d.i0 + li) * cf.ny + (d.j0 + lj)] * ed;
-        double s = S[cf.ids[global_cell(cf, d, li, lj, lk)]];
-        // the FP32 form takes float speeds, except with the phantom-wide bound,
-        // whose purpose is the plain method's step sequence
-        inv = fmax(inv, cf.fp32 && !cf.cfl_floor ? cfl_term<float>(cf, bm.rf, u, s, lk == 0, phi_in, use)
-                                                 : cfl_term<double>(cf, bm.rf, u, s, lk == 0, phi_in, use));
+        inv = fmax(inv, cell_cfl(cf, bm, d, S, ed, u, li, lj, lk, use));
     }
-    if (cf.cfl_floor && use_box_coeffs && blockIdx.x == 0 && threadIdx.x == 0) {
-        // the cells outside the box hold no fluence; on the full grid they would
-        // bound the step with the vacuum speed (wave_speeds.py:36-103) in the
-        // material of least stopping power
-        double smin = INFINITY;
-        for (int m = 0; m < cf.nm; ++m)
-            if (cf.present >> m & 1u) smin = fmin(smin, S[m]);
-        const double a = cf.unit_speeds ? 1.0 : 1.0 / sqrt(3.0);
-        inv = fmax(inv, a / (smin * cf.dx) + a / (smin * cf.dy) + a / (smin * cf.dz));
-    }
+    if (cf.cfl_floor && use_box_coeffs && blockIdx.x == 0 && threadIdx.x == 0)
+        inv = fmax(inv, phantom_cfl_floor(cf, S));
     block_max_atomic(inv, &st->inv_bits);
 }
 
@@ -484,10 +497,14 @@ __global__ void __launch_bounds__(256) box_kernel(const ConfigDev *cfp, Coeffs *
     if (s_done) return;
     const DomainDev d = st->dom;
     const double E = st->E;
-    if (t == 0) s_ed = energy_density(bm, E);
+    // init_kernel and prologue_kernel leave S1 = S(E_next) and ed_next =
+    // spectrum(E_next), with E_next the energy this step starts from
+    const bool known = co->E_next == E;
+    if (t == 0) s_ed = known ? co->ed_next : energy_density(bm, E);
     if (t < cf.nm) {
         double sv = 1.0;
-        if (!stopping_power_dev(cf.mats[t], E, sv)) atomicOr(&st->error, ERR_DEV_RANGE);
+        if (known) sv = co->S1[t];
+        else if (!stopping_power_dev(cf.mats[t], E, sv)) atomicOr(&st->error, ERR_DEV_RANGE);
         co->S_cfl[t] = sv;
     }
     __syncthreads();
@@ -527,31 +544,50 @@ __global__ void __launch_bounds__(256) box_kernel(const ConfigDev *cfp, Coeffs *
 
 // Copy the overlap of the previous box into the new one (zeros elsewhere,
 // moving_active_domain.py:196-232); for the vacuum-aware CFL also the max phi
-// of the new box.
-__global__ void __launch_bounds__(NT) rebox_kernel(const ConfigDev *cfp, MarchState *sts) {
+// of the new box.  With `with_cfl` (no vacuum-aware masks) the CFL bound of
+// the new box as cfl_kernel computes it, from the values in registers.
+__global__ void __launch_bounds__(NT) rebox_kernel(const ConfigDev *cfp, const Coeffs *cos, MarchState *sts,
+                                                   int with_cfl) {
     const ConfigDev &cf = *cfp;
-    MarchState *st = sts + blockIdx.y;
+    const int b = blockIdx.y;
+    MarchState *st = sts + b;
     if (st->done || st->error) return;
     const DomainDev d = st->dom;
     const bool moved = st->reboxed != 0;
-    if (!moved && !cf.vacuum_aware) return;
+    if (!moved && !cf.vacuum_aware && !with_cfl) return;
     const DomainDev p = st->prev;
     const double *Up = st->Uprev;
     double *Ua = st->Ua;
+    const BeamDev &bm = cf.beams[b];
+    const double *S = cos[b].S_cfl;
+    const double ed = cos[b].ed_cfl;
+    const bool all_axes[3] = {true, true, true};
     const size_t N = (size_t)d.nx * d.ny * d.nz, NP = (size_t)p.nx * p.ny * p.nz;
-    double m = 0.0;
+    double m = 0.0, inv = 0.0;
     for (size_t o = (size_t)blockIdx.x * NT + threadIdx.x; o < N; o += (size_t)gridDim.x * NT) {
+        const int lk = (int)(o % d.nz), lj = (int)((o / d.nz) % d.ny), li = (int)(o / ((size_t)d.nz * d.ny));
+        double u[4];
         if (moved) {
-            int lk = (int)(o % d.nz), lj = (int)((o / d.nz) % d.ny), li = (int)(o / ((size_t)d.nz * d.ny));
             int pi = d.i0 + li - p.i0, pj = d.j0 + lj - p.j0, pk = d.k0 + lk - p.k0;
             bool in = pi >= 0 && pi < p.nx && pj >= 0 && pj < p.ny && pk >= 0 && pk < p.nz;
             size_t po = in ? ((size_t)pi * p.ny + pj) * p.nz + pk : 0;
 #pragma unroll
-            for (int c = 0; c < 4; ++c) Ua[c * N + o] = in ? Up[c * NP + po] : 0.0;
+            for (int c = 0; c < 4; ++c) {
+                u[c] = in ? Up[c * NP + po] : 0.0;
+                Ua[c * N + o] = u[c];
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) u[c] = Ua[c * N + o];
         }
-        m = fmax(m, Ua[o]);
+        m = fmax(m, u[0]);
+        if (with_cfl) inv = fmax(inv, cell_cfl(cf, bm, d, S, ed, u, li, lj, lk, all_axes));
     }
     if (cf.vacuum_aware) block_max_atomic(m, &st->newmax_bits);
+    if (with_cfl) {
+        if (cf.cfl_floor && blockIdx.x == 0 && threadIdx.x == 0) inv = fmax(inv, phantom_cfl_floor(cf, S));
+        block_max_atomic(inv, &st->inv_bits);
+    }
 }
 
 // Activity mask of the vacuum-aware CFL: phi above tol * max(phi, phi_in),
@@ -885,12 +921,15 @@ int launch_box_step(pdm1_plan *pl, cudaStream_t stream) {
         launch_box_learn(pl->d_cf, pl->d_co, pl->d_st, pl->nbeams, stream);
         n += 2;
     }
-    rebox_kernel<<<cells, NT, 0, stream>>>(pl->d_cf, pl->d_st);
     if (p.vacuum_aware_cfl) {
+        rebox_kernel<<<cells, NT, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, 0);
         mask_kernel<<<cells, NT, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st);
+        cfl_kernel<<<cells, NT, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, 1);
         ++n;
+    } else {   // the CFL bound of the new box within the box move
+        rebox_kernel<<<cells, NT, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, 1);
+        --n;
     }
-    cfl_kernel<<<cells, NT, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, 1);
     return n;
 }
 
