@@ -1202,8 +1202,10 @@ int create_plan(const pdm1_problem *problem, const pdm1_beam *beams, int nbeams,
     {
         int dev = 0, sms = 148;
         if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        // resident CTAs per SM of the stage kernel: 2 in double, 3 in float
-        int per_sm = p.precision == PDM1_FP32_FP64 ? 3 : 2;
+        // resident CTAs per SM of the stage kernel: 2 in double, 4 in float
+        // (64 registers; 4 x 256 threads hide more of the MUFU and shared-memory
+        // latency than 3 x 256 at 80 registers: -4 % stage time on field256)
+        int per_sm = p.precision == PDM1_FP32_FP64 ? 4 : 2;
         size_t tiles = (size_t)make_domain(0, 0, 0, p.nx, p.ny, p.nz, 1, cf.tile).ntiles * B;
         cf.grid_ctas = (int)std::max<size_t>(1, std::min<size_t>(tiles, (size_t)per_sm * sms));
     }

@@ -120,14 +120,25 @@ PDM1_HD T weno_left(T v0, T v1, T v2, T v3, T v4) {
         al2 = T(0.3) * (T(1) + r2 * r2);
     }
     T s = al0 + al1 + al2;
-    if (sizeof(T) < sizeof(double)) return (al0 * p0 + al1 * p1 + al2 * p2) / s;   // one division
     T w0 = al0 / s, w1 = al1 / s, w2 = al2 / s;
     return w0 * p0 + w1 * p1 + w2 * p2;
 }
 
+// Single-precision quotient on the MUFU reciprocal: a * (1/b), two
+// instructions, within 2 ulp for |b| below 2^126 (every denominator of the
+// float face path: smoothness indicators up to phi^2, weight sums below
+// 1e31, |J|, phi, wave-speed denominators of order 1).
+PDM1_HD float fast_div(float a, float b) {
+#ifdef __CUDA_ARCH__
+    return __fdividef(a, b);
+#else
+    return a / b;
+#endif
+}
+
 // Single-precision WENO-Z5 with the arithmetic regrouped for fewer
 // instructions: the candidate polynomials as integer combinations times 1/6,
-// the 1/6 folded into the one division by the weight sum.  Same weights and
+// the 1/6 folded into the one reciprocal of the weight sum.  Same weights and
 // overflow guard as weno_left<float>.
 PDM1_HD float weno_left_f32(float v0, float v1, float v2, float v3, float v4) {
     const float q0 = 2.0f * v0 - 7.0f * v1 + 11.0f * v2;   // 6 p0
@@ -140,13 +151,15 @@ PDM1_HD float weno_left_f32(float v0, float v1, float v2, float v3, float v4) {
     a = v2 - 2.0f * v3 + v4; b = 3.0f * v2 - 4.0f * v3 + v4;
     const float beta2 = float(13.0 / 12.0) * (a * a) + 0.25f * (b * b);
     const float tau5 = fabsf(beta2 - beta0);
-    const float r0 = tau5 / (beta0 + float(kWenoEps));
-    const float r1 = tau5 / (beta1 + float(kWenoEps));
-    const float r2 = tau5 / (beta2 + float(kWenoEps));
+    // r = tau5 / (beta + eps) reaches phi^2 / eps ~ 1e35 for 1e6 protons
+    // and overflows beyond; held at 1e30, where the other weights are 1e-60 of it
+    const float r0 = fminf(fast_div(tau5, beta0 + float(kWenoEps)), 1e30f);
+    const float r1 = fminf(fast_div(tau5, beta1 + float(kWenoEps)), 1e30f);
+    const float r2 = fminf(fast_div(tau5, beta2 + float(kWenoEps)), 1e30f);
     float al0, al1, al2;
     const float rmax = fmaxf(r0, fmaxf(r1, r2));
     if (rmax > 1e15f) {   // r^2 would overflow: divide every alpha by rmax^2
-        const float inv = 1.0f / rmax, e = inv * inv;
+        const float inv = fast_div(1.0f, rmax), e = inv * inv;
         const float t0 = r0 * inv, t1 = r1 * inv, t2 = r2 * inv;
         al0 = 0.1f * (e + t0 * t0);
         al1 = 0.6f * (e + t1 * t1);
@@ -156,7 +169,10 @@ PDM1_HD float weno_left_f32(float v0, float v1, float v2, float v3, float v4) {
         al1 = 0.6f * (1.0f + r1 * r1);
         al2 = 0.3f * (1.0f + r2 * r2);
     }
-    return (al0 * q0 + al1 * q1 + al2 * q2) / (6.0f * (al0 + al1 + al2));
+    // normalised weights first: al * q itself overflows (al up to 6e29 below
+    // the guard, q up to 20 max|v|)
+    const float inv = fast_div(1.0f, 6.0f * (al0 + al1 + al2));
+    return (al0 * inv) * q0 + (al1 * inv) * q1 + (al2 * inv) * q2;
 }
 
 // ---------------------------------------------------------------------------
@@ -346,10 +362,10 @@ PDM1_HD void hll_flux(const T L[4], const T R[4], int axis, bool unit_speeds, T 
 struct SideF32 { float phi, jx, jy, jz, jn, f, nx, ny, nz, iso, dir; };
 
 PDM1_HD void closure_f32(float phi, float jn, float &f, float &iso, float &dir) {
-    f = phi > 0.0f ? fminf(jn / phi, 1.0f) : 0.0f;
+    f = phi > 0.0f ? fminf(fast_div(jn, phi), 1.0f) : 0.0f;
     const float q = (1.0f - f) * (1.0f + f);
     const float r = sqrtf(1.0f + 3.0f * q);
-    iso = q / (r + 1.0f);
+    iso = fast_div(q, r + 1.0f);
     dir = 2.0f - r;
 }
 
@@ -360,13 +376,13 @@ PDM1_HD SideF32 side_f32(const float u[4]) {
     s.jn = sqrtf(s.jx * s.jx + s.jy * s.jy + s.jz * s.jz);
     const float jmax = float(1.0 - kRealEps) * s.phi;
     if (s.jn > jmax) {   // realizability projection onto |J| = jmax
-        const float sc = jmax / s.jn;
+        const float sc = fast_div(jmax, s.jn);
         s.jx *= sc; s.jy *= sc; s.jz *= sc;
         s.jn = jmax;
     }
     closure_f32(s.phi, s.jn, s.f, s.iso, s.dir);
     if (s.jn > 0.0f) {
-        const float inv = 1.0f / s.jn;
+        const float inv = fast_div(1.0f, s.jn);
         s.nx = s.jx * inv; s.ny = s.jy * inv; s.nz = s.jz * inv;
     } else {
         s.nx = s.ny = s.nz = 0.0f;
@@ -387,7 +403,7 @@ PDM1_HD void speeds_f32(const SideF32 &s, int axis, float &lmin, float &lmax) {
     const float den = 2.0f + 6.0f * iso;
     float disc = 4.0f * f * f * mu * mu - den * (2.0f * dir * mu * mu - 4.0f * iso);
     disc = fmaxf(disc, 0.0f);
-    const float root = sqrtf(disc), inv = 1.0f / den, c = 2.0f * f * mu;
+    const float root = sqrtf(disc), inv = fast_div(1.0f, den), c = 2.0f * f * mu;
     lmin = (c - root) * inv;
     lmax = (c + root) * inv;
 }
@@ -435,7 +451,7 @@ PDM1_HD void face_flux_f32(const float L[4], const float R[4], int axis, bool un
         for (int c = 0; c < 4; ++c) F[c] = 0.5f * (FL[c] + FR[c]);
         return;
     }
-    const float inv = 1.0f / den, sp = sl * sr;
+    const float inv = fast_div(1.0f, den), sp = sl * sr;
     const float dl[4] = {b.phi - a.phi, b.jx - a.jx, b.jy - a.jy, b.jz - a.jz};
 #pragma unroll
     for (int c = 0; c < 4; ++c) F[c] = (sr * FL[c] - sl * FR[c] + sp * dl[c]) * inv;

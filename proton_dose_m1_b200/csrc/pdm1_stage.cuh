@@ -9,7 +9,7 @@
 namespace pdm1 {
 
 template <typename T, int MODE, class Tl>
-__global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 3) stage_kernel(StageArgs a) {
+__global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 4) stage_kernel(StageArgs a) {
     constexpr int TX = Tl::TX, TY = Tl::TY, TZ = Tl::TZ;
     constexpr int NF = Tl::NF, NFX = Tl::NFX, NFY = Tl::NFY;
     constexpr int SX = Tl::SX, SY = Tl::SY, SZ = Tl::SZ;

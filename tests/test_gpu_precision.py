@@ -68,3 +68,18 @@ def test_fp32_gate_full_size_slab(moving):
                        numerics=Numerics(energy_scheme=EnergyScheme.IF_SSPRK3, cfl=0.9, max_energy_step=0.5))
     score = check_gate(cfg, moving)
     assert abs(score["range"]["r80_difference_mm"]) < 0.1
+
+
+@pytest.mark.parametrize("n_protons", [1e6, 1e12])
+def test_fp32_gate_holds_at_high_fluence(n_protons):
+    """WENO-Z's smoothness ratio tau5 / (beta + 1e-12) grows with the square
+    of the fluence (beta ~ phi^2 against an absolute epsilon): with 1e12
+    protons it leaves the float range.  The FP32 form holds it at 1e30 and
+    keeps the gate against the FP64 march of the same beam."""
+    geo = Geometry(size=(0.03, 0.03, 0.06), resolution=(30, 30, 60),
+                   objects=[Box(-0.015, 0.0, -0.015, 0.015, 0.02, 0.03, Material.BONE_COMPACT)])
+    cfg = SolverConfig(geometry=geo,
+                       beam=Beam(n_protons=n_protons, energy=60.0, energy_spread=1.0, sigma=(0.003, 0.003)),
+                       physics=Physics(scattering=Scattering.WENTZEL, nuclear=True),
+                       numerics=Numerics(energy_scheme=EnergyScheme.IF_SSPRK3, cfl=0.9, max_energy_step=0.5))
+    check_gate(cfg, True)
