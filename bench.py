@@ -59,10 +59,12 @@ FIELDS = {
                           "1e6 protons) on a 128x128x256 @1 mm water phantom with 6-12 seeded ellipsoids "
                           "of water/lung/bone/muscle; Wentzel-VI + nuclear, WENO-Z/HLL/IF-SSPRK3, "
                           "cfl 0.9, max dE 0.5"),
-    # with the phantom-wide CFL bound and the fused float face flux, the FP32
-    # form keeps the three gate spots at |dDmax| 0.08 / 0.27 / 0.03 %
+    # FP64 stencil: on this phantom the FP32 form's maximum-dose difference
+    # lands on either side of the 0.5 % bar (0.22 % and 0.81 % for two builds
+    # that differ only in float rounding: its energy-step sequence departs
+    # from the FP64 one, and the pelvis' Bragg-peak maxima move ~1 % with it)
     "pelvis1024": dict(phantom="pelvis", seed=5, n_side=32, pitch=3e-3, energy=(70.0, 230.0),
-                       gate_beams=3, precision="fp32",
+                       gate_beams=3, precision="fp64",
                        desc="1024 spots (32x32 at 3 mm, E~U[70,230] MeV, sigma~U[2,6] mm, sigma_E 1 MeV, "
                             "1e6 protons) on a 256x256x320 @1 mm synthetic pelvis (water/muscle body, "
                             "ADIPOSE_SYNTH shell = water scaled to 950 kg/m3, bone ring, two bone femoral "

@@ -323,11 +323,10 @@ __device__ void mlp_warp16(const BoxModelDev &M, const __nv_bfloat16 *x, __nv_bf
 // plans) also reduces the slab maxima the significant box is taken from.
 __global__ void __launch_bounds__(NT) box_moments_kernel(const ConfigDev *cfp, const MarchState *sts, int record) {
     const ConfigDev &cf = *cfp;
-    constexpr int kSums = ACC_MAX;   // summed entries; max phi separately
-    __shared__ double part[NT / 32][kSums + 1];
+    __shared__ double part[NT / 32][ACC_MAX + 1];
     __shared__ double pl[kMaxTileZ];
     __shared__ double buf[NT];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x;
     const int total = record ? sts[0].dom.ntiles : cf.tile_off[cf.nbeams];
     for (int gt = blockIdx.x; gt < total; gt += gridDim.x) {
         const int b = (record || cf.nbeams == 1) ? 0 : beam_of_tile(cf.tile_off, cf.nbeams, gt);
@@ -340,73 +339,45 @@ __global__ void __launch_bounds__(NT) box_moments_kernel(const ConfigDev *cfp, c
         const int i0 = tx * TX, j0 = ty * TY, k0 = tz * TZ;
         const int ii = tid / (TY * TZ), jj = (tid / TZ) % TY, kk = tid % TZ;
         const int li = i0 + ii, lj = j0 + jj, lk = k0 + kk;
-        if (tid < TZ) pl[tid] = 0.0;
-        double v[kSums + 1];
-#pragma unroll
-        for (int q = 0; q <= kSums; ++q) v[q] = 0.0;
-        double phi = 0.0;
-        if (li < d.nx && lj < d.ny && lk < d.nz) {
+        const bool valid = li < d.nx && lj < d.ny && lk < d.nz;
+        double u[4] = {0.0, 0.0, 0.0, 0.0};
+        if (valid) {
             const size_t N = (size_t)d.nx * d.ny * d.nz, o = ((size_t)li * d.ny + lj) * d.nz + lk;
-            const double *U = st.Ua;
-            phi = U[o];
-            const double jx = U[N + o], jy = U[2 * N + o], jz = U[3 * N + o];
-            const double gx = d.i0 + li + 0.5, gy = d.j0 + lj + 0.5, gz = d.k0 + lk + 0.5;
-            v[ACC_M] = phi;
-            v[ACC_X] = phi * gx; v[ACC_X + 1] = phi * gy; v[ACC_X + 2] = phi * gz;
-            v[ACC_X2] = phi * gx * gx; v[ACC_X2 + 1] = phi * gy * gy; v[ACC_X2 + 2] = phi * gz * gz;
-            v[ACC_J] = jx; v[ACC_J + 1] = jy; v[ACC_J + 2] = jz;
-            v[ACC_JABS] = fabs(jx); v[ACC_JABS + 1] = fabs(jy);
-            if (li == 0 && d.i0 > 0) v[ACC_FACE + 0] = fabs(jx);
-            if (li == d.nx - 1 && d.i0 + d.nx < cf.nx) v[ACC_FACE + 1] = fabs(jx);
-            if (lj == 0 && d.j0 > 0) v[ACC_FACE + 2] = fabs(jy);
-            if (lj == d.ny - 1 && d.j0 + d.ny < cf.ny) v[ACC_FACE + 3] = fabs(jy);
-            if (lk == 0 && d.k0 > 0) v[ACC_FACE + 4] = fabs(jz);
-            if (lk == d.nz - 1 && d.k0 + d.nz < cf.nz) v[ACC_FACE + 5] = fabs(jz);
-            v[kSums] = phi;
-        }
-        buf[tid] = phi;
-        __syncthreads();   // pl zeroed, buf filled
-        atomicAdd(&pl[kk], v[ACC_J + 2]);
 #pragma unroll
-        for (int q = 0; q < kSums; ++q)
-            for (int w = 16; w > 0; w >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], w);
-        for (int w = 16; w > 0; w >>= 1) v[kSums] = fmax(v[kSums], __shfl_xor_sync(0xffffffffu, v[kSums], w));
-        if (lane == 0)
-            for (int q = 0; q <= kSums; ++q) part[warp][q] = v[q];
-        if (record) tile_slab_max(cf, cf.slab, d, buf, i0, j0, k0);
-        __syncthreads();
-        double *acc = cf.acc + (size_t)b * kAcc;
-        if (tid < kSums) {
-            double s = 0.0;
-            for (int w = 0; w < NT / 32; ++w) s += part[w][tid];
-            if (s != 0.0) atomicAdd(&acc[tid], s);
-        } else if (tid == kSums) {
-            double m = 0.0;
-            for (int w = 0; w < NT / 32; ++w) m = fmax(m, part[w][kSums]);
-            atomic_max_double(reinterpret_cast<unsigned long long *>(&acc[ACC_MAX]), m);
-        } else if (tid >= 32 && tid < 32 + TZ) {
-            const int k = tid - 32;
-            if (k0 + k < d.nz && pl[k] != 0.0) atomicAdd(&cf.plane[(size_t)b * cf.nz + d.k0 + k0 + k], pl[k]);
+            for (int c = 0; c < 4; ++c) u[c] = st.Ua[c * N + o];
         }
-        __syncthreads();
+        if (record) {
+            buf[tid] = valid ? u[0] : 0.0;
+            __syncthreads();
+            tile_slab_max(cf, cf.slab, d, buf, i0, j0, k0);
+        }
+        tile_moments_cta(cf, b, d, k0, valid, li, lj, lk, u, part, pl);
     }
+}
+
+// Largest z-plane current density over the planes [k_lo, k_hi), by one warp
+// (every lane returns it).
+__device__ __forceinline__ double plane_max_warp(const double *plane, int k_lo, int k_hi, int lane) {
+    double m = 0.0;
+    for (int k = k_lo + lane; k < k_hi; k += 32) m = fmax(m, plane[k]);
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    return m;
 }
 
 // Features of a beam's state (one thread): energy, last dE, the significant
 // box, and the fluence moments relative to it.  Returns false when the box
-// holds no fluence.  *current receives the largest z-plane current over the
-// planes [k_lo, k_hi) (particles per MeV).
-__device__ bool box_features(const ConfigDev &cf, const double *acc, const double *plane, int k_lo, int k_hi,
-                             const int sig[6], double E, double dE, float *f, double *current) {
-    double I = 0.0;
-    for (int k = k_lo; k < k_hi; ++k) I = fmax(I, plane[k]);
-    I *= cf.dx * cf.dy;
+// holds no fluence.  plane_max: the largest z-plane current density of the
+// box (plane_max_warp); *current receives it as a current (particles per
+// MeV).  S_E: the stopping power of material 0 at E when known, else <= 0.
+__device__ bool box_features(const ConfigDev &cf, const double *acc, double plane_max, const int sig[6], double E,
+                             double dE, double S_E, float *f, double *current) {
+    const double I = plane_max * (cf.dx * cf.dy);
     *current = I;
     const double M = acc[ACC_M];
     for (int q = 0; q < kFeat; ++q) f[q] = 0.f;
     if (!(M > 0.0) || sig[1] < 0) return false;
-    double S = 0.0;
-    if (!stopping_power_dev(cf.mats[0], E, S) || !(S > 0.0)) S = 1.0;
+    double S = S_E;
+    if (!(S > 0.0) && (!stopping_power_dev(cf.mats[0], E, S) || !(S > 0.0))) S = 1.0;
     f[0] = (float)(E / 100.0);
     f[1] = (float)(dE / cf.max_dE);
     for (int a = 0; a < 3; ++a) {
@@ -434,18 +405,30 @@ __global__ void __launch_bounds__(128) box_learn_kernel(const ConfigDev *cfp, Co
     __shared__ __align__(16) __nv_bfloat16 hs[4][16 * kHid];
     __shared__ float os[4][16 * kOutPad];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int b = (blockIdx.x * 4 + warp) * 16 + lane;
+    const int b0 = (blockIdx.x * 4 + warp) * 16, b = b0 + lane;
     const bool mine = lane < 16 && b < cf.nbeams;
     MarchState *st = mine ? sts + b : nullptr;
     const bool live = mine && !(st->done || st->error);
+    // the z-plane current maxima of the warp's beams, all 32 lanes per beam;
+    // each lane clears the planes it read for the next step's moments
+    double pmax = 0.0;
+    for (int q = 0; q < 16 && b0 + q < cf.nbeams; ++q) {
+        const MarchState &sq = sts[b0 + q];
+        if (sq.done || sq.error) continue;   // the same for every lane
+        double *pq = cf.plane + (size_t)(b0 + q) * cf.nz;
+        const int k_lo = sq.dom.k0, k_hi = sq.dom.k0 + sq.dom.nz;
+        const double v = plane_max_warp(pq, k_lo, k_hi, lane);
+        for (int k = k_lo + lane; k < k_hi; k += 32) pq[k] = 0.0;
+        if (lane == q) pmax = v;
+    }
     float f[kFeat];
     double current = 0.0;
     bool valid = false;
     if (live) {
         const double *acc = cf.acc + (size_t)b * kAcc;
-        const double *plane = cf.plane + (size_t)b * cf.nz;
-        valid = box_features(cf, acc, plane, st->dom.k0, st->dom.k0 + st->dom.nz, st->sig, st->E, cos[b].dE, f,
-                             &current);
+        // prologue_kernel left S1 = S(E_next) with E_next the energy of this step
+        const double S_E = cos[b].E_next == st->E ? cos[b].S1[0] : 0.0;
+        valid = box_features(cf, acc, pmax, st->sig, st->E, cos[b].dE, S_E, f, &current);
     } else {
         for (int q = 0; q < kFeat; ++q) f[q] = 0.f;
     }
@@ -457,7 +440,7 @@ __global__ void __launch_bounds__(128) box_learn_kernel(const ConfigDev *cfp, Co
     if (!live) return;
     const BeamDev &bm = cf.beams[b];
     Coeffs *co = cos + b;
-    const double ed = energy_density(bm, st->E);
+    const double ed = co->E_next == st->E ? co->ed_next : energy_density(bm, st->E);
     double *acc = cf.acc + (size_t)b * kAcc;
     DomainDev nb;
     if (st->sig[1] < 0) {
@@ -494,8 +477,6 @@ __global__ void __launch_bounds__(128) box_learn_kernel(const ConfigDev *cfp, Co
         }
     }
     for (int q = 0; q < kAcc; ++q) acc[q] = 0.0;
-    double *plane = cf.plane + (size_t)b * cf.nz;
-    for (int k = 0; k < cf.nz; ++k) plane[k] = 0.0;
     switch_box(cf, bm, co, st, b, nb, ed);
 }
 
@@ -519,6 +500,7 @@ __global__ void __launch_bounds__(256) record_kernel(const ConfigDev *cfp, const
         significant_box_cta(cf, bm, d, slab, ed, red, s_lo, s_hi, &s_scale, cf.tol);
         significant_box_cta(cf, bm, d, slab, ed, red, s_lo2[0], s_hi2[0], &s_scale2, cf.rec_tail_tol[0]);
         significant_box_cta(cf, bm, d, slab, ed, red, s_lo2[1], s_hi2[1], &s_scale2, cf.rec_tail_tol[1]);
+        const double pmax = t < 32 ? plane_max_warp(cf.plane, 0, cf.nz, t) : 0.0;
         if (t == 0) {
             const int row = st->step - 1;
             const bool none = s_scale == 0.0 || s_hi[0] < 0 || s_hi[1] < 0 || s_hi[2] < 0;
@@ -535,7 +517,7 @@ __global__ void __launch_bounds__(256) record_kernel(const ConfigDev *cfp, const
             }
             float f[kFeat];
             double current = 0.0;
-            box_features(cf, acc, cf.plane, 0, cf.nz, sig, st->E, co->dE, f, &current);
+            box_features(cf, acc, pmax, sig, st->E, co->dE, 0.0, f, &current);
             if (cf.rec && row >= 0 && row < cf.rec_max) {
                 float *r = cf.rec + (size_t)row * PDM1_RECORD_WIDTH;
                 r[0] = (float)st->E;

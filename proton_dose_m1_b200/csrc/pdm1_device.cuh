@@ -260,7 +260,8 @@ __host__ __device__ inline DomainDev make_domain(int i0, int j0, int k0, int nx,
     return d;
 }
 
-enum StageMode { MODE_A = 0, MODE_B = 1, MODE_C = 2, MODE_EULER = 3, MODE_RHS = 4 };
+enum StageMode { MODE_A = 0, MODE_B = 1, MODE_C = 2, MODE_EULER = 3, MODE_RHS = 4,
+                 MODE_C_LEARN = 5 };   // launch selector: stage C with the learned box's moments
 
 struct StageArgs {
     const ConfigDev *cf;
@@ -436,6 +437,62 @@ __device__ __forceinline__ int beam_of_tile(const int *tile_off, int nbeams, int
 
 __device__ __forceinline__ unsigned long long *beam_slab(const ConfigDev &cf, int b) {
     return cf.slab + (size_t)b * (cf.nx + cf.ny + cf.nz);
+}
+
+// Learned box: one tile's contribution to the beam's fluence moments, face
+// currents and z-plane currents (acc, plane) from the state u of each cell
+// (cell (li, lj, lk) of domain d, `valid` inside it).  Called by every thread
+// of a CTA of NT threads laid out as the stage tile (k fastest); `part` and
+// `pl` are shared scratch of NT/32 x (ACC_MAX + 1) and kMaxTileZ doubles.
+__device__ __forceinline__ void tile_moments_cta(const ConfigDev &cf, int b, const DomainDev &d, int k0,
+                                                 bool valid, int li, int lj, int lk, const double u[4],
+                                                 double (*part)[ACC_MAX + 1], double *pl) {
+    constexpr int kSums = ACC_MAX;   // summed entries; max phi separately
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int kk = tid % d.tz;
+    if (tid < d.tz) pl[tid] = 0.0;
+    double v[kSums + 1];
+#pragma unroll
+    for (int q = 0; q <= kSums; ++q) v[q] = 0.0;
+    if (valid) {
+        const double phi = u[0], jx = u[1], jy = u[2], jz = u[3];
+        const double gx = d.i0 + li + 0.5, gy = d.j0 + lj + 0.5, gz = d.k0 + lk + 0.5;
+        v[ACC_M] = phi;
+        v[ACC_X] = phi * gx; v[ACC_X + 1] = phi * gy; v[ACC_X + 2] = phi * gz;
+        v[ACC_X2] = phi * gx * gx; v[ACC_X2 + 1] = phi * gy * gy; v[ACC_X2 + 2] = phi * gz * gz;
+        v[ACC_J] = jx; v[ACC_J + 1] = jy; v[ACC_J + 2] = jz;
+        v[ACC_JABS] = fabs(jx); v[ACC_JABS + 1] = fabs(jy);
+        if (li == 0 && d.i0 > 0) v[ACC_FACE + 0] = fabs(jx);
+        if (li == d.nx - 1 && d.i0 + d.nx < cf.nx) v[ACC_FACE + 1] = fabs(jx);
+        if (lj == 0 && d.j0 > 0) v[ACC_FACE + 2] = fabs(jy);
+        if (lj == d.ny - 1 && d.j0 + d.ny < cf.ny) v[ACC_FACE + 3] = fabs(jy);
+        if (lk == 0 && d.k0 > 0) v[ACC_FACE + 4] = fabs(jz);
+        if (lk == d.nz - 1 && d.k0 + d.nz < cf.nz) v[ACC_FACE + 5] = fabs(jz);
+        v[kSums] = phi;
+    }
+    __syncthreads();   // pl zeroed
+    atomicAdd(&pl[kk], v[ACC_J + 2]);
+#pragma unroll
+    for (int q = 0; q < kSums; ++q)
+        for (int w = 16; w > 0; w >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], w);
+    for (int w = 16; w > 0; w >>= 1) v[kSums] = fmax(v[kSums], __shfl_xor_sync(0xffffffffu, v[kSums], w));
+    if (lane == 0)
+        for (int q = 0; q <= kSums; ++q) part[warp][q] = v[q];
+    __syncthreads();
+    double *acc = cf.acc + (size_t)b * kAcc;
+    if (tid < kSums) {
+        double s = 0.0;
+        for (int w = 0; w < NT / 32; ++w) s += part[w][tid];
+        if (s != 0.0) atomicAdd(&acc[tid], s);
+    } else if (tid == kSums) {
+        double m = 0.0;
+        for (int w = 0; w < NT / 32; ++w) m = fmax(m, part[w][kSums]);
+        atomic_max_double(reinterpret_cast<unsigned long long *>(&acc[ACC_MAX]), m);
+    } else if (tid >= 32 && tid < 32 + d.tz) {
+        const int k = tid - 32;
+        if (k0 + k < d.nz && pl[k] != 0.0) atomicAdd(&cf.plane[(size_t)b * cf.nz + d.k0 + k0 + k], pl[k]);
+    }
+    __syncthreads();
 }
 
 // The significant box of desired_box (moving_active_domain.py:107-151):

@@ -891,6 +891,7 @@ void launch_stage64(int mode, int grid, const StageArgs &a, cudaStream_t stream)
     case MODE_A: stage_kernel<double, MODE_A, Tl><<<grid, NT, bytes, stream>>>(a); break;
     case MODE_B: stage_kernel<double, MODE_B, Tl><<<grid, NT, bytes, stream>>>(a); break;
     case MODE_C: stage_kernel<double, MODE_C, Tl><<<grid, NT, bytes, stream>>>(a); break;
+    case MODE_C_LEARN: stage_kernel<double, MODE_C, Tl, true><<<grid, NT, bytes, stream>>>(a); break;
     case MODE_EULER: stage_kernel<double, MODE_EULER, Tl><<<grid, NT, bytes, stream>>>(a); break;
     default: stage_kernel<double, MODE_RHS, Tl><<<grid, NT, bytes, stream>>>(a); break;
     }
@@ -898,6 +899,7 @@ void launch_stage64(int mode, int grid, const StageArgs &a, cudaStream_t stream)
 
 // One stage launch in the plan's precision and tile shape.
 void launch_stage(const pdm1_plan *pl, int mode, int grid, const StageArgs &a, cudaStream_t stream) {
+    if (mode == MODE_C && pl->cf.learned) mode = MODE_C_LEARN;
     if (pl->p.precision == PDM1_FP32_FP64) {
         launch_stage_fp32(mode, pl->cf.tile_id, grid, a, stream);
         return;
@@ -917,9 +919,10 @@ int launch_box_step(pdm1_plan *pl, cudaStream_t stream) {
     box_kernel<<<pl->nbeams, 256, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st);
     int n = 3;
     if (pl->cf.learned) {
-        launch_box_moments(pl->d_cf, pl->d_st, pl->cf.grid_ctas, 0, stream);
+        // the moments of the state come from the last stage C (tile_moments_cta);
+        // before the first step the accumulators hold zeros (no stage C yet)
         launch_box_learn(pl->d_cf, pl->d_co, pl->d_st, pl->nbeams, stream);
-        n += 2;
+        n += 1;
     }
     if (p.vacuum_aware_cfl) {
         rebox_kernel<<<cells, NT, 0, stream>>>(pl->d_cf, pl->d_co, pl->d_st, 0);
@@ -978,6 +981,7 @@ cudaError_t set_attributes64() {
     cudaError_t e = cudaFuncSetAttribute(stage_kernel<double, MODE_A, Tl>, attr, bytes);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<double, MODE_B, Tl>, attr, bytes);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<double, MODE_C, Tl>, attr, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<double, MODE_C, Tl, true>, attr, bytes);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<double, MODE_EULER, Tl>, attr, bytes);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<double, MODE_RHS, Tl>, attr, bytes);
     return e;

@@ -8,7 +8,9 @@
 
 namespace pdm1 {
 
-template <typename T, int MODE, class Tl>
+// LEARN (stage C of a plan with a learned box): the tile's fluence moments of
+// the new state are accumulated for the next step's proposer.
+template <typename T, int MODE, class Tl, bool LEARN = false>
 __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 4) stage_kernel(StageArgs a) {
     constexpr int TX = Tl::TX, TY = Tl::TY, TZ = Tl::TZ;
     constexpr int NF = Tl::NF, NFX = Tl::NFX, NFY = Tl::NFY;
@@ -182,6 +184,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 4) stage
         const int li = i0 + i, lj = j0 + j, lk = k0 + k;
         const bool valid = li < nx && lj < ny && lk < nz;
         double phi_new = -1.0;   // for the moving box's slab maxima
+        double um[4] = {0.0, 0.0, 0.0, 0.0};   // the new state, for the learned box's moments
         if (valid) {
             const int fx0 = (i * TY + j) * TZ + k, fx1 = ((i + 1) * TY + j) * TZ + k;
             const int fy0 = NFX + (i * (TY + 1) + j) * TZ + k, fy1 = NFX + (i * (TY + 1) + j + 1) * TZ + k;
@@ -281,6 +284,9 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 4) stage
 #pragma unroll
                             for (int c = 1; c < 4; ++c) unew[c] *= co.hs[m];
                     }
+                    if (MODE == MODE_C)
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) um[c] = unew[c];
                     double *dst = MODE == MODE_C ? Ua : U1;
                     bool finite = true;
 #pragma unroll
@@ -315,6 +321,12 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 4) stage
             slab_buf[tid] = phi_new;
             __syncthreads();
             tile_slab_max(cf, beam_slab(cf, b), d, slab_buf, i0, j0, k0);
+        }
+        if constexpr (LEARN && MODE == MODE_C) {
+            // learned box: the moments of the new state feed the next step's proposer
+            __shared__ double mom_part[NT / 32][ACC_MAX + 1];
+            __shared__ double mom_pl[kMaxTileZ];
+            tile_moments_cta(cf, b, d, k0, valid, li, lj, lk, um, mom_part, mom_pl);
         }
         __syncthreads();   // shared memory is reused by the next tile
     }

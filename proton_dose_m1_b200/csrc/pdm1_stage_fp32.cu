@@ -19,6 +19,7 @@ cudaError_t set_attributes() {
     cudaError_t e = cudaFuncSetAttribute(stage_kernel<float, MODE_A, Tl>, attr, bytes);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<float, MODE_B, Tl>, attr, bytes);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<float, MODE_C, Tl>, attr, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<float, MODE_C, Tl, true>, attr, bytes);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<float, MODE_EULER, Tl>, attr, bytes);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(stage_kernel<float, MODE_RHS, Tl>, attr, bytes);
     return e;
@@ -31,6 +32,7 @@ void launch(int mode, int grid, const StageArgs &a, cudaStream_t stream) {
     case MODE_A: stage_kernel<float, MODE_A, Tl><<<grid, NT, bytes, stream>>>(a); break;
     case MODE_B: stage_kernel<float, MODE_B, Tl><<<grid, NT, bytes, stream>>>(a); break;
     case MODE_C: stage_kernel<float, MODE_C, Tl><<<grid, NT, bytes, stream>>>(a); break;
+    case MODE_C_LEARN: stage_kernel<float, MODE_C, Tl, true><<<grid, NT, bytes, stream>>>(a); break;
     case MODE_EULER: stage_kernel<float, MODE_EULER, Tl><<<grid, NT, bytes, stream>>>(a); break;
     default: stage_kernel<float, MODE_RHS, Tl><<<grid, NT, bytes, stream>>>(a); break;
     }
