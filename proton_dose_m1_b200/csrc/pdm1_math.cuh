@@ -97,28 +97,10 @@ PDM1_HD T weno_left(T v0, T v1, T v2, T v3, T v4) {
     T r0 = tau5 / (beta0 + T(kWenoEps));
     T r1 = tau5 / (beta1 + T(kWenoEps));
     T r2 = tau5 / (beta2 + T(kWenoEps));
-    T al0, al1, al2;
-    if (sizeof(T) < sizeof(double)) {
-        // single precision: r^2 overflows above ~1.8e19, which a flat stencil
-        // next to a steep one reaches (beta ~ 0 against beta ~ phi^2 ~ 1e22);
-        // divide every alpha by rmax^2 first -- the weights are unchanged
-        T rmax = fmax(r0, fmax(r1, r2));
-        if (rmax > T(1e15)) {
-            T inv = T(1) / rmax;
-            T q0 = r0 * inv, q1 = r1 * inv, q2 = r2 * inv, e = inv * inv;
-            al0 = T(0.1) * (e + q0 * q0);
-            al1 = T(0.6) * (e + q1 * q1);
-            al2 = T(0.3) * (e + q2 * q2);
-        } else {
-            al0 = T(0.1) * (T(1) + r0 * r0);
-            al1 = T(0.6) * (T(1) + r1 * r1);
-            al2 = T(0.3) * (T(1) + r2 * r2);
-        }
-    } else {
-        al0 = T(0.1) * (T(1) + r0 * r0);
-        al1 = T(0.6) * (T(1) + r1 * r1);
-        al2 = T(0.3) * (T(1) + r2 * r2);
-    }
+    // the FP64 path; single precision has its own form, weno_left_f32
+    T al0 = T(0.1) * (T(1) + r0 * r0);
+    T al1 = T(0.6) * (T(1) + r1 * r1);
+    T al2 = T(0.3) * (T(1) + r2 * r2);
     T s = al0 + al1 + al2;
     T w0 = al0 / s, w1 = al1 / s, w2 = al2 / s;
     return w0 * p0 + w1 * p1 + w2 * p2;
