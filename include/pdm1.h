@@ -163,9 +163,14 @@ int pdm1_march_steps(pdm1_plan *plan, double *U, double *dose, double *energies,
  * (roughly more than 130000 cells) are rejected with PDM1_ERR_ARGUMENT.  The
  * caller passes the problem (host), U (device, in/out), dose and energies
  * (device, out) exactly as for pdm1_plan_create + pdm1_march, without snapshots.
+ * It marches the full domain in FP64: a problem asking for the moving active
+ * box or the FP32 stencil is rejected with PDM1_ERR_UNSUPPORTED.
  * The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress) and sets kernel attributes, so make it before any
- * stream capture.  All calls on a device share the one array and it keeps the
+ * stream capture; first calls from several host threads take turns on a lock.
+ * The looked-up address is kept for the life of the process: after a
+ * cudaDeviceReset of that device this entry point must not be called again.
+ * All calls on a device share the one array and it keeps the
  * last call's contents (the march state is cleared at the start of every
  * call): calls that overlap on the GPU race.  Launches directly on `stream`
  * (no graph, no events) and synchronises it before returning. */

@@ -27,6 +27,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1678,6 +1679,7 @@ constexpr int kNoAllocMaxDevices = 64;
 // Device address of g_noalloc_scratch per device: in host code the symbol is
 // only a host-side stand-in, so the address comes from cudaGetSymbolAddress.
 void *g_noalloc_base[kNoAllocMaxDevices];
+std::mutex g_noalloc_setup_mutex;
 
 // PCHIP nodal slopes on the device, the same expressions as pchip_slopes()
 // (physics/stopping_power.py:94-138), one thread per node.
@@ -1756,6 +1758,9 @@ extern "C" int pdm1_march_noalloc(const pdm1_problem *problem, double *U, double
     const pdm1_problem &p = *problem;
     if (p.moving_active_domain)
         return set_error(PDM1_ERR_UNSUPPORTED, "pdm1_march_noalloc: the moving active box needs a plan");
+    if (p.precision != PDM1_FP64)
+        return set_error(PDM1_ERR_UNSUPPORTED,
+                         "pdm1_march_noalloc: marches in FP64 only (the FP32 stencil needs a plan)");
     const size_t N = (size_t)p.nx * p.ny * p.nz;
 
     // layout of the scratch array
@@ -1809,6 +1814,9 @@ extern "C" int pdm1_march_noalloc(const pdm1_problem *problem, double *U, double
     int dev = 0;
     CUDA_TRY(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kNoAllocMaxDevices) return set_error(PDM1_ERR_ARGUMENT, "device ordinal too large");
+    // host threads making their first call on a device at the same time take turns
+    // (the lock is held for the set-up only, not for the march)
+    std::unique_lock<std::mutex> setup_lock(g_noalloc_setup_mutex);
     if (!g_noalloc_base[dev]) {
         void *ptr = nullptr;
         CUDA_TRY(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
@@ -1819,6 +1827,7 @@ extern "C" int pdm1_march_noalloc(const pdm1_problem *problem, double *U, double
         g_noalloc_base[dev] = ptr;
     }
     unsigned char *base = static_cast<unsigned char *>(g_noalloc_base[dev]);
+    setup_lock.unlock();
     cudaStream_t stream = (cudaStream_t)stream_;
     ConfigDev *d_cf = reinterpret_cast<ConfigDev *>(base + o_cf);
     Coeffs *d_co = reinterpret_cast<Coeffs *>(base + o_co);

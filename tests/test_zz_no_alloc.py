@@ -19,7 +19,7 @@ torch = pytest.importorskip("torch")
 
 from proton_dose_m1_b200 import _native
 from proton_dose_m1_b200 import Beam, Geometry, Numerics, SolverConfig
-from proton_dose_m1_b200.enums import EnergyScheme
+from proton_dose_m1_b200.enums import EnergyScheme, SpatialScheme
 from proton_dose_m1_b200.numerics.boundary import BeamInflow
 from proton_dose_m1_b200.numerics.energy import M1Plan
 from proton_dose_m1_b200.numerics.grid import Grid
@@ -31,6 +31,7 @@ pytestmark = pytest.mark.gpu
 
 _SCATTER = {"OFF": 0, "ROSSI": 1, "WENTZEL": 2}
 _SCHEME = {"FORWARD_EULER": 0, "SSPRK3": 1, "IF_SSPRK3": 2}
+_SPATIAL = {"WENO_Z": 0, "FIRST_ORDER": 1, "MUSCL": 2, "WENO3": 3}
 
 
 def problem_struct(cfg):
@@ -72,6 +73,7 @@ def problem_struct(cfg):
     p.energy_min, p.energy_window_sigma = num.energy_min, num.energy_window_sigma
     p.active_guard_cells = num.active_guard_cells
     p.precision = 0
+    p.spatial_scheme = _SPATIAL[num.spatial_scheme.name]
     return p, keep, (mm, grid, inflow)
 
 
@@ -107,6 +109,46 @@ def test_noalloc_matches_planned_march_twice(lib, name):
         np.testing.assert_array_equal(E, E_ref)
         np.testing.assert_array_equal(dose, dose_ref)
         np.testing.assert_array_equal(U, U_ref)
+
+
+def _variant(name, **numerics):
+    from dataclasses import replace
+    cfg = cases.march_config(cases.march_specs()[name])
+    return replace(cfg, numerics=replace(cfg.numerics, **numerics))
+
+
+# the integrators and reconstructions besides IF-SSPRK3 + WENO-Z: forward Euler
+# (its own stage and finishing kernel), SSPRK3 with the Strang-split sources,
+# and the narrower reconstructions with their own inflow ghosts
+VARIANTS = {
+    "forward_euler": dict(energy_scheme=EnergyScheme.FORWARD_EULER),
+    "ssprk3_strang": dict(energy_scheme=EnergyScheme.SSPRK3),
+    "muscl": dict(spatial_scheme=SpatialScheme.MUSCL),
+    "weno3_euler": dict(spatial_scheme=SpatialScheme.WENO3, energy_scheme=EnergyScheme.FORWARD_EULER),
+}
+
+
+@pytest.mark.parametrize("variant", sorted(VARIANTS))
+def test_noalloc_matches_planned_march_other_schemes(lib, variant):
+    cfg = _variant("hetero_snapshots", **VARIANTS[variant])
+    p, keep, (mm, grid, inflow) = problem_struct(cfg)
+    plan = M1Plan(cfg, mm, grid, inflow)
+    U_ref, dose_ref, E_ref, _ = plan.march(None)
+    U_ref, dose_ref = U_ref.cpu().numpy(), dose_ref.cpu().numpy()
+    plan.close()
+    for _ in range(2):
+        U, dose, E = noalloc_march(lib, p, grid.shape)
+        np.testing.assert_array_equal(E, E_ref)
+        np.testing.assert_array_equal(dose, dose_ref)
+        np.testing.assert_array_equal(U, U_ref)
+
+
+def test_noalloc_rejects_the_fp32_form(lib):
+    cfg = cases.march_config(cases.march_specs()["hetero_snapshots"])
+    p, keep, (_, grid, _) = problem_struct(cfg)
+    p.precision = 1
+    with pytest.raises(NotImplementedError, match="FP64"):
+        noalloc_march(lib, p, grid.shape, max_steps=10)
 
 
 def test_noalloc_alternating_sizes(lib):
