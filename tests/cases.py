@@ -13,13 +13,25 @@ from proton_dose_m1_b200.enums import (CoefficientInterpolation, EnergyScheme, M
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
 
-# Dose parity bar against the reference's own fixtures, relative to the maximum
-# dose.  Two builds of the oracle that differ only in FMA contraction disagree
-# by 4.9e-10 on kat2mm_reduced_water: the M1 closure near free streaming
-# (chi -> 1, isotropic part 0.5*(1-chi) -> 1e-10) amplifies one-ulp differences,
-# and the reference runs its HLL loop under Numba fastmath.  The bar is four
-# times that measured floor.
-REFERENCE_DOSE_RTOL = 2e-9
+# Dose parity bars against the reference's own fixtures, relative to the
+# maximum dose.  With scattering (Wentzel-VI) the oracle lands within 1e-10 of
+# every reference fixture (measured: <= 9.4e-12 on the marches, <= 4.2e-12 on
+# the published 2 mm maxima), so the bar is 1e-10.  Without scattering the
+# fluence streams almost freely: the M1 closure's isotropic part
+# 0.5*(1-chi) falls to ~1e-10 and one-ulp differences in chi move the
+# transverse fluxes at 1e-6 relative.  There the distance is a rounding floor,
+# not a defect: 1.9e-10 .. 1.4e-9 on the published 2 mm reduced-physics maxima,
+# 6.2e-10 on kat2mm_reduced_water; builds of the oracle with FMA contraction
+# (5.6e-10) or with fast-math reassociation (1.8e-9) do not get closer, and the
+# reference itself evaluates its HLL loop under Numba fastmath.  The bar there
+# is 2e-9.
+REFERENCE_DOSE_RTOL = 1e-10
+FREE_STREAMING_DOSE_RTOL = 2e-9
+
+
+def reference_rtol(cfg) -> float:
+    """The parity bar against the reference for configuration ``cfg``."""
+    return REFERENCE_DOSE_RTOL if cfg.physics.scattering.name != "OFF" else FREE_STREAMING_DOSE_RTOL
 
 
 def load(name: str):

@@ -6,7 +6,7 @@ outputs as small ``.npz`` files; also collects the deterministic maxima the
 reference publishes for its 2 mm coarse-grid runs.  Only this script reads
 the reference; the tests read the fixtures.
 
-Usage:  NUMBA_CACHE_DIR=/tmp/numba_cache python tests/golden/make_golden.py <reference root>
+Usage:  NUMBA_CACHE_DIR=/tmp/numba_cache python tests/golden/make_golden.py <reference root> [part]
 
 The reference imports plotting and gamma modules at import time that are not
 on the energy-march path (matplotlib, pymedphys); they are replaced by empty
@@ -333,6 +333,42 @@ def published(root: Path):
     (OUT / "published_kats.json").write_text(json.dumps(cases, indent=1))
 
 
+# Groups of published WENO-Z runs at full size (a GPU march each; the CPU
+# oracle is pinned on the 2 mm grids of published()):
+#   coarse_grid_1mm  24x24x200, 1 mm cubes;   coarse_grid  50x50x200;
+#   full             100x100x400 (0.24 x 0.24 x 0.5 mm), static full domain;
+#   moving           the same grids on the reference's moving active box.
+FULL_GROUPS = {
+    "coarse_grid_1mm": "thesis_results/robustness/coarse_grid_1mm/{model}/{case}/weno_z",
+    "coarse_grid": "thesis_results/robustness/coarse_grid/{model}/{case}/weno_z",
+    "full": "thesis_results/{model}/{case}/weno_z",
+    "moving": "thesis_results/robustness/moving_active_domain/{model}/{case}/weno_z",
+}
+
+
+def published_full(root: Path):
+    """Deterministic maxima, R80 and DFW the reference publishes for its
+    WENO-Z runs on finer grids (published_kats_full.json)."""
+    cases = {}
+    for group, pattern in FULL_GROUPS.items():
+        for model in ("reduced_physics", "scattering_nuclear"):
+            for case in ("homogeneous_water", "longitudinal_slabs", "transversal_slabs"):
+                rel = pattern.format(model=model, case=case)
+                d = root / rel
+                cfg = json.loads((d / "config.json").read_text())
+                met = json.loads((d / "metrics.json").read_text())
+                cases[f"{group}/{model}/{case}"] = {
+                    "source": rel,
+                    "config": {k: cfg[k] for k in ("beam", "geometry", "numerics", "physics")},
+                    "maximum_dose_Gy": met["maximum_dose"]["deterministic_Gy"],
+                    "r80_mm": met["range"]["deterministic_r80_mm"],
+                    "dfw_mm": met["range"]["deterministic_dfw_mm"],
+                    "peak_search_from_mm": met["range"].get("peak_search_from_mm"),
+                    "runtime_s": met["performance"]["deterministic_runtime_seconds"],
+                }
+    (OUT / "published_kats_full.json").write_text(json.dumps(cases, indent=1))
+
+
 def published_configs(root: Path):
     """The canonical configurations and their hashes from the reference's own
     run directories (config.json, metadata.json of thesis_results/)."""
@@ -346,9 +382,15 @@ def published_configs(root: Path):
 
 
 if __name__ == "__main__":
-    root = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) < 2:
+        sys.exit("usage: make_golden.py <reference root> [configs|published|schemes|analytical]")
+    root = Path(sys.argv[1])
     if len(sys.argv) > 2 and sys.argv[2] == "configs":
         published_configs(root)
+        sys.exit(0)
+    if len(sys.argv) > 2 and sys.argv[2] == "published":
+        published(root)
+        published_full(root)
         sys.exit(0)
     ps = import_reference(root)
     if len(sys.argv) > 2 and sys.argv[2] == "schemes":
@@ -359,6 +401,7 @@ if __name__ == "__main__":
         sys.exit(0)
     rng = np.random.default_rng(20261203)
     published(root)
+    published_full(root)
     published_configs(root)
     unit_vectors(ps, rng)
     operators(ps, rng)

@@ -115,14 +115,14 @@ def test_march_matches_reference(name):
     U, dose, energies, snaps = p.march(U0, snapshot_energies=tuple(spec["snapshots"]))
     g = cases.load(f"march_{name}.npz")
     np.testing.assert_allclose(energies, g["energies"], rtol=0, atol=1e-12)
-    assert np.abs(dose - g["dose"]).max() <= cases.REFERENCE_DOSE_RTOL * g["dose"].max()
+    assert np.abs(dose - g["dose"]).max() <= cases.reference_rtol(cfg) * g["dose"].max()
     assert len(snaps) == len(spec["snapshots"])
     for k, e in enumerate(sorted(snaps, reverse=True)):
         assert e == float(g[f"snap{k}_energy"])
         ref = g[f"snap{k}"]
-        assert np.abs(snaps[e] - ref).max() <= cases.REFERENCE_DOSE_RTOL * np.abs(ref[0]).max()
+        assert np.abs(snaps[e] - ref).max() <= cases.reference_rtol(cfg) * np.abs(ref[0]).max()
     if "phi" in g:
-        assert np.abs(U[0] - g["phi"]).max() <= cases.REFERENCE_DOSE_RTOL * np.abs(g["phi"]).max()
+        assert np.abs(U[0] - g["phi"]).max() <= cases.reference_rtol(cfg) * np.abs(g["phi"]).max()
 
 
 @pytest.mark.parametrize("case", ["reduced_physics/homogeneous_water",
@@ -132,7 +132,7 @@ def test_published_maximum_dose(case):
     cfg = cases.published_config(kat)
     p = O.OracleProblem(cfg)
     _, dose, _, _ = p.march(np.zeros((4, *cfg.geometry.resolution)))
-    assert abs(dose.max() - kat["maximum_dose_Gy"]) <= cases.REFERENCE_DOSE_RTOL * kat["maximum_dose_Gy"]
+    assert abs(dose.max() - kat["maximum_dose_Gy"]) <= cases.reference_rtol(cfg) * kat["maximum_dose_Gy"]
 
 
 @pytest.mark.parametrize("scheme", cases.SCHEMES, ids=lambda s: s.name)
@@ -161,5 +161,5 @@ def test_other_reconstruction_marches(name):
     _, dose, energies, snaps = p.march(U0, snapshot_energies=tuple(spec["snapshots"]))
     g = cases.load(f"march_{name}.npz")
     np.testing.assert_allclose(energies, g["energies"], rtol=0, atol=1e-12)
-    assert np.abs(dose - g["dose"]).max() <= cases.REFERENCE_DOSE_RTOL * g["dose"].max()
+    assert np.abs(dose - g["dose"]).max() <= cases.reference_rtol(cfg) * g["dose"].max()
     assert len(snaps) == len(spec["snapshots"])
