@@ -1,21 +1,28 @@
 """Benchmark of the M1 energy march on B200.
 
-A "step" is one complete energy march of one pencil-beam spot (150 MeV ->
-1e-4 MeV) over the workload's phantom.  ``value`` is spots/s with inputs
-resident in HBM, timed with CUDA events on the march stream; ``e2e`` is the
-same metric through the public ``energy_march`` call with host NumPy
-buffers (plan upload, host->device and device->host copies inside the timed
-region).  ``--impl reference`` times the CPU restatement of the reference
-algorithm (oracle/) on the host cores.
+Default workload: pelvis1024, a 1024-spot scanning field on a 256x256x320
+synthetic pelvis at 1 mm, in the accelerated form (moving active box,
+batched spots, FP32 stencil / FP64 dose, autotuned tile).  A "step" marches
+one batch of the field's spots (1/K of them, by decreasing energy) as one
+batched march; the K timed steps march the whole field once, and ``value``
+is the field's spots/s with inputs resident in HBM, timed with CUDA events
+on the march stream.  ``e2e`` is the same through the public
+``field_march`` call with host NumPy buffers (upload and copy-back inside
+the timed region).  ``gate`` scores a sample of the field's spots against
+the plain FP64 full-domain GPU march (gamma 1%/1 mm, max dose).
+
+Single-spot workloads (slab80, water40): a step is one complete march of
+the spot.
+
+``--impl reference`` times the CPU restatement of the reference algorithm
+(oracle/) on the host cores: one complete moving-box spot march per step.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-       [--workload slab80|water40|field256|pelvis1024]
-Under torchrun (N > 1) every rank marches its own spots (independent pencil
-beams, no data-path collective) and rank 0 prints one JSON line.
-
-Field workloads (field256: 256 spots on a 128x128x256 ellipsoid phantom;
-pelvis1024: 1024 spots on a 256x256x320 pelvis phantom): a "step" is one
-march of the whole field, batched; ``value`` is spots/s of the field.
+       [--workload pelvis1024|field256|slab80|water40] [--box heuristic|learned]
+       [--precision fp32|fp64]
+Under torchrun (N > 1) the field's spots are shared out over the ranks
+(longest-processing-time), each rank marches its share, and one all-reduce
+sums the FP64 dose; rank 0 prints one JSON line.
 """
 
 from __future__ import annotations
@@ -232,101 +239,105 @@ def static_config(cfg, beam=None):
                         numerics=replace(cfg.numerics, moving_active_domain=False))
 
 
-def oracle_cell_rate(cfg, material_map=None, target_s: float = 10.0, min_steps: int = 1):
-    """Cell-steps per second of the oracle (CPU restatement, all host threads)
-    on full-domain energy steps of ``cfg``: a bounded timing sample."""
-    from oracle.oracle import OracleProblem
-    orc = OracleProblem(static_config(cfg), material_map)
-    n_cells = float(np.prod(orc.shape))
+def reference_sample(workload_name: str, n: int):
+    """``n`` spots of a workload for the CPU reference: (config, material map,
+    energy) each, on the reference's moving active box (its fastest CPU mode,
+    numerics/energy.py:1262-1494, with its own CFL rule).  Fields: the spots at
+    the energy quantiles (k + 1/2) / n of the field; single-spot workloads: the
+    workload's spot."""
+    from dataclasses import replace
+    from proton_dose_m1_b200 import SolverConfig
+    if workload_name in FIELDS:
+        cfg, mm, grid, beams, _ = field_workload(workload_name)
+        order = sorted(range(len(beams)), key=lambda k: beams[k].energy)
+        picks = [order[min(len(order) - 1, int((k + 0.5) * len(order) / n))] for k in range(n)]
+        out = []
+        for k in picks:
+            c = SolverConfig(geometry=cfg.geometry, beam=beams[k], physics=cfg.physics,
+                             numerics=replace(cfg.numerics, moving_active_domain=True))
+            out.append((c, mm, beams[k].energy))
+        return out
+    cfg, _ = workload(workload_name)
+    c = SolverConfig(geometry=cfg.geometry, beam=cfg.beam, physics=cfg.physics,
+                     numerics=replace(cfg.numerics, moving_active_domain=True))
+    return [(c, None, cfg.beam.energy)] * n
+
+
+def oracle_spots(sample, workers: int, threads_per_worker: int):
+    """March every spot of ``sample`` completely with the oracle (moving box),
+    ``workers`` spots at a time, each on ``threads_per_worker`` OpenMP
+    threads.  Returns (wall seconds, [(energy, steps, seconds)])."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle.oracle import OracleProblem, set_threads
+
+    def one(item):
+        cfg, mm, energy = item
+        set_threads(threads_per_worker)   # per host thread (OpenMP nthreads-var)
+        prob = OracleProblem(cfg, mm)
+        t0 = time.perf_counter()
+        _, _, E, _ = prob.march(None)
+        return energy, len(E) - 1, time.perf_counter() - t0
+
     t0 = time.perf_counter()
-    _, _, done = orc.march_steps(1)
-    first = time.perf_counter() - t0
-    k = max(min_steps, min(50, int(target_s / max(first, 1e-3))))
-    t0 = time.perf_counter()
-    _, _, done = orc.march_steps(k)
-    dt = time.perf_counter() - t0
-    return done * n_cells / dt, done, dt
+    with ThreadPoolExecutor(max_workers=workers) as pool:
+        rows = list(pool.map(one, sample))
+    return time.perf_counter() - t0, rows
 
 
-def cpu_baseline(cfg, cell_steps_per_unit: float, units: int = 1, material_map=None,
-                 what: str = "one spot"):
-    """Oracle throughput on a bounded sample, expressed in spots/s of the
-    workload: the oracle's cell-step rate (measured on full-domain energy
-    steps) divided by the cell-steps the moving-box march of the workload
-    takes (the reference's fastest CPU mode marches the same boxes)."""
-    rate, done, dt = oracle_cell_rate(cfg, material_map)
-    return {"value": units * rate / cell_steps_per_unit, "unit": "spots/s", "cores": os.cpu_count() or 1,
-            "kind": "port",
-            "sample": f"{done} full-domain energy steps in {dt:.1f} s -> {rate:.3e} cell-steps/s; "
-                      f"{what} = {cell_steps_per_unit:.4e} moving-box cell-steps"}
+def host_split(n_spots: int):
+    """(workers, OpenMP threads per worker) over this host's cores.  The
+    oracle's per-spot OpenMP loops scale to ~4.6x on 8 threads; several spots
+    at once on fewer threads each use the cores better (1.7x on 8 cores)."""
+    cores = os.cpu_count() or 1
+    workers = max(1, min(n_spots, cores // 2 if cores >= 4 else 1, 8))
+    return workers, max(1, cores // workers)
 
 
-def estimated_step_count(cfg) -> int:
-    """Energy steps of a full-domain march when the vacuum speed 1/sqrt(3) sets
-    the CFL bound (numerics/energy.py:539-660): dE = min(cfl*S_min*d/sqrt(3)*..., max)."""
-    from oracle.oracle import OracleProblem
-    orc = OracleProblem(cfg)
-    num, beam = cfg.numerics, cfg.beam
-    dx, dy, dz = cfg.geometry.spacing
-    E = beam.energy + num.energy_window_sigma * beam.energy_spread
-    n = 0
-    nm = len(orc.materials)
-    while E > num.energy_min:
-        S = min(orc.stopping_power(m, E) for m in range(nm))
-        inv = (1.0 / math.sqrt(3.0)) * (1.0 / (S * dx) + 1.0 / (S * dy) + 1.0 / (S * dz))
-        dE = min(num.cfl / inv, num.max_energy_step, E - num.energy_min)
-        E -= dE
-        n += 1
-    return n
-
-
-# Cell-steps of the moving-box march of each workload (per spot for single-spot
-# workloads, per field for fields): the work the reference's fastest CPU mode
-# (its moving active box) does.  Measured by this library's moving-box march of
-# the workload with the reference's box rule: slab80 in FP64 (the same boxes as
-# the reference, bit for bit), the fields in the FP32 form (boxes within 0.1 %
-# of the FP64 ones on slab80).
-MOVING_CELL_STEPS = {"slab80": 302_300_556.0, "field256": 3.2113e10, "pelvis1024": 1.1100e11}
+def cpu_baseline(workload_name: str, n: int = 2):
+    """Oracle throughput on a bounded sample of the workload: ``n`` complete
+    moving-box spots (the reference's fastest CPU mode), marched concurrently
+    over the host cores; spots/s = n / wall time."""
+    sample = reference_sample(workload_name, n)
+    workers, tpw = host_split(len(sample))
+    wall, rows = oracle_spots(sample, workers, tpw)
+    return {"value": len(sample) / wall, "unit": "spots/s", "cores": workers * tpw, "kind": "port",
+            "sample": f"{len(sample)} complete moving-box spot marches (energies "
+                      f"{[round(r[0], 1) for r in rows]} MeV, {[r[1] for r in rows]} energy steps) in "
+                      f"{wall:.1f} s, {workers} at a time x {tpw} OpenMP threads"}
 
 
 def run_reference(args, rank, world):
-    """The oracle (CPU restatement of the reference path) on the host cores."""
+    """The oracle (CPU restatement of the reference path) on the host cores:
+    every timed step marches one complete spot of the workload on the
+    reference's moving active box; the K spots run concurrently over the
+    cores (spot-level parallelism on top of the oracle's OpenMP loops)."""
     if rank != 0:
         return
-    from oracle.oracle import OracleProblem
-    threads = os.cpu_count() or 1
-    if args.workload in FIELDS:
-        cfg, mm, grid, beams, desc = field_workload(args.workload)
-        units = len(beams)
-        cfg = static_config(cfg, beams[gate_sample(beams, 1)[0]])
-    else:
-        (cfg, desc), mm, units = workload(args.workload), None, 1
-    cell_steps = MOVING_CELL_STEPS.get(args.workload)
-    orc = OracleProblem(static_config(cfg), mm)
-    n_cells = float(np.prod(orc.shape))
-    if cell_steps is None:   # no moving-box measurement: the full-domain march
-        cell_steps = units * n_cells * estimated_step_count(cfg)
-        basis = "full-domain march (estimated step count)"
-    else:
-        basis = "moving-box march (measured cell-steps)"
+    desc = FIELDS[args.workload]["desc"] if args.workload in FIELDS else workload(args.workload)[1]
+    sample = reference_sample(args.workload, args.steps)
+    workers, tpw = host_split(len(sample))
+    # warm-up: the first energy steps of one spot (the oracle has no JIT to warm)
+    from oracle.oracle import OracleProblem, set_threads
+    set_threads(workers * tpw)
+    warm = OracleProblem(sample[0][0], sample[0][1])
     for _ in range(args.warmup):
-        orc.march_steps(1)
-    rates = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        _, _, done = orc.march_steps(2)
-        rates.append(done * n_cells / (time.perf_counter() - t0))
-    rate = statistics.median(rates)
-    value = units * rate / cell_steps
+        warm.march_steps(2)
+    del warm
+    wall, rows = oracle_spots(sample, workers, tpw)
+    value = len(sample) / wall
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "spots/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": units / value * 1e3, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": wall / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "strong" if args.workload in FIELDS else "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded phantom, no dataset)",
         "config": {"workload": args.workload, "description": desc},
-        "cpu_baseline": {"value": value, "unit": "spots/s", "cores": threads, "kind": "port",
-                         "sample": f"2 full-domain energy steps per timed step ({rate:.3e} cell-steps/s), "
-                                   f"scaled to the {basis}: {cell_steps:.4e} cell-steps for {units} spot(s)"},
+        "cpu_baseline": {"value": value, "unit": "spots/s", "cores": workers * tpw, "kind": "port",
+                         "sample": f"{len(sample)} complete moving-box spot marches, one per timed step "
+                                   f"(energies {[round(r[0], 1) for r in rows]} MeV; "
+                                   f"{[r[1] for r in rows]} energy steps; "
+                                   f"{[round(r[2], 1) for r in rows]} s each), {workers} at a time x "
+                                   f"{tpw} OpenMP threads, {wall:.1f} s wall"},
         "e2e": {"value": value, "unit": "spots/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -488,67 +499,91 @@ def run_ours(args, cfg, desc, rank, world, local_rank):
         "clocks": clocks.summary(),
     }
     if not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(cfg, cell_steps / max(args.steps, 1))
+        line["cpu_baseline"] = cpu_baseline(args.workload, 1)
     print(json.dumps(line), flush=True)
 
 
+def field_batches(share, beams, k):
+    """This rank's spots, highest energy first, in ``k`` contiguous batches of
+    near-equal size: the batches of one step take similar numbers of energy
+    steps, and the ``k`` timed steps march every spot of the share once."""
+    order = sorted(share, key=lambda i: (-beams[i].energy, i))
+    n = len(order)
+    return [order[(q * n) // k:((q + 1) * n) // k] for q in range(k)]
+
+
 def run_field(args, rank, world, local_rank):
-    """A batched spot-scanning field: all spots in one batched march."""
+    """A spot-scanning field.  One step marches one batch of the field's
+    spots (1/K of them, by decreasing energy) as one batched field march; the
+    K timed steps together march the whole field once, so ``value`` is the
+    field's spots over the time of all K steps.  Over N ranks the spots are
+    shared out first (sharding.sharded_field_dose, longest-processing-time on
+    the moving-box cost model) and one all-reduce sums the FP64 field dose."""
     import torch
     import torch.distributed as dist
     from proton_dose_m1_b200 import metrics
+    from proton_dose_m1_b200.numerics.boundary import BeamInflow, transverse_profile
     from proton_dose_m1_b200.numerics.energy import FieldPlan, M1Plan, field_march
-    from proton_dose_m1_b200.numerics.boundary import BeamInflow
+    from proton_dose_m1_b200.sharding import assign_spots, sharded_field_dose, spot_cost
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    from proton_dose_m1_b200.sharding import assign_spots, spot_cost
-
     cfg, mm, grid, beams, desc = field_workload(args.workload)
     run_cfg = accelerated_config(cfg)
-    # strong scaling: the field's spots are shared out over the ranks
-    # (longest-processing-time on the moving-box cost model); each rank marches
-    # its share as one batched field and one all-reduce sums the FP64 dose
-    share = assign_spots([spot_cost(b, run_cfg, grid) for b in beams], world)[rank]
-    mine = [beams[k] for k in share]
+    costs = [spot_cost(b, run_cfg, grid) for b in beams]
+    n_spots = len(beams)
+    K = args.steps
     stream = torch.cuda.Stream(device=dev)
+    # inflow profiles of every spot: input data, computed once outside the timed region
+    profiles = [np.ascontiguousarray(b.n_protons * transverse_profile(b, grid)) for b in beams]
 
     def reduce_dose(d):
         if world > 1:
             dist.all_reduce(d)
 
-    with torch.cuda.stream(stream):
-        plan = FieldPlan(run_cfg, mm, grid, mine) if mine else None
+    def march_batches(share, batches, stats=None):
+        """Dose of ``share`` marched in ``batches`` steps (device)."""
         dose = torch.zeros(grid.shape, dtype=torch.float64, device=dev)
+        part = torch.empty_like(dose)
+        for batch in field_batches(share, beams, batches):
+            if not batch:
+                continue
+            plan = FieldPlan(run_cfg, mm, grid, [beams[i] for i in batch],
+                             profiles=[profiles[i] for i in batch])
+            steps = plan.march_device(part)
+            dose.add_(part)
+            if stats is not None:
+                info = plan.last_info
+                stats["stage_ms"] += info.stage_ms
+                stats["stage_launches"] += info.stage_launches
+                stats["launches"] += info.kernel_launches + 1   # + the dose sum
+                stats["cell_steps"] += info.cell_steps
+                stats["max_box"] = max(stats["max_box"], info.max_box_cells)
+                stats["waves"] += len(plan.waves)
+                stats["cap"] = max(stats["cap"], plan.cap)
+                stats["retries"] += plan.capacity_retries
+                stats["grow"] += info.box_grow_events
+                stats["fallbacks"] += info.box_fallbacks
+                stats["steps"] += list(steps)
+            plan.close()
+        return dose
 
-        def one_field():
-            if plan is not None:
-                out = plan.march_device(dose)
-            else:
-                dose.zero_()
-                out = []
-            reduce_dose(dose)
-            return out
-
-        for _ in range(args.warmup):
-            one_field()
+    stats = dict(stage_ms=0.0, stage_launches=0, launches=0, cell_steps=0.0, max_box=0.0, waves=0,
+                 cap=0, retries=0, grow=0, fallbacks=0, steps=[])
+    with torch.cuda.stream(stream):
+        # warm-up: the first W batches of this rank's share (the tile autotuner runs here)
+        mine = assign_spots(costs, world)[rank]
+        warm = [i for q in field_batches(mine, beams, K)[:args.warmup] for i in q]
+        if warm:
+            march_batches(warm, min(args.warmup, len(warm)))
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        stage_ms, stage_launches, launches, cell_steps, max_box = 0.0, 0, 0, 0.0, 0.0
         with ClockSampler(local_rank) as clocks:
             start.record(stream)
-            for _ in range(args.steps):
-                steps = one_field()
-                if plan is None:
-                    continue
-                info = plan.last_info
-                stage_ms += info.stage_ms
-                stage_launches += info.stage_launches
-                cell_steps += info.cell_steps
-                launches += info.kernel_launches
-                max_box = max(max_box, info.max_box_cells)
+            field_dose, share = sharded_field_dose(beams, costs, rank, world,
+                                                   lambda idx: march_batches(idx, K, stats), reduce_dose)
             end.record(stream)
             torch.cuda.synchronize()
         if world > 1:
@@ -558,32 +593,28 @@ def run_field(args, rank, world, local_rank):
             t = torch.tensor([ms], dtype=torch.float64, device=dev)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ms = float(t.item())
-        n_spots = len(beams)
-        value = n_spots * args.steps / (ms / 1e3)
-        workspace = plan.workspace_bytes if plan else 0
-        waves, cap = (len(plan.waves), plan.cap) if plan else (0, 0)
-        if plan:
-            plan.close()
+        value = n_spots / (ms / 1e3)
+        del field_dose
 
         gate = None
         plain_spots_per_s = None
-        if rank == 0:
+        if rank == 0 and args.gate_spots != 0:
             # gate: a sample of the field's spots, accelerated (batched) vs the
             # plain FP64 full-domain path one spot at a time
-            sample = gate_sample(beams, FIELDS[args.workload]["gate_beams"])
+            sample = gate_sample(beams, args.gate_spots if args.gate_spots > 0
+                                 else FIELDS[args.workload]["gate_beams"])
             sub = [beams[k] for k in sample]
             sp = FieldPlan(run_cfg, mm, grid, sub)
-            dose_acc = torch.empty_like(dose)
+            dose_acc = torch.empty(grid.shape, dtype=torch.float64, device=dev)
             sp.march_device(dose_acc)
             sp.close()
-            dose_plain = torch.zeros_like(dose)
-            d1 = torch.empty_like(dose)
+            dose_plain = torch.zeros_like(dose_acc)
+            d1 = torch.empty_like(dose_acc)
             U = torch.empty((4, *grid.shape), dtype=torch.float64, device=dev)
             energies = torch.empty(200_001, dtype=torch.float64, device=dev)
             plain_ms = 0.0
             for b in sub:
-                pc = static_config(cfg, b)
-                pplan = M1Plan(pc, mm, grid, BeamInflow.from_beam(b, grid))
+                pplan = M1Plan(static_config(cfg, b), mm, grid, BeamInflow.from_beam(b, grid))
                 U.zero_()
                 s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 s0.record(stream)
@@ -605,81 +636,97 @@ def run_field(args, rank, world, local_rank):
                                    and abs(score["maximum_dose_relative_difference"]) <= 0.005)}
             del dose_acc, dose_plain, d1
 
-    # end to end through the public API with host buffers: this rank's share
-    # through field_march, the sum over ranks, the field dose back on the host
+    # end to end through the public API with host buffers: field_march per
+    # batch (phantom, tables and profiles uploaded, the batch's dose copied
+    # back), the sum over batches and ranks on the host side
+    def march_batches_host(share):
+        dose_h = np.zeros(grid.shape)
+        for batch in field_batches(share, beams, K):
+            if batch:
+                d, _ = field_march(run_cfg, mm, grid, [beams[i] for i in batch])
+                dose_h += d
+        return torch.from_numpy(dose_h)
+
+    def reduce_host(d):
+        if world > 1:
+            dd = d.to(dev)
+            dist.all_reduce(dd)
+            d.copy_(dd.cpu())
+
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     t0 = time.perf_counter()
-    e2e_stats = {}
-    if mine:
-        dose_h, _ = field_march(run_cfg, mm, grid, mine, stats=e2e_stats)
-    else:
-        dose_h = np.zeros(grid.shape)
-    if world > 1:
-        dd = torch.as_tensor(dose_h, device=dev)
-        dist.all_reduce(dd)
-        dose_h = dd.cpu().numpy()
+    _, share_e2e = sharded_field_dose(beams, costs, rank, world, march_batches_host, reduce_host)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     if world > 1:
         t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    h2d = (mm.ids.nbytes + len(mine) * grid.shape[0] * grid.shape[1] * 8)
-    d2h = dose_h.nbytes
+    nxy = grid.shape[0] * grid.shape[1]
+    n_batches = sum(1 for q in field_batches(share_e2e, beams, K) if q)
+    h2d = n_batches * mm.ids.nbytes + len(share_e2e) * nxy * 8
+    d2h = n_batches * int(np.prod(grid.shape)) * 8
 
     if rank != 0:
         return
     peak, peak_kind = measured_peaks()
-    alg_total = cell_steps * ALG_BYTES_PER_CELL_STEP["FP32_FP64"]
+    precision = "FP32_FP64" if PRECISION == "fp32" else "FP64"
+    alg_total = stats["cell_steps"] * ALG_BYTES_PER_CELL_STEP[precision]
+    stage_ms = stats["stage_ms"]
     achieved = alg_total / (stage_ms / 1e3) / 1e9 if stage_ms > 0 else 0.0
-    traffic = stage_traffic(f"{args.workload}/accelerated", cell_steps, stage_launches)
+    traffic = stage_traffic(f"{args.workload}/accelerated", stats["cell_steps"], stats["stage_launches"])
+    steps = stats["steps"]
     line = {
         "metric": METRIC, "value": value, "unit": "spots/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "steps": K, "warmup": args.warmup, "ms_per_step": ms / K,
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "f32 stencil / f64 dose" if PRECISION == "fp32" else "f64",
         "data": "synthetic (seeded phantom and spots, no dataset)",
         "config": {"workload": args.workload, "description": desc,
                    "method": "batched field, " + accelerated_label(),
-                   "spots": n_spots, "spots_rank0": len(mine), "waves": waves, "box_capacity_cells": cap,
+                   "step": f"one batch of ~{n_spots // max(world, 1) // K} spots (by decreasing energy) "
+                           f"per rank; the {K} timed steps march all {n_spots} spots once",
+                   "spots": n_spots, "spots_rank0": len(share),
+                   "waves": stats["waves"], "box_capacity_cells": stats["cap"],
+                   "capacity_retries": stats["retries"],
+                   "box_grow_events": stats["grow"], "box_fallbacks": stats["fallbacks"],
                    "parallelism": f"spot sharding over {world} GPU(s), one FP64 dose all-reduce",
-                   "workspace_bytes": workspace, "max_box_cells": max_box,
+                   "max_box_cells": stats["max_box"],
                    "energy_steps_max": max(steps, default=0), "energy_steps_min": min(steps, default=0),
-                   "cells_marched_per_field": cell_steps / max(args.steps, 1),
+                   "cells_marched_per_field": stats["cell_steps"],
                    "plain_fp64_spots_per_s": plain_spots_per_s,
+                   "in_timed_region": "per batch: plan set-up from pooled buffers (phantom ids and inflow "
+                                      "profiles uploaded), the batched march, the batch dose summed on device",
                    "l2": "per-spot state buffers (GBs) exceed the 126 MB L2"},
         "gate": gate,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "kernel": f"stage_kernel<{'float' if PRECISION == 'fp32' else 'double'}> (A/B/C), "
-                               "all spots per launch",
-                     "avg_launch_ms": stage_ms / max(stage_launches, 1),
-                     "algorithmic_bytes_per_launch": alg_total / max(stage_launches, 1),
-                     "algorithmic_bytes_per_cell_step": ALG_BYTES_PER_CELL_STEP["FP32_FP64"],
+                               "all spots of a batch per launch",
+                     "avg_launch_ms": stage_ms / max(stats["stage_launches"], 1),
+                     "algorithmic_bytes_per_launch": alg_total / max(stats["stage_launches"], 1),
+                     "algorithmic_bytes_per_cell_step": ALG_BYTES_PER_CELL_STEP[precision],
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                     "compute": compute_roofline(cell_steps, stage_ms,
-                                                 "FP32_FP64" if PRECISION == "fp32" else "FP64")},
-        "e2e": {"value": n_spots / e2e_s, "unit": "spots/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h), "rank0_breakdown": e2e_stats},
-        "gpu_launches": launches,
+                     "compute": compute_roofline(stats["cell_steps"], stage_ms, precision)},
+        "e2e": {"value": n_spots / e2e_s, "unit": "spots/s", "h2d_bytes_per_step": int(h2d / K),
+                "d2h_bytes_per_step": int(d2h / K)},
+        "gpu_launches": stats["launches"],
         "clocks": clocks.summary(),
     }
     if not args.no_cpu_baseline:
-        mid = beams[gate_sample(beams, 1)[0]]
-        line["cpu_baseline"] = cpu_baseline(static_config(cfg, mid), cell_steps / max(args.steps, 1),
-                                            units=n_spots, material_map=mm, what=f"the {n_spots}-spot field")
+        line["cpu_baseline"] = cpu_baseline(args.workload, 2)
     print(json.dumps(line), flush=True)
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=16)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--workload", default="slab80")
+    ap.add_argument("--workload", default="pelvis1024")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--method", choices=("accelerated", "plain"), default="accelerated",
                     help="accelerated: moving box + FP32 stencil/FP64 dose; plain: FP64 full domain")
@@ -689,6 +736,8 @@ def main():
                     help="moving box of the accelerated form")
     ap.add_argument("--precision", choices=("fp32", "fp64"), default=None,
                     help="stencil arithmetic of the accelerated form (default: fp32; fields: their own)")
+    ap.add_argument("--gate-spots", type=int, default=-1,
+                    help="field workloads: spots of the accuracy gate (-1: the workload's own, 0: no gate)")
     ap.add_argument("--profile-spots", type=int, default=0,
                     help="field workloads: march K spots of the field once (for ncu captures) and exit")
     args = ap.parse_args()

@@ -81,6 +81,9 @@ PDM1_HD double dd_exp(double x) {
 // ---------------------------------------------------------------------------
 template <typename T>
 PDM1_HD T weno_left(T v0, T v1, T v2, T v3, T v4) {
+    // r * r below overflows single precision above r ~ 1.8e19 (reached for
+    // fluences of ~1e6 protons); single precision uses weno_left_f32
+    static_assert(sizeof(T) == sizeof(double), "weno_left is the FP64 path; use weno_left_f32");
     const T c3 = T(3), c6 = T(6);
     T p0 = v0 / c3 - T(7) * v1 / c6 + T(11) * v2 / c6;
     T p1 = -v1 / c6 + T(5) * v2 / c6 + v3 / c3;
@@ -120,8 +123,9 @@ PDM1_HD float fast_div(float a, float b) {
 
 // Single-precision WENO-Z5 with the arithmetic regrouped for fewer
 // instructions: the candidate polynomials as integer combinations times 1/6,
-// the 1/6 folded into the one reciprocal of the weight sum.  Same weights and
-// overflow guard as weno_left<float>.
+// the 1/6 folded into the one reciprocal of the weight sum.  Same weights as
+// weno_left; the ratios tau5 / (beta + eps) are held at 1e30 and the alphas
+// rescaled by the largest ratio, so that nothing overflows single precision.
 PDM1_HD float weno_left_f32(float v0, float v1, float v2, float v3, float v4) {
     const float q0 = 2.0f * v0 - 7.0f * v1 + 11.0f * v2;   // 6 p0
     const float q1 = -v1 + 5.0f * v2 + 2.0f * v3;          // 6 p1
@@ -156,6 +160,66 @@ PDM1_HD float weno_left_f32(float v0, float v1, float v2, float v3, float v4) {
     const float inv = fast_div(1.0f, 6.0f * (al0 + al1 + al2));
     return (al0 * inv) * q0 + (al1 * inv) * q1 + (al2 * inv) * q2;
 }
+
+#if defined(__CUDACC__)
+// ---------------------------------------------------------------------------
+// WENO-Z5 of two components at once on sm_100's packed single-precision
+// pipe (fma/mul/add.rn.f32x2: one instruction for both lanes).  Lane x and
+// lane y are two state components of the same cells, so the five inputs are
+// five 64-bit shared-memory loads.  The arithmetic per lane is that of
+// weno_left_f32: the candidate polynomials as integer combinations times 1/6,
+// the Jiang-Shu indicators, r = tau5 / (beta + eps) held at 1e30, and, where
+// r^2 could overflow (r > 1e15), every alpha rescaled by 1 / max r^2; the
+// weights are normalised before they multiply the polynomials.  Quotients
+// and the comparisons stay per lane (no packed reciprocal or min/max).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 pk(float s) { return make_float2(s, s); }
+__device__ __forceinline__ float2 pk_fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 pk_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 pk_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+// approximate reciprocal per lane (MUFU), within 2 ulp for |x| below 2^126
+__device__ __forceinline__ float2 pk_rcp(float2 x) { return make_float2(__fdividef(1.0f, x.x), __fdividef(1.0f, x.y)); }
+__device__ __forceinline__ float2 pk_sqrt(float2 x) { return make_float2(sqrtf(x.x), sqrtf(x.y)); }
+
+// Jiang-Shu smoothness indicator 13/12 a^2 + 1/4 b^2
+__device__ __forceinline__ float2 pk_beta(float2 a, float2 b) {
+    return pk_fma(pk_mul(pk(float(13.0 / 12.0)), a), a, pk_mul(pk_mul(pk(0.25f), b), b));
+}
+
+__device__ __forceinline__ float2 weno_left_f32x2(float2 v0, float2 v1, float2 v2, float2 v3, float2 v4) {
+    const float2 q0 = pk_fma(pk(2.0f), v0, pk_fma(pk(-7.0f), v1, pk_mul(pk(11.0f), v2)));   // 6 p0
+    const float2 q1 = pk_fma(pk(-1.0f), v1, pk_fma(pk(5.0f), v2, pk_mul(pk(2.0f), v3)));    // 6 p1
+    const float2 q2 = pk_fma(pk(-1.0f), v4, pk_fma(pk(2.0f), v2, pk_mul(pk(5.0f), v3)));    // 6 p2
+    const float2 beta0 = pk_beta(pk_add(pk_fma(pk(-2.0f), v1, v0), v2),
+                                 pk_fma(pk(3.0f), v2, pk_fma(pk(-4.0f), v1, v0)));
+    const float2 beta1 = pk_beta(pk_add(pk_fma(pk(-2.0f), v2, v1), v3), pk_fma(pk(-1.0f), v3, v1));
+    const float2 beta2 = pk_beta(pk_add(pk_fma(pk(-2.0f), v3, v2), v4),
+                                 pk_fma(pk(-4.0f), v3, pk_fma(pk(3.0f), v2, v4)));
+    const float2 d = pk_fma(pk(-1.0f), beta0, beta2);
+    const float2 tau5 = make_float2(fabsf(d.x), fabsf(d.y));
+    const float2 eps = pk(float(kWenoEps));
+    float2 r0 = pk_mul(tau5, pk_rcp(pk_add(beta0, eps)));
+    float2 r1 = pk_mul(tau5, pk_rcp(pk_add(beta1, eps)));
+    float2 r2 = pk_mul(tau5, pk_rcp(pk_add(beta2, eps)));
+    r0 = make_float2(fminf(r0.x, 1e30f), fminf(r0.y, 1e30f));
+    r1 = make_float2(fminf(r1.x, 1e30f), fminf(r1.y, 1e30f));
+    r2 = make_float2(fminf(r2.x, 1e30f), fminf(r2.y, 1e30f));
+    // alpha_k / s^2 = d_k (s^-2 + (r_k / s)^2) with s = max r where r^2 could overflow, else s = 1
+    float2 sc = pk(1.0f);
+    const float mx = fmaxf(r0.x, fmaxf(r1.x, r2.x)), my = fmaxf(r0.y, fmaxf(r1.y, r2.y));
+    if (mx > 1e15f || my > 1e15f) {
+        if (mx > 1e15f) sc.x = __fdividef(1.0f, mx);
+        if (my > 1e15f) sc.y = __fdividef(1.0f, my);
+    }
+    const float2 e = pk_mul(sc, sc);
+    const float2 t0 = pk_mul(r0, sc), t1 = pk_mul(r1, sc), t2 = pk_mul(r2, sc);
+    const float2 al0 = pk_mul(pk(0.1f), pk_fma(t0, t0, e));
+    const float2 al1 = pk_mul(pk(0.6f), pk_fma(t1, t1, e));
+    const float2 al2 = pk_mul(pk(0.3f), pk_fma(t2, t2, e));
+    const float2 inv = pk_rcp(pk_mul(pk(6.0f), pk_add(pk_add(al0, al1), al2)));
+    return pk_fma(pk_mul(al2, inv), q2, pk_fma(pk_mul(al1, inv), q1, pk_mul(pk_mul(al0, inv), q0)));
+}
+#endif
 
 // ---------------------------------------------------------------------------
 // WENO3-Z left reconstruction (p = 2), reconstruction_methods/weno3.py:15-62
@@ -438,6 +502,88 @@ PDM1_HD void face_flux_f32(const float L[4], const float R[4], int axis, bool un
 #pragma unroll
     for (int c = 0; c < 4; ++c) F[c] = (sr * FL[c] - sl * FR[c] + sp * dl[c]) * inv;
 }
+
+#if defined(__CUDACC__)
+// ---------------------------------------------------------------------------
+// The single-precision face flux with the two sides of the face in the two
+// lanes of sm_100's packed f32x2 arithmetic (x = left state, y = right
+// state).  Per lane the arithmetic is that of side_f32 / speeds_f32 /
+// side_flux_f32 above: realizability projection, closure through
+// iso = (1 - f)(1 + f) / (r + 1) and dir = 2 - r with r = sqrt(1 + 3(1 - f^2)),
+// the exact wave speeds from iso and dir, the physical flux.  Square roots,
+// reciprocals, comparisons and the HLL combination (which mixes the lanes)
+// are per lane.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void face_flux_f32x2(const float L[4], const float R[4], int axis, bool unit_speeds,
+                                                float F[4]) {
+    const float2 one = pk(1.0f);
+    float2 phi = make_float2(L[0] < 0.0f ? 0.0f : L[0], R[0] < 0.0f ? 0.0f : R[0]);
+    float2 jx = make_float2(L[1], R[1]), jy = make_float2(L[2], R[2]), jz = make_float2(L[3], R[3]);
+    float2 jn = pk_sqrt(pk_fma(jx, jx, pk_fma(jy, jy, pk_mul(jz, jz))));
+    const float2 jmax = pk_mul(pk(float(1.0 - kRealEps)), phi);
+    if (jn.x > jmax.x || jn.y > jmax.y) {   // realizability projection onto |J| = jmax
+        float2 sc = one;
+        if (jn.x > jmax.x) { sc.x = fast_div(jmax.x, jn.x); jn.x = jmax.x; }
+        if (jn.y > jmax.y) { sc.y = fast_div(jmax.y, jn.y); jn.y = jmax.y; }
+        jx = pk_mul(jx, sc); jy = pk_mul(jy, sc); jz = pk_mul(jz, sc);
+    }
+    // closure: f = |J| / phi (0 without fluence)
+    float2 f = pk_mul(jn, pk_rcp(phi));
+    f = make_float2(phi.x > 0.0f ? fminf(f.x, 1.0f) : 0.0f, phi.y > 0.0f ? fminf(f.y, 1.0f) : 0.0f);
+    const float2 q = pk_mul(pk_fma(pk(-1.0f), f, one), pk_add(f, one));
+    const float2 r = pk_sqrt(pk_fma(pk(3.0f), q, one));
+    float2 iso = pk_mul(q, pk_rcp(pk_add(r, one)));
+    float2 dir = pk_fma(pk(-1.0f), r, pk(2.0f));
+    const float2 rjn = make_float2(jn.x > 0.0f ? __fdividef(1.0f, jn.x) : 0.0f,
+                                   jn.y > 0.0f ? __fdividef(1.0f, jn.y) : 0.0f);
+    const float2 nx = pk_mul(jx, rjn), ny = pk_mul(jy, rjn), nz = pk_mul(jz, rjn);
+    const float2 na = axis == 0 ? nx : (axis == 1 ? ny : nz);
+    const float2 ja = axis == 0 ? jx : (axis == 1 ? jy : jz);
+    // physical fluxes of both sides
+    const float2 pdn = pk_mul(pk_mul(phi, dir), na);
+    const float2 pi = pk_mul(phi, iso);   // the isotropic pressure on the normal component
+    float2 Fc[4];
+    Fc[0] = ja;
+    Fc[1] = axis == 0 ? pk_fma(pdn, nx, pi) : pk_mul(pdn, nx);
+    Fc[2] = axis == 1 ? pk_fma(pdn, ny, pi) : pk_mul(pdn, ny);
+    Fc[3] = axis == 2 ? pk_fma(pdn, nz, pi) : pk_mul(pdn, nz);
+    float sl = -1.0f, sr = 1.0f;
+    if (!unit_speeds) {
+        // exact wave speeds; below the eigenvalue floor of phi the closure is
+        // taken at phi = 1e-10 (wave_speeds.py:36-103), |J| below it: +-1/sqrt(3)
+        if (phi.x < float(kEigEps) || phi.y < float(kEigEps)) {
+            if (phi.x < float(kEigEps)) closure_f32(float(kEigEps), jn.x, f.x, iso.x, dir.x);
+            if (phi.y < float(kEigEps)) closure_f32(float(kEigEps), jn.y, f.y, iso.y, dir.y);
+        }
+        f = make_float2(fminf(f.x, float(1.0 - kEigEps)), fminf(f.y, float(1.0 - kEigEps)));
+        const float2 den = pk_fma(pk(6.0f), iso, pk(2.0f));
+        const float2 mu2 = pk_mul(na, na), fm = pk_mul(f, na);
+        const float2 t = pk_fma(pk_mul(pk(2.0f), dir), mu2, pk_mul(pk(-4.0f), iso));
+        float2 disc = pk_fma(pk_mul(pk(-1.0f), den), t, pk_mul(pk_mul(pk(4.0f), fm), fm));
+        disc = make_float2(fmaxf(disc.x, 0.0f), fmaxf(disc.y, 0.0f));
+        const float2 root = pk_sqrt(disc), rden = pk_rcp(den), c = pk_mul(pk(2.0f), fm);
+        float2 lmin = pk_mul(pk_fma(pk(-1.0f), root, c), rden);
+        float2 lmax = pk_mul(pk_add(c, root), rden);
+        const float iso3 = 0.57735026918962576f;   // 1/sqrt(3)
+        if (jn.x < float(kEigEps)) { lmin.x = -iso3; lmax.x = iso3; }
+        if (jn.y < float(kEigEps)) { lmin.y = -iso3; lmax.y = iso3; }
+        sl = fminf(fminf(lmin.x, lmin.y), 0.0f);
+        sr = fmaxf(fmaxf(lmax.x, lmax.y), 0.0f);
+    }
+    const float den = sr - sl;
+    if (!(den > 0.0f)) {
+        // |J|/phi rounds to 1 for an exactly directed state: both speeds normal
+        // to J are 0 and the fan collapses; the HLL flux tends to the central flux
+#pragma unroll
+        for (int c = 0; c < 4; ++c) F[c] = 0.5f * (Fc[c].x + Fc[c].y);
+        return;
+    }
+    const float inv = fast_div(1.0f, den), sp = sl * sr;
+    const float dl[4] = {phi.y - phi.x, jx.y - jx.x, jy.y - jy.x, jz.y - jz.x};
+#pragma unroll
+    for (int c = 0; c < 4; ++c) F[c] = (sr * Fc[c].x - sl * Fc[c].y + sp * dl[c]) * inv;
+}
+#endif
 
 // ---------------------------------------------------------------------------
 // Coefficient tables (physics/stopping_power.py, coefficient_interpolation.py,

@@ -8,6 +8,15 @@
 
 namespace pdm1 {
 
+// Element e of component c's copy of an arm of asz elements.  Double arms are
+// [c][e]; float arms hold the components in pairs, [c / 2][e][c % 2], so a
+// 64-bit load brings two components of a cell into the packed f32x2 lanes.
+template <typename T>
+__device__ __forceinline__ T &arm_at(T *arm, int asz, int c, int e) {
+    if constexpr (sizeof(T) == sizeof(float)) return arm[((c >> 1) * asz + e) * 2 + (c & 1)];
+    else return arm[c * asz + e];
+}
+
 // LEARN (stage C of a plan with a learned box): the tile's fluence moments of
 // the new state are accumulated for the next step's proposer.
 template <typename T, int MODE, class Tl, bool LEARN = false>
@@ -21,7 +30,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 4) stage
     T *smem = reinterpret_cast<T *>(smem_raw);
     __shared__ double slab_buf[NT];   // moving box: phi of the tile's cells
     SmemT<T> s;
-    s.X = smem;            // [c][i + 3][j][k]
+    s.X = smem;            // [c][i + 3][j][k]  (float: [c / 2][i + 3][j][k][c % 2], arm_at)
     s.Y = s.X + 4 * AX;    // [c][i][j + 3][k]
     s.Z = s.Y + 4 * AY;    // [c][i][j][k + 3]
     s.F = s.Z + 4 * AZ;
@@ -57,13 +66,16 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 4) stage
             double u[4];
             load_cell<MODE>(cf, co, d, src, i0 + ii - 3, j0 + j, k0 + k, u);
             const bool core = ii >= 3 && ii < TX + 3;
+            const int ex = (ii * TY + j) * TZ + k;
+            const int ey = ((ii - 3) * (TY + 6) + j + 3) * TZ + k;
+            const int ez = ((ii - 3) * TY + j) * (TZ + 6) + k + 3;
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
                 const T v = T(u[c]);
-                s.X[((c * (TX + 6) + ii) * TY + j) * TZ + k] = v;
+                arm_at(s.X, AX, c, ex) = v;
                 if (core) {
-                    s.Y[((c * TX + ii - 3) * (TY + 6) + j + 3) * TZ + k] = v;
-                    s.Z[((c * TX + ii - 3) * TY + j) * (TZ + 6) + k + 3] = v;
+                    arm_at(s.Y, AY, c, ey) = v;
+                    arm_at(s.Z, AZ, c, ez) = v;
                 }
             }
         }
@@ -74,7 +86,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 4) stage
             double u[4];
             load_cell<MODE>(cf, co, d, src, i0 + i, gj, k0 + k, u);
 #pragma unroll
-            for (int c = 0; c < 4; ++c) s.Y[((c * TX + i) * (TY + 6) + aj) * TZ + k] = T(u[c]);
+            for (int c = 0; c < 4; ++c) arm_at(s.Y, AY, c, (i * (TY + 6) + aj) * TZ + k) = T(u[c]);
         }
         for (int e = tid; e < SZ; e += NT) {
             int kk = e % 6, j = (e / 6) % TY, i = e / (6 * TY);
@@ -84,7 +96,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 4) stage
             double u[4];
             load_cell<MODE>(cf, co, d, src, i0 + i, j0 + j, gk, u);
 #pragma unroll
-            for (int c = 0; c < 4; ++c) s.Z[((c * TX + i) * TY + j) * (TZ + 6) + ak] = T(u[c]);
+            for (int c = 0; c < 4; ++c) arm_at(s.Z, AZ, c, (i * TY + j) * (TZ + 6) + ak) = T(u[c]);
         }
         __syncthreads();
         // ---- 2. z-min ghost cells: quartic extrapolation through the inflow ----
@@ -94,17 +106,18 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 4) stage
                 int li = i0 + i, lj = j0 + j;
                 if (li >= nx || lj >= ny) continue;
                 T ui = T(boundary_value<MODE>(a, cf, bm, co, d, c, li, lj));
-                T *z = &s.Z[((c * TX + i) * TY + j) * (TZ + 6)];
-                T u0 = z[3], u1 = z[4], u2 = z[5], u3 = z[6];
+                const int ez = (i * TY + j) * (TZ + 6);
+                auto z = [&](int kk) -> T & { return arm_at(s.Z, AZ, c, ez + kk); };
+                T u0 = z(3), u1 = z(4), u2 = z(5), u3 = z(6);
                 if (cf.spatial == PDM1_SPATIAL_WENO_Z) {   // quartic, boundary.py:247-320
-                    z[2] = T(5.0) * ui - T(77.0 / 12.0) * u0 + T(43.0 / 12.0) * u1 - T(17.0 / 12.0) * u2 + T(0.25) * u3;
-                    z[1] = T(25.0) * ui - T(505.0 / 12.0) * u0 + T(335.0 / 12.0) * u1 - T(145.0 / 12.0) * u2 + T(9.0 / 4.0) * u3;
-                    z[0] = T(75.0) * ui - T(545.0 / 4.0) * u0 + T(395.0 / 4.0) * u1 - T(181.0 / 4.0) * u2 + T(35.0 / 4.0) * u3;
+                    z(2) = T(5.0) * ui - T(77.0 / 12.0) * u0 + T(43.0 / 12.0) * u1 - T(17.0 / 12.0) * u2 + T(0.25) * u3;
+                    z(1) = T(25.0) * ui - T(505.0 / 12.0) * u0 + T(335.0 / 12.0) * u1 - T(145.0 / 12.0) * u2 + T(9.0 / 4.0) * u3;
+                    z(0) = T(75.0) * ui - T(545.0 / 4.0) * u0 + T(395.0 / 4.0) * u1 - T(181.0 / 4.0) * u2 + T(35.0 / 4.0) * u3;
                 } else if (cf.spatial == PDM1_SPATIAL_FIRST_ORDER) {   // boundary.py:205-212
-                    z[2] = ui;
+                    z(2) = ui;
                 } else {   // MUSCL / WENO3: quadratic, boundary.py:214-245
-                    z[2] = T(3.0) * ui - T(2.5) * u0 + T(0.5) * u1;
-                    z[1] = T(9.0) * ui - T(10.5) * u0 + T(2.5) * u1;
+                    z(2) = T(3.0) * ui - T(2.5) * u0 + T(0.5) * u1;
+                    z(1) = T(9.0) * ui - T(10.5) * u0 + T(2.5) * u1;
                 }
             }
             __syncthreads();
@@ -124,25 +137,36 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 4) stage
             T L[4], R[4];
             // the six cells along the axis, i - 3 .. i + 2 (face between i - 1 and i),
             // are arm indices i .. i + 5
-            const T *base;
-            int stride, cs;
+            T *arm;
+            int e0, stride, cs;
             if (axis == 0) {
-                base = s.X + (i * TY + j) * TZ + k; stride = TY * TZ; cs = AX;
+                arm = s.X; e0 = (i * TY + j) * TZ + k; stride = TY * TZ; cs = AX;
             } else if (axis == 1) {
-                base = s.Y + (i * (TY + 6) + j) * TZ + k; stride = TZ; cs = AY;
+                arm = s.Y; e0 = (i * (TY + 6) + j) * TZ + k; stride = TZ; cs = AY;
             } else {
-                base = s.Z + (i * TY + j) * (TZ + 6) + k; stride = 1; cs = AZ;
+                arm = s.Z; e0 = (i * TY + j) * (TZ + 6) + k; stride = 1; cs = AZ;
             }
             if (cf.spatial == PDM1_SPATIAL_WENO_Z) {
+                if constexpr (sizeof(T) == sizeof(float)) {
+                    // two components per packed reconstruction, L and R from the same loads
+                    const float2 *b2 = reinterpret_cast<const float2 *>(arm) + e0;
 #pragma unroll
-                for (int c = 0; c < 4; ++c) {
-                    T w[6];
+                    for (int pc = 0; pc < 2; ++pc) {
+                        float2 w[6];
 #pragma unroll
-                    for (int q = 0; q < 6; ++q) w[q] = base[c * cs + q * stride];
-                    if constexpr (sizeof(T) == sizeof(float)) {
-                        L[c] = weno_left_f32(w[0], w[1], w[2], w[3], w[4]);
-                        R[c] = weno_left_f32(w[5], w[4], w[3], w[2], w[1]);
-                    } else {
+                        for (int q = 0; q < 6; ++q) w[q] = b2[pc * cs + q * stride];
+                        const float2 l = weno_left_f32x2(w[0], w[1], w[2], w[3], w[4]);
+                        const float2 r = weno_left_f32x2(w[5], w[4], w[3], w[2], w[1]);
+                        L[2 * pc] = l.x; L[2 * pc + 1] = l.y;
+                        R[2 * pc] = r.x; R[2 * pc + 1] = r.y;
+                    }
+                } else {
+                    const T *base = arm + e0;
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        T w[6];
+#pragma unroll
+                        for (int q = 0; q < 6; ++q) w[q] = base[c * cs + q * stride];
                         L[c] = weno_left(w[0], w[1], w[2], w[3], w[4]);
                         R[c] = weno_left(w[5], w[4], w[3], w[2], w[1]);
                     }
@@ -150,8 +174,8 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 4) stage
             } else {
                 // the narrower stencils read cells i-2 .. i+1 (arm indices i+1 .. i+4)
                 for (int c = 0; c < 4; ++c) {
-                    const T *p = base + c * cs;
-                    const T wm = p[stride], w0 = p[2 * stride], w1 = p[3 * stride], wp = p[4 * stride];
+                    const T wm = arm_at(arm, cs, c, e0 + stride), w0 = arm_at(arm, cs, c, e0 + 2 * stride);
+                    const T w1 = arm_at(arm, cs, c, e0 + 3 * stride), wp = arm_at(arm, cs, c, e0 + 4 * stride);
                     if (cf.spatial == PDM1_SPATIAL_FIRST_ORDER) {   // first_order.py:66-111
                         L[c] = w0;
                         R[c] = w1;
@@ -169,7 +193,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 4) stage
             }
             T F[4];
             if constexpr (sizeof(T) == sizeof(float)) {
-                face_flux_f32(L, R, axis, unit, F);
+                face_flux_f32x2(L, R, axis, unit, F);
             } else {
                 project(L[0], L[1], L[2], L[3]);
                 project(R[0], R[1], R[2], R[3]);

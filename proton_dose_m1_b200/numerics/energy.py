@@ -337,6 +337,9 @@ class FieldPlan:
     dose is the sum of the beams' doses.  ``config`` gives the phantom,
     physics, numerics and precision; ``beams`` are ``Beam`` objects.
 
+    ``profiles`` (optional) are the beams' inflow profiles, n_protons times
+    ``transverse_profile`` (nx, ny), when the caller already holds them.
+
     Each beam's box buffers hold ``box_capacity_cells`` (0: the largest
     ``estimate_box_cells`` over the beams).  When all beams do not fit in
     ``max_workspace_bytes`` (0: 70% of the free device memory), the beams run
@@ -345,7 +348,7 @@ class FieldPlan:
     """
 
     def __init__(self, config, material_map, grid, beams, box_capacity_cells: int = 0,
-                 max_workspace_bytes: int = 0):
+                 max_workspace_bytes: int = 0, profiles=None):
         from dataclasses import replace
         from .boundary import transverse_profile
         num = config.numerics
@@ -367,8 +370,11 @@ class FieldPlan:
         self.n_beams = len(beams)
         self.auto_capacity = not box_capacity_cells
         self.capacity_retries = 0
-        self.profiles = [np.ascontiguousarray(b.n_protons * transverse_profile(b, grid), dtype=np.float64)
-                         for b in beams]
+        if profiles is None:
+            profiles = [b.n_protons * transverse_profile(b, grid) for b in beams]
+        elif len(profiles) != len(beams):
+            raise ValueError("one inflow profile per beam is needed")
+        self.profiles = [np.ascontiguousarray(q, dtype=np.float64) for q in profiles]
         self._budget = max_workspace_bytes
         self._plans = {}
         self._layout(int(box_capacity_cells or max(estimate_box_cells(config, grid, b) for b in beams)))
