@@ -33,7 +33,8 @@ enum pdm1_status {
     PDM1_ERR_MAX_STEPS = 4,     /* the energies buffer is shorter than the march */
     PDM1_ERR_NO_BEAM = 5,       /* the inflow profile is empty (ValueError) */
     PDM1_ERR_UNSUPPORTED = 6,   /* option without a GPU kernel (NotImplementedError) */
-    PDM1_ERR_NONFINITE = 7      /* a non-finite energy step was produced */
+    PDM1_ERR_NONFINITE = 7,     /* a non-finite energy step was produced */
+    PDM1_ERR_TIMEOUT = 8        /* a bounded wait inside a kernel ran out */
 };
 
 enum { PDM1_SCATTERING_OFF = 0, PDM1_SCATTERING_ROSSI = 1, PDM1_SCATTERING_WENTZEL = 2 };
@@ -218,6 +219,13 @@ int pdm1_gamma(const double *dose_ref, const double *dose_eval, int nx, int ny, 
                double distance_mm, double lower_cutoff_percent, int interp_fraction,
                double max_gamma, double global_normalisation, double *gamma_out,
                double *pass_rate_out, pdm1_stream_t stream);
+
+/* Staging of the FP32 form's stages B and C (no counterpart in the reference;
+ * the reference has no GPU tiles): bulk = 1 (the default) copies each z row of
+ * the tile and its halo with cp.async.bulk onto a shared-memory mbarrier,
+ * bulk = 0 loads cell by cell.  Both fill shared memory with the same values,
+ * so the march is the same bit for bit.  No effect on FP64 plans. */
+int pdm1_plan_set_staging(pdm1_plan *plan, int bulk);
 
 /* ---- Tile shape of the stage kernels ---------------------------------------
  * No reference counterpart.  The fused stage kernels are built for

@@ -13,7 +13,7 @@ from pathlib import Path
 LIB_PATH = Path(__file__).resolve().parent / "libpdm1.so"
 
 PDM1_OK = 0
-ERR_ARGUMENT, ERR_RANGE, ERR_CUDA, ERR_MAX_STEPS, ERR_NO_BEAM, ERR_UNSUPPORTED, ERR_NONFINITE = range(1, 8)
+ERR_ARGUMENT, ERR_RANGE, ERR_CUDA, ERR_MAX_STEPS, ERR_NO_BEAM, ERR_UNSUPPORTED, ERR_NONFINITE, ERR_TIMEOUT = range(1, 9)
 
 _dp = C.POINTER(C.c_double)
 _vp = C.c_void_p
@@ -91,6 +91,7 @@ def lib():
         L.pdm1_pool_cached_bytes.restype = C.c_size_t
         L.pdm1_pool_release.argtypes = []
         L.pdm1_pool_release.restype = C.c_int
+        L.pdm1_plan_set_staging.argtypes = [_vp, C.c_int]
         L.pdm1_march.argtypes = [_vp, _vp, _vp, _vp, C.c_int, _dp, C.c_int, _vp, _dp,
                                  C.POINTER(MarchInfo), _vp]
         L.pdm1_field_plan_create.argtypes = [C.POINTER(Problem), C.POINTER(BeamDesc), C.c_int,
@@ -146,6 +147,6 @@ EXPORTED_SYMBOLS = (
     "pdm1_march_noalloc", "pdm1_plan_set_box_model", "pdm1_plan_set_recorder", "pdm1_mlp_train",
     "pdm1_mlp_gradients", "pdm1_mlp_forward", "pdm1_box_model_infer",
     "pdm1_tile_shape", "pdm1_plan_set_tile", "pdm1_plan_autotune", "pdm1_analytical_csda_dose",
-    "pdm1_pool_cached_bytes", "pdm1_pool_release",
+    "pdm1_pool_cached_bytes", "pdm1_pool_release", "pdm1_plan_set_staging",
 )
 NUM_TILES = 3

@@ -33,7 +33,7 @@ struct BoxModelDev {
 
 int pack_box_model(const pdm1_box_model *m, BoxModelDev &out);
 
-enum { ERR_DEV_RANGE = 1, ERR_DEV_MAXSTEPS = 2, ERR_DEV_NONFINITE = 4, ERR_DEV_CAPACITY = 8 };
+enum { ERR_DEV_RANGE = 1, ERR_DEV_MAXSTEPS = 2, ERR_DEV_NONFINITE = 4, ERR_DEV_CAPACITY = 8, ERR_DEV_TIMEOUT = 16 };
 // ---------------------------------------------------------------------------
 // Device-side plan data
 // ---------------------------------------------------------------------------
@@ -105,6 +105,7 @@ struct ConfigDev {
     TileDims tile;              // tile shape of the stage kernels (kTiles[tile_id])
     int tile_id;
     int fp32;                   // FP32-stencil form: float eigenvalues in the CFL bound (not with cfl_floor)
+    int bulk_stage;             // FP32 form: stages B and C stage their float4 source by bulk copies
     // learned moving box and training-data recorder
     int learned;                // a box model proposes the margins
     const BoxModelDev *model;

@@ -1004,6 +1004,7 @@ int device_error_status(int error) {
     if (error & ERR_DEV_MAXSTEPS) return set_error(PDM1_ERR_MAX_STEPS, "energies buffer shorter than the march");
     if (error & ERR_DEV_NONFINITE) return set_error(PDM1_ERR_NONFINITE, "non-finite state or non-positive energy step during the march");
     if (error & ERR_DEV_CAPACITY) return set_error(PDM1_ERR_ARGUMENT, "a beam's moving box outgrew the plan's box capacity");
+    if (error & ERR_DEV_TIMEOUT) return set_error(PDM1_ERR_TIMEOUT, "a bounded device wait (bulk tile copy) timed out");
     return PDM1_OK;
 }
 
@@ -1191,6 +1192,7 @@ int create_plan(const pdm1_problem *problem, const pdm1_beam *beams, int nbeams,
     cf.summary = pl->d_sum;
     cf.moving = p.moving_active_domain ? 1 : 0;
     cf.fp32 = p.precision == PDM1_FP32_FP64 ? 1 : 0;
+    cf.bulk_stage = cf.fp32;
     cf.vacuum_aware = (p.moving_active_domain && p.vacuum_aware_cfl) ? 1 : 0;
     cf.guard = p.active_guard_cells;
     cf.tol = p.active_relative_tolerance;
@@ -1443,6 +1445,12 @@ int pdm1_plan_set_tile(pdm1_plan *pl, int tile_id) {
         bd.init_box = make_domain(o.i0, o.j0, o.k0, o.nx, o.ny, o.nz, o.inflow, t);
     }
     CUDA_TRY(cudaMemcpy(pl->d_beams, pl->h_beams.data(), pl->h_beams.size() * sizeof(BeamDev), cudaMemcpyHostToDevice));
+    return PDM1_OK;
+}
+
+int pdm1_plan_set_staging(pdm1_plan *pl, int bulk) {
+    if (!pl) return set_error(PDM1_ERR_ARGUMENT, "plan is NULL");
+    pl->cf.bulk_stage = (bulk && pl->cf.fp32) ? 1 : 0;
     return PDM1_OK;
 }
 

@@ -9,12 +9,132 @@
 namespace pdm1 {
 
 // Element e of component c's copy of an arm of asz elements.  Double arms are
-// [c][e]; float arms hold the components in pairs, [c / 2][e][c % 2], so a
-// 64-bit load brings two components of a cell into the packed f32x2 lanes.
+// [c][e]; float arms hold a cell's four components together, [e][c] (one
+// float4 per cell, the layout of the FP32 form's stage states in HBM), so a
+// 128-bit load brings (phi, Jx) and (Jy, Jz) into two packed f32x2 pairs.
 template <typename T>
 __device__ __forceinline__ T &arm_at(T *arm, int asz, int c, int e) {
-    if constexpr (sizeof(T) == sizeof(float)) return arm[((c >> 1) * asz + e) * 2 + (c & 1)];
+    if constexpr (sizeof(T) == sizeof(float)) return arm[e * 4 + c];
     else return arm[c * asz + e];
+}
+
+// The FP32 form keeps its stage states U1, U2 as one float4 (phi, Jx, Jy, Jz)
+// per cell: stage A writes U1, stage B reads U1 and writes U2, stage C reads
+// U2.  The stencil reads them in float in any case, so storing them rounded
+// changes no result; the state itself (U^n, V) and the dose stay in double.
+template <typename T, int MODE>
+constexpr bool kF4Source = sizeof(T) == sizeof(float) && (MODE == MODE_B || MODE == MODE_C);
+template <typename T, int MODE>
+constexpr bool kF4Dest = sizeof(T) == sizeof(float) && (MODE == MODE_A || MODE == MODE_B);
+
+// ---------------------------------------------------------------------------
+// Bulk staging of a float4 tile (cp.async.bulk, the TMA engine's untiled
+// copy, completed on a shared-memory mbarrier).  Every z row of every arm is
+// one contiguous copy of 16-byte cells; rows outside the domain in x or y
+// are the clamped rows (zero-gradient ghosts, numerics/boundary.py:327-397),
+// rows are clipped to [0, nz) in z and the z-max ghosts patched afterwards.
+// No multicast: each CTA copies from this GPU's own memory into its own
+// shared memory.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+    asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(unsigned long long *bar) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(smem_u32(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+
+// One row: `bytes` (a multiple of 16) from 16-byte aligned global memory to
+// 16-byte aligned shared memory, counted on `bar`.
+__device__ __forceinline__ void bulk_row(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
+    mbar_expect_tx(bar, bytes);
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// Issue the rows of one tile (x arm with its x halo, y arm, z arm), each
+// thread its share, then arrive once.  The x and y arms hold the tile's own
+// z range k0 .. k0 + TZ - 1, the z arm k0 - 3 .. k0 + TZ + 2.
+template <class Tl>
+__device__ __forceinline__ void bulk_stage_tile(const float4 *src, const DomainDev &d, int i0, int j0, int k0,
+                                                float4 *X, float4 *Y, float4 *Z, unsigned long long *bar) {
+    constexpr int TX = Tl::TX, TY = Tl::TY, TZ = Tl::TZ;
+    constexpr int RX = (TX + 6) * TY, RY = TX * (TY + 6), RZ = TX * TY;
+    const int nx = d.nx, ny = d.ny, nz = d.nz;
+    // shared memory read or written by the threads before (the last tile) is
+    // overwritten by the async proxy next
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    for (int r = threadIdx.x; r < RX + RY + RZ; r += NT) {
+        int li, lj, ka, kb, dst_e;
+        float4 *arm;
+        if (r < RX) {
+            const int j = r % TY, ii = r / TY;
+            li = i0 + ii - 3; lj = j0 + j; ka = k0; kb = k0 + TZ;
+            arm = X; dst_e = (ii * TY + j) * TZ;
+        } else if (r < RX + RY) {
+            const int q = r - RX, jj = q % (TY + 6), i = q / (TY + 6);
+            li = i0 + i; lj = j0 + jj - 3; ka = k0; kb = k0 + TZ;
+            arm = Y; dst_e = (i * (TY + 6) + jj) * TZ;
+        } else {
+            const int q = r - RX - RY, j = q % TY, i = q / TY;
+            li = i0 + i; lj = j0 + j; ka = k0 - 3; kb = k0 + TZ + 3;
+            arm = Z; dst_e = (i * TY + j) * (TZ + 6);
+        }
+        li = li < 0 ? 0 : (li >= nx ? nx - 1 : li);
+        lj = lj < 0 ? 0 : (lj >= ny ? ny - 1 : lj);
+        const int k_lo = ka < 0 ? 0 : ka, k_hi = kb > nz ? nz : kb;
+        if (k_hi > k_lo)
+            bulk_row(arm + dst_e + (k_lo - ka), src + ((size_t)li * ny + lj) * nz + k_lo,
+                     (unsigned)(k_hi - k_lo) * 16u, bar);
+    }
+    mbar_arrive(bar);
+}
+
+// Wait for the tile's rows; a wait past ~2^31 cycles (about a second) flags
+// ERR_DEV_TIMEOUT and lets the march end with an error instead of hanging.
+__device__ __forceinline__ void bulk_wait(unsigned long long *bar, unsigned parity, int *error) {
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity)) {
+        if (clock64() - t0 > (1ll << 31)) {
+            atomicOr(error, ERR_DEV_TIMEOUT);
+            return;
+        }
+    }
+}
+
+// z-max ghosts of the z arm of a tile whose z range passes nz: the cells
+// beyond hold the last cell's value (zero gradient).
+template <class Tl>
+__device__ __forceinline__ void patch_zmax(const DomainDev &d, int k0, float4 *Z) {
+    constexpr int TX = Tl::TX, TY = Tl::TY, TZ = Tl::TZ;
+    const int over = k0 + TZ + 3 - d.nz;   // cells of each z-arm row beyond nz
+    if (over <= 0) return;
+    const int last = d.nz - 1 - (k0 - 3);   // arm index of the domain's last z cell
+    for (int e = threadIdx.x; e < TX * TY * over; e += NT) {
+        const int row = e / over, kk = last + 1 + e % over;
+        Z[row * (TZ + 6) + kk] = Z[row * (TZ + 6) + last];
+    }
 }
 
 // LEARN (stage C of a plan with a learned box): the tile's fluence moments of
@@ -38,6 +158,15 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 4) stage
     const bool unit = cf.unit_speeds != 0;
     const bool all_axes[3] = {true, true, true};
     double cta_inv = 0.0;
+    // FP32 stages B and C: bulk copies of the float4 stage state, one mbarrier phase per tile
+    __shared__ __align__(8) unsigned long long stage_bar;
+    unsigned bar_phase = 0;
+    if constexpr (kF4Source<T, MODE>) {
+        if (cf.bulk_stage) {
+            if (tid == 0) mbar_init(&stage_bar, NT);
+            __syncthreads();
+        }
+    }
     // tiles of all marching beams, back to back (one beam: its domain's tiles)
     const int total = MODE == MODE_RHS ? a.st[0].dom.ntiles : cf.tile_off[cf.nbeams];
 
@@ -61,6 +190,48 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 4) stage
         const int i0 = tx * TX, j0 = ty * TY, k0 = tz * TZ;
 
         // ---- 1. stage the stencil source + halo (the core into all three arms) ----
+        if constexpr (kF4Source<T, MODE>) {
+            // the float4 stage state: bulk copies, or (bulk_stage == 0) one
+            // 128-bit load per cell; the arms receive the same values either way
+            const float4 *src4 = reinterpret_cast<const float4 *>(src);
+            float4 *X4 = reinterpret_cast<float4 *>(s.X), *Y4 = reinterpret_cast<float4 *>(s.Y);
+            float4 *Z4 = reinterpret_cast<float4 *>(s.Z);
+            if (cf.bulk_stage) {
+                bulk_stage_tile<Tl>(src4, d, i0, j0, k0, X4, Y4, Z4, &stage_bar);
+                bulk_wait(&stage_bar, bar_phase, &stb.error);
+                bar_phase ^= 1u;
+                patch_zmax<Tl>(d, k0, Z4);
+            } else {
+                auto cell = [&](int li, int lj, int lk) {
+                    li = li < 0 ? 0 : (li >= nx ? nx - 1 : li);
+                    lj = lj < 0 ? 0 : (lj >= ny ? ny - 1 : lj);
+                    lk = lk >= nz ? nz - 1 : lk;
+                    return src4[((size_t)li * ny + lj) * nz + lk];
+                };
+                for (int e = tid; e < SX; e += NT) {
+                    const int k = e % TZ, j = (e / TZ) % TY, ii = e / (TZ * TY);
+                    const float4 v = cell(i0 + ii - 3, j0 + j, k0 + k);
+                    X4[(ii * TY + j) * TZ + k] = v;
+                    if (ii >= 3 && ii < TX + 3) {
+                        Y4[((ii - 3) * (TY + 6) + j + 3) * TZ + k] = v;
+                        Z4[((ii - 3) * TY + j) * (TZ + 6) + k + 3] = v;
+                    }
+                }
+                for (int e = tid; e < SY; e += NT) {
+                    const int k = e % TZ, jj = (e / TZ) % 6, i = e / (TZ * 6);
+                    const int gj = jj < 3 ? j0 + jj - 3 : j0 + TY + jj - 3;
+                    const int aj = jj < 3 ? jj : TY + jj;
+                    Y4[(i * (TY + 6) + aj) * TZ + k] = cell(i0 + i, gj, k0 + k);
+                }
+                for (int e = tid; e < SZ; e += NT) {
+                    const int kk = e % 6, j = (e / 6) % TY, i = e / (6 * TY);
+                    const int gk = kk < 3 ? k0 + kk - 3 : k0 + TZ + kk - 3;
+                    const int ak = kk < 3 ? kk : TZ + kk;
+                    if (gk < 0) continue;   // z-min ghost, filled below
+                    Z4[(i * TY + j) * (TZ + 6) + ak] = cell(i0 + i, j0 + j, gk);
+                }
+            }
+        } else {
         for (int e = tid; e < SX; e += NT) {
             int k = e % TZ, j = (e / TZ) % TY, ii = e / (TZ * TY);
             double u[4];
@@ -98,6 +269,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 4) stage
 #pragma unroll
             for (int c = 0; c < 4; ++c) arm_at(s.Z, AZ, c, (i * TY + j) * (TZ + 6) + ak) = T(u[c]);
         }
+        }   // the double-precision source
         __syncthreads();
         // ---- 2. z-min ghost cells: quartic extrapolation through the inflow ----
         if (k0 == 0) {
@@ -148,18 +320,22 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 4) stage
             }
             if (cf.spatial == PDM1_SPATIAL_WENO_Z) {
                 if constexpr (sizeof(T) == sizeof(float)) {
-                    // two components per packed reconstruction, L and R from the same loads
-                    const float2 *b2 = reinterpret_cast<const float2 *>(arm) + e0;
+                    // two components per packed reconstruction, L and R from the
+                    // same six 128-bit loads: (phi, Jx) and (Jy, Jz) of each cell
+                    const float4 *b4 = reinterpret_cast<const float4 *>(arm) + e0;
+                    float2 w01[6], w23[6];
 #pragma unroll
-                    for (int pc = 0; pc < 2; ++pc) {
-                        float2 w[6];
-#pragma unroll
-                        for (int q = 0; q < 6; ++q) w[q] = b2[pc * cs + q * stride];
-                        const float2 l = weno_left_f32x2(w[0], w[1], w[2], w[3], w[4]);
-                        const float2 r = weno_left_f32x2(w[5], w[4], w[3], w[2], w[1]);
-                        L[2 * pc] = l.x; L[2 * pc + 1] = l.y;
-                        R[2 * pc] = r.x; R[2 * pc + 1] = r.y;
+                    for (int q = 0; q < 6; ++q) {
+                        const float4 v = b4[q * stride];
+                        w01[q] = make_float2(v.x, v.y);
+                        w23[q] = make_float2(v.z, v.w);
                     }
+                    float2 l = weno_left_f32x2(w01[0], w01[1], w01[2], w01[3], w01[4]);
+                    float2 r = weno_left_f32x2(w01[5], w01[4], w01[3], w01[2], w01[1]);
+                    L[0] = l.x; L[1] = l.y; R[0] = r.x; R[1] = r.y;
+                    l = weno_left_f32x2(w23[0], w23[1], w23[2], w23[3], w23[4]);
+                    r = weno_left_f32x2(w23[5], w23[4], w23[3], w23[2], w23[1]);
+                    L[2] = l.x; L[3] = l.y; R[2] = r.x; R[3] = r.y;
                 } else {
                     const T *base = arm + e0;
 #pragma unroll
@@ -252,9 +428,12 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 4) stage
                         u1[c] = w / co.S1[m];
                     }
                     project(u1[0], u1[1], u1[2], u1[3]);
+                    if constexpr (kF4Dest<T, MODE>)
+                        reinterpret_cast<float4 *>(U1)[o] = make_float4(float(u1[0]), float(u1[1]), float(u1[2]),
+                                                                        float(u1[3]));
 #pragma unroll
                     for (int c = 0; c < 4; ++c) {
-                        U1[c * N + o] = u1[c];
+                        if constexpr (!kF4Dest<T, MODE>) U1[c * N + o] = u1[c];
                         Vb[c * N + o] = v1[c];
                     }
                     double q0 = un[0] * s0, q1 = u1[0] * co.S1[m];
@@ -271,8 +450,17 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 4) stage
                         u2[c] = w / co.S2[m];
                     }
                     project(u2[0], u2[1], u2[2], u2[3]);
+                    if constexpr (kF4Dest<T, MODE>) {
+                        reinterpret_cast<float4 *>(U2)[o] = make_float4(float(u2[0]), float(u2[1]), float(u2[2]),
+                                                                        float(u2[3]));
+                        // the dose quadrature's stage-2 term, from the double state
+                        // (stage C reads the sum; the same sum, rounded as it would be there)
+                        double q2 = u2[0] * co.S2[m];
+                        qb[o] = qb[o] + 2.0 / 3.0 * q2;
+                    } else {
 #pragma unroll
-                    for (int c = 0; c < 4; ++c) U2[c * N + o] = u2[c];
+                        for (int c = 0; c < 4; ++c) U2[c * N + o] = u2[c];
+                    }
                 } else {
                     double unew[4];
                     double ed;
@@ -286,11 +474,13 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 4) stage
                             unew[c] = w / co.S1[m];
                         }
                         project(unew[0], unew[1], unew[2], unew[3]);
-                        double u2c = sizeof(T) == sizeof(double)
-                                         ? double(s.X[((0 * (TX + 6) + (i + 3)) * TY + j) * TZ + k])
-                                         : U2[o];
-                        double q2 = u2c * co.S2[m];
-                        ed = dE * (qb[o] + 2.0 / 3.0 * q2);
+                        if constexpr (sizeof(T) == sizeof(double)) {
+                            double u2c = double(s.X[((0 * (TX + 6) + (i + 3)) * TY + j) * TZ + k]);
+                            double q2 = u2c * co.S2[m];
+                            ed = dE * (qb[o] + 2.0 / 3.0 * q2);
+                        } else {
+                            ed = dE * qb[o];   // stage B added 2/3 q2
+                        }
                     } else {   // forward Euler, numerics/energy.py:663-722
 #pragma unroll
                         for (int c = 0; c < 4; ++c) {
