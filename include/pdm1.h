@@ -220,6 +220,15 @@ int pdm1_gamma(const double *dose_ref, const double *dose_eval, int nx, int ny, 
                double max_gamma, double global_normalisation, double *gamma_out,
                double *pass_rate_out, pdm1_stream_t stream);
 
+/* A prescribed energy schedule for a one-beam plan: the march steps through
+ * energies[0..n-1] (energies[0] the start energy, strictly decreasing)
+ * instead of its CFL steps, then on to energy_min in one step; n = 0 restores
+ * the CFL rule.  No reference function; it is the fixed-schedule mode the
+ * reference's own harness gets by patching compute_energy_step
+ * (numerics/energy.py:539-660): a march given the reference's own energies
+ * isolates the per-step arithmetic from the choice of step. */
+int pdm1_plan_set_schedule(pdm1_plan *plan, const double *energies, int n);
+
 /* Staging of the FP32 form's stages B and C (no counterpart in the reference;
  * the reference has no GPU tiles): bulk = 1 (the default) copies each z row of
  * the tile and its halo with cp.async.bulk onto a shared-memory mbarrier,

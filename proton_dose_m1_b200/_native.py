@@ -92,6 +92,7 @@ def lib():
         L.pdm1_pool_release.argtypes = []
         L.pdm1_pool_release.restype = C.c_int
         L.pdm1_plan_set_staging.argtypes = [_vp, C.c_int]
+        L.pdm1_plan_set_schedule.argtypes = [_vp, _dp, C.c_int]
         L.pdm1_march.argtypes = [_vp, _vp, _vp, _vp, C.c_int, _dp, C.c_int, _vp, _dp,
                                  C.POINTER(MarchInfo), _vp]
         L.pdm1_field_plan_create.argtypes = [C.POINTER(Problem), C.POINTER(BeamDesc), C.c_int,
@@ -148,5 +149,6 @@ EXPORTED_SYMBOLS = (
     "pdm1_mlp_gradients", "pdm1_mlp_forward", "pdm1_box_model_infer",
     "pdm1_tile_shape", "pdm1_plan_set_tile", "pdm1_plan_autotune", "pdm1_analytical_csda_dose",
     "pdm1_pool_cached_bytes", "pdm1_pool_release", "pdm1_plan_set_staging",
+    "pdm1_plan_set_schedule",
 )
 NUM_TILES = 3

@@ -106,6 +106,8 @@ struct ConfigDev {
     int tile_id;
     int fp32;                   // FP32-stencil form: float eigenvalues in the CFL bound (not with cfl_floor)
     int bulk_stage;             // FP32 form: stages B and C stage their float4 source by bulk copies
+    const double *schedule;     // prescribed energies E_0 .. E_{n-1} (replaces the CFL step), or NULL
+    int n_schedule;
     // learned moving box and training-data recorder
     int learned;                // a box model proposes the margins
     const BoxModelDev *model;

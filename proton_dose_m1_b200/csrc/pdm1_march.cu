@@ -178,6 +178,10 @@ __global__ void __launch_bounds__(256) prologue_kernel(const ConfigDev *cfp, Coe
             } else {
                 if (st->forced_dE > 0.0) {
                     dE = st->forced_dE;
+                } else if (cf.schedule) {
+                    // a prescribed energy schedule (another run's steps): the
+                    // next energy is taken as given, past its end down to Emin
+                    dE = st->step + 1 < cf.n_schedule ? E - cf.schedule[st->step + 1] : E - cf.Emin;
                 } else {
                     double inv = __longlong_as_double((long long)st->inv_bits);
                     dE = cf.cfl / inv;
@@ -194,6 +198,8 @@ __global__ void __launch_bounds__(256) prologue_kernel(const ConfigDev *cfp, Coe
                 } else {
                     active = 1;
                     En = E - dE;
+                    if (cf.schedule && st->forced_dE <= 0.0 && st->step + 1 < cf.n_schedule)
+                        En = cf.schedule[st->step + 1];
                     int step = st->step + 1;
                     if (energies) energies[step] = En;
                     if (st->ti < cf.n_targets && fabs(En - cf.targets[st->ti]) <= 1e-12) {
@@ -742,6 +748,7 @@ struct pdm1_plan {
     int32_t *d_ids = nullptr;
     double *d_spatial = nullptr;    // nbeams x (nx, ny)
     double *d_targets = nullptr;
+    double *d_schedule = nullptr;   // prescribed energies (pdm1_plan_set_schedule)
     double *d_U1 = nullptr, *d_U2 = nullptr, *d_V = nullptr, *d_q = nullptr;
     double *d_bufA = nullptr, *d_bufB = nullptr;   // moving box: compact-state ping-pong
     unsigned long long *d_slab = nullptr;
@@ -1047,6 +1054,7 @@ void destroy_plan(pdm1_plan *pl) {
     pool_free(pl->d_ids);
     pool_free(pl->d_spatial);
     pool_free(pl->d_targets);
+    pool_free(pl->d_schedule);
     pool_free(pl->d_U1);
     pool_free(pl->d_U2);
     pool_free(pl->d_V);
@@ -1445,6 +1453,25 @@ int pdm1_plan_set_tile(pdm1_plan *pl, int tile_id) {
         bd.init_box = make_domain(o.i0, o.j0, o.k0, o.nx, o.ny, o.nz, o.inflow, t);
     }
     CUDA_TRY(cudaMemcpy(pl->d_beams, pl->h_beams.data(), pl->h_beams.size() * sizeof(BeamDev), cudaMemcpyHostToDevice));
+    return PDM1_OK;
+}
+
+int pdm1_plan_set_schedule(pdm1_plan *pl, const double *energies, int n) {
+    if (!pl) return set_error(PDM1_ERR_ARGUMENT, "plan is NULL");
+    if (n < 0 || (n > 0 && !energies)) return set_error(PDM1_ERR_ARGUMENT, "schedule: NULL energies or n < 0");
+    if (pl->nbeams != 1) return set_error(PDM1_ERR_UNSUPPORTED, "a prescribed schedule is for one-beam plans");
+    for (int k = 1; k < n; ++k)
+        if (!(energies[k] < energies[k - 1]))
+            return set_error(PDM1_ERR_ARGUMENT, "schedule: energies must decrease strictly");
+    pool_free(pl->d_schedule);
+    pl->d_schedule = nullptr;
+    pl->cf.schedule = nullptr;
+    pl->cf.n_schedule = 0;
+    if (n == 0) return PDM1_OK;
+    CUDA_TRY(pool_malloc((void **)&pl->d_schedule, (size_t)n * sizeof(double)));
+    CUDA_TRY(cudaMemcpy(pl->d_schedule, energies, (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
+    pl->cf.schedule = pl->d_schedule;
+    pl->cf.n_schedule = n;
     return PDM1_OK;
 }
 

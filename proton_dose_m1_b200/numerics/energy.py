@@ -182,6 +182,14 @@ class M1Plan:
     def workspace_bytes(self) -> int:
         return int(_native.lib().pdm1_plan_workspace_bytes(self._h))
 
+    def set_schedule(self, energies=None) -> None:
+        """March through the given energies (start energy first, decreasing)
+        instead of the CFL steps; None restores the CFL rule."""
+        E = np.ascontiguousarray([] if energies is None else energies, dtype=np.float64)
+        _native.check(_native.lib().pdm1_plan_set_schedule(
+            self._h, E.ctypes.data_as(C.POINTER(C.c_double)) if len(E) else None, len(E)))
+        self._schedule = E
+
     @staticmethod
     def _stream():
         torch = _torch()

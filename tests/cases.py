@@ -76,7 +76,7 @@ def published_config(case: dict) -> SolverConfig:
                 sigma=tuple(b["sigma"]), center=tuple(b["center"]),
                 angular_spread=b["angular_spread"], cutoff_sigma=b["cutoff_sigma"])
     phys = Physics(scattering=Scattering[p["scattering"]], nuclear=p["nuclear"],
-                   coefficient_interpolation=CoefficientInterpolation[p["coefficient_interpolation"]])
+                   coefficient_interpolation=CoefficientInterpolation[p.get("coefficient_interpolation", "LINEAR")])
     num = Numerics(spatial_scheme=SpatialScheme[n["spatial_scheme"]],
                    energy_scheme=EnergyScheme[n["energy_scheme"]],
                    wave_speeds=WaveSpeeds[n["wave_speeds"]], max_energy_step=n["max_energy_step"],

@@ -369,6 +369,45 @@ def published_full(root: Path):
     (OUT / "published_kats_full.json").write_text(json.dumps(cases, indent=1))
 
 
+def _reference_config(ps, c):
+    """The reference's SolverConfig for a published config dict (no reference solve)."""
+    g, b, n, ph = c["geometry"], c["beam"], c["numerics"], c["physics"]
+    objects = [ps.Box(o["x_min"], o["x_max"], o["y_min"], o["y_max"], o["z_min"], o["z_max"],
+                      ps.Material[o["material"]]) for o in g["objects"]]
+    geo = ps.Geometry(size=tuple(g["size"]), resolution=tuple(g["resolution"]),
+                      background_material=ps.Material[g["background_material"]], objects=objects)
+    beam = ps.Beam(n_protons=b["n_protons"], energy=b["energy"], energy_spread=b["energy_spread"],
+                   sigma=tuple(b["sigma"]), center=tuple(b["center"]), angular_spread=b["angular_spread"],
+                   cutoff_sigma=b["cutoff_sigma"])
+    phys = ps.Physics(scattering=ps.Scattering[ph["scattering"]], nuclear=ph["nuclear"])
+    num = ps.Numerics(spatial_scheme=ps.SpatialScheme[n["spatial_scheme"]],
+                      energy_scheme=ps.EnergyScheme[n["energy_scheme"]], wave_speeds=ps.WaveSpeeds[n["wave_speeds"]],
+                      max_energy_step=n["max_energy_step"], cfl=n["cfl"], energy_min=n["energy_min"],
+                      energy_window_sigma=n["energy_window_sigma"], moving_active_domain=n["moving_active_domain"],
+                      vacuum_aware_cfl=n["vacuum_aware_cfl"], active_truncation_sigma=n["active_truncation_sigma"],
+                      active_guard_cells=n["active_guard_cells"])
+    return ps.SolverConfig(geometry=geo, beam=beam, physics=phys, numerics=num, backend=ps.Backend.CPU,
+                           references=ps.References(reference=ps.Reference.NONE))
+
+
+def published_schedules(ps, groups):
+    """The reference's own energy steps (and maximum dose) for the full-size
+    published cases of ``groups``, run here with the unmodified reference:
+    published_schedules.npz, keys '<case>/energies' and '<case>/max_dose'.
+    Cases already in the file are kept."""
+    kats = json.loads((OUT / "published_kats_full.json").read_text())
+    out_file = OUT / "published_schedules.npz"
+    out = dict(np.load(out_file)) if out_file.exists() else {}
+    for name, kat in kats.items():
+        if name.split("/")[0] not in groups or f"{name}/energies" in out:
+            continue
+        r = ps.Solver(_reference_config(ps, kat["config"])).solve()
+        out[f"{name}/energies"] = np.asarray(r.energies, dtype=np.float64)
+        out[f"{name}/max_dose"] = np.float64(r.dose.max())
+        print(name, len(r.energies) - 1, float(r.dose.max()), r.runtime, flush=True)
+        np.savez_compressed(out_file, **out)
+
+
 def published_configs(root: Path):
     """The canonical configurations and their hashes from the reference's own
     run directories (config.json, metadata.json of thesis_results/)."""
@@ -383,7 +422,7 @@ def published_configs(root: Path):
 
 if __name__ == "__main__":
     if len(sys.argv) < 2:
-        sys.exit("usage: make_golden.py <reference root> [configs|published|schemes|analytical]")
+        sys.exit("usage: make_golden.py <reference root> [configs|published|schedules [groups]|schemes|analytical]")
     root = Path(sys.argv[1])
     if len(sys.argv) > 2 and sys.argv[2] == "configs":
         published_configs(root)
@@ -393,6 +432,9 @@ if __name__ == "__main__":
         published_full(root)
         sys.exit(0)
     ps = import_reference(root)
+    if len(sys.argv) > 2 and sys.argv[2] == "schedules":
+        published_schedules(ps, sys.argv[3].split(",") if len(sys.argv) > 3 else ["coarse_grid_1mm"])
+        sys.exit(0)
     if len(sys.argv) > 2 and sys.argv[2] == "schemes":
         schemes(ps)
         sys.exit(0)
