@@ -44,12 +44,13 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "spots/s at gamma1%/1mm>=99.5% vs plain FP64 GPU path; stage-kernel HBM GB/s"
-# Algorithmic DRAM bytes per cell-step of the march: U^n read by each of the
-# three stages (96), three stage states written (96) and two read back (64),
-# dose read+write (16), material id per stage (3).  The state and the stage
-# states are stored in double in both precision modes (the FP32 form converts
-# on load), so the count is the same for both.
-ALG_BYTES_PER_CELL_STEP = {"FP64": 275.0, "FP32_FP64": 275.0}
+# Algorithmic DRAM bytes per cell-step of the march (three stages), every array
+# once per use: U^n read by each stage (96), the stage states U1 and U2 written
+# and read (FP64: 128; the FP32 form keeps them as float4: 64), U^{n+1} written
+# (32), the marched variable V written, read and written, read (128), the dose
+# quadrature part (FP64: 16; FP32: 32, stage B adds its term), the dose read and
+# written (16), the int32 material ids per stage (12).
+ALG_BYTES_PER_CELL_STEP = {"FP64": 428.0, "FP32_FP64": 380.0}
 # Algorithmic floating-point operations per cell-step of the WENO-Z march:
 # three stages x (three owned faces x (8 reconstructions, 2 projections, HLL
 # with both closures and wave-speed pairs) + divergence and stage update),
