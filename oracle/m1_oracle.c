@@ -136,6 +136,8 @@ struct orc_problem {
     mat_t *mats;
     int32_t *ids;
     double *spatial;     /* n_protons * normalised profile, (nx, ny) */
+    double *schedule;    /* prescribed energies E_0 .. E_{n-1} (orc_set_schedule), or NULL */
+    int n_schedule;
 };
 
 static double sign_of(double x) { return (x > 0.0) - (x < 0.0); }
@@ -547,6 +549,19 @@ static int build_inflow(orc_problem *p)
     return ORC_OK;
 }
 
+int orc_set_schedule(orc_problem *p, const double *energies, int n)
+{
+    free(p->schedule);
+    p->schedule = NULL;
+    p->n_schedule = 0;
+    if (n <= 0) return ORC_OK;
+    p->schedule = malloc(sizeof(double) * n);
+    if (!p->schedule) return fail(ORC_ERR_ARG, "schedule: out of memory");
+    memcpy(p->schedule, energies, sizeof(double) * n);
+    p->n_schedule = n;
+    return ORC_OK;
+}
+
 void orc_problem_destroy(orc_problem *p)
 {
     if (!p) return;
@@ -559,6 +574,7 @@ void orc_problem_destroy(orc_problem *p)
     }
     free(p->ids);
     free(p->spatial);
+    free(p->schedule);
     free(p);
 }
 
@@ -1521,6 +1537,9 @@ static int march_impl(const orc_problem *p, double *U, double *dose, double *ene
         double dE;
         rc = energy_step(p, &L.dm, Ua, E, (moving && d->vacuum_aware_cfl) ? tol : -1.0, &dE);
         if (rc) { free_local(&L); break; }
+        /* a prescribed schedule replaces the CFL step (the fixed-schedule mode
+           of the reference's harness: a patched compute_energy_step) */
+        if (p->schedule) dE = steps + 1 < p->n_schedule ? E - p->schedule[steps + 1] : E - Emin;
         if (ti < nt) {
             double t = targets[ti];
             if (E > t && t >= E - dE) dE = E - t;
@@ -1543,6 +1562,7 @@ static int march_impl(const orc_problem *p, double *U, double *dose, double *ene
         free(edep);
         free_local(&L);
         E -= dE;
+        if (p->schedule && steps + 1 < p->n_schedule) E = p->schedule[steps + 1];
         steps++;
         if (energies) energies[steps] = E;
         if (ti < nt && fabs(E - targets[ti]) <= 1e-12) {

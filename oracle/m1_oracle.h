@@ -125,6 +125,8 @@ int orc_march(const orc_problem *p, double *U, double *dose,
  * from the configured start energy and return the number actually run. */
 int orc_march_steps(const orc_problem *p, double *U, double *dose, int steps, int *n_done);
 
+/* March through energies[0..n-1] instead of the CFL steps (n = 0: the CFL rule). */
+int  orc_set_schedule(orc_problem *p, const double *energies, int n);
 void orc_set_threads(int n);
 
 #ifdef __cplusplus

@@ -88,6 +88,7 @@ def lib():
                                 _dp, C.c_int, _dp, _dp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.orc_march_steps.argtypes = [C.c_void_p, _dp, _dp, C.c_int, C.POINTER(C.c_int)]
         L.orc_set_threads.argtypes = [C.c_int]
+        L.orc_set_schedule.argtypes = [C.c_void_p, _dp, C.c_int]
         _lib = L
     return _lib
 
@@ -256,6 +257,12 @@ class OracleProblem:
         edep = np.empty(self.shape)
         _check(lib().orc_advance(self._h, _ptr(U), energy, dE, _ptr(edep)))
         return U, edep
+
+    def set_schedule(self, energies=None):
+        """March through the given energies instead of the CFL steps (None: CFL rule)."""
+        E = np.ascontiguousarray([] if energies is None else energies, dtype=float)
+        self._schedule = E
+        _check(lib().orc_set_schedule(self._h, _ptr(E) if len(E) else None, len(E)))
 
     # -- the march ----------------------------------------------------------
     def march(self, U=None, snapshot_energies=(), max_steps=200000):

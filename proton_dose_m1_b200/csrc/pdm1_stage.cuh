@@ -169,25 +169,6 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 4) stage
     }
     // tiles of all marching beams, back to back (one beam: its domain's tiles)
     const int total = MODE == MODE_RHS ? a.st[0].dom.ntiles : cf.tile_off[cf.nbeams];
-    // bulk staging: the copies of a tile are issued while the previous tile
-    // finishes (its arms are free once the faces are done), so their latency
-    // hides behind the previous tile's stage update
-    auto issue_tile = [&](int g) {
-        if constexpr (kF4Source<T, MODE>) {
-            const int bb = cf.nbeams == 1 ? 0 : beam_of_tile(cf.tile_off, cf.nbeams, g);
-            const DomainDev dd = a.st[bb].dom;
-            const int tl = g - cf.tile_off[bb];
-            const int z = tl % dd.tiles_z, y = (tl / dd.tiles_z) % dd.tiles_y, x = tl / (dd.tiles_z * dd.tiles_y);
-            const double *base = (MODE == MODE_B ? a.U1 : a.U2) + 4 * (size_t)bb * cf.cap;
-            bulk_stage_tile<Tl>(reinterpret_cast<const float4 *>(base), dd, x * TX, y * TY, z * TZ,
-                                reinterpret_cast<float4 *>(s.X), reinterpret_cast<float4 *>(s.Y),
-                                reinterpret_cast<float4 *>(s.Z), &stage_bar);
-        }
-    };
-    if constexpr (kF4Source<T, MODE>) {
-        if (cf.bulk_stage && (int)blockIdx.x < total) issue_tile(blockIdx.x);
-    }
-
     for (int gt = blockIdx.x; gt < total; gt += gridDim.x) {
         const int b = (MODE == MODE_RHS || cf.nbeams == 1) ? 0 : beam_of_tile(cf.tile_off, cf.nbeams, gt);
         const int tile = MODE == MODE_RHS ? gt : gt - cf.tile_off[b];
@@ -214,7 +195,8 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 4) stage
             const float4 *src4 = reinterpret_cast<const float4 *>(src);
             float4 *X4 = reinterpret_cast<float4 *>(s.X), *Y4 = reinterpret_cast<float4 *>(s.Y);
             float4 *Z4 = reinterpret_cast<float4 *>(s.Z);
-            if (cf.bulk_stage) {   // issued before the loop or during the previous tile
+            if (cf.bulk_stage) {
+                bulk_stage_tile<Tl>(src4, d, i0, j0, k0, X4, Y4, Z4, &stage_bar);
                 bulk_wait(&stage_bar, bar_phase, &stb.error);
                 bar_phase ^= 1u;
                 patch_zmax<Tl>(d, k0, Z4);
@@ -396,9 +378,6 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 4) stage
             for (int c = 0; c < 4; ++c) s.F[c * NF + f] = F[c];
         }
         __syncthreads();
-        if constexpr (kF4Source<T, MODE>) {
-            if (cf.bulk_stage && gt + (int)gridDim.x < total) issue_tile(gt + gridDim.x);
-        }
         // ---- 4. divergence and the stage update, one cell per thread ----
         const int k = tid % TZ, j = (tid / TZ) % TY, i = tid / (TZ * TY);
         const int li = i0 + i, lj = j0 + j, lk = k0 + k;
