@@ -354,6 +354,9 @@ BOX = "learned"
 PRECISION = "fp32"
 
 
+TILE_OVERRIDE = []   # --tile: a fixed stage tile shape instead of the autotuner's
+
+
 def accelerated_config(cfg):
     """The accelerated form: moving active box (learned proposer, or the fixed
     heuristic) + FP32 stencil / FP64 dose + autotuned tile shape."""
@@ -364,7 +367,8 @@ def accelerated_config(cfg):
     precision = Precision.FP32_FP64 if PRECISION == "fp32" else Precision.FP64
     return SolverConfig(geometry=cfg.geometry, beam=cfg.beam, physics=cfg.physics,
                         numerics=replace(cfg.numerics, moving_active_domain=True),
-                        accel=Accel(precision=precision, box_model=model, tile="auto", phantom_cfl=True))
+                        accel=Accel(precision=precision, box_model=model,
+                                    tile=TILE_OVERRIDE[0] if TILE_OVERRIDE else "auto", phantom_cfl=True))
 
 
 def accelerated_label():
@@ -736,6 +740,8 @@ def main():
                     help="moving box of the accelerated form")
     ap.add_argument("--precision", choices=("fp32", "fp64"), default=None,
                     help="stencil arithmetic of the accelerated form (default: fp32; fields: their own)")
+    ap.add_argument("--tile", default=None,
+                    help="stage tile shape instead of the autotuner's (e.g. 2x8x16, or 'default'; profiling)")
     ap.add_argument("--gate-spots", type=int, default=-1,
                     help="field workloads: spots of the accuracy gate (-1: the workload's own, 0: no gate)")
     ap.add_argument("--profile-spots", type=int, default=0,
@@ -750,6 +756,22 @@ def main():
     cfg, desc = (None, None) if args.workload in FIELDS else workload(args.workload)
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.tile:
+        TILE_OVERRIDE.append(None if args.tile == "default" else tuple(int(v) for v in args.tile.split("x")))
+    if args.profile_spots > 0 and args.workload in FIELDS and args.profile_steps > 0:
+        # the first K energy steps of the spots (a bounded prefix for profiler captures)
+        from proton_dose_m1_b200.numerics.energy import FieldPlan
+        import torch
+        fcfg, mm, grid, beams, _ = field_workload(args.workload)
+        sub = [beams[k] for k in gate_sample(beams, args.profile_spots)]
+        plan = FieldPlan(accelerated_config(fcfg), mm, grid, sub)
+        plan.march_steps(args.profile_steps)
+        torch.cuda.synchronize()
+        info = plan.last_info
+        print(json.dumps({"profile_spots": len(sub), "profile_steps": args.profile_steps,
+                          "stage_launches": info.stage_launches, "stage_ms": info.stage_ms,
+                          "cell_steps": info.cell_steps, "box_capacity_cells": plan.cap}))
         return
     if args.profile_spots > 0 and args.workload in FIELDS:
         from proton_dose_m1_b200.numerics.energy import FieldPlan

@@ -150,7 +150,9 @@ int pdm1_field_march(pdm1_plan *plan, double *field_dose, int max_steps, int *st
                      pdm1_march_info *info, pdm1_stream_t stream);
 
 /* The first `step_limit` steps of the march (a bounded prefix, for timing
- * samples and prefix parity); otherwise as pdm1_march without snapshots. */
+ * samples, profiler captures and prefix parity); otherwise as pdm1_march
+ * without snapshots.  For a field plan U and energies are not used (may be
+ * NULL) and `dose` receives the field dose of those steps. */
 int pdm1_march_steps(pdm1_plan *plan, double *U, double *dose, double *energies, int max_steps,
                      int step_limit, pdm1_march_info *info, pdm1_stream_t stream);
 

@@ -366,9 +366,11 @@ __device__ __forceinline__ double cfl_term(const ConfigDev &cf, double rf, const
         a0 = a1 = a2 = 1.0;
     } else {
         const T p = T(u[0]), x = T(u[1]), y = T(u[2]), z = T(u[3]);
-        a0 = double(max_abs_speed(p, x, y, z, 0));
-        a1 = double(max_abs_speed(p, x, y, z, 1));
-        a2 = double(max_abs_speed(p, x, y, z, 2));
+        T a[3];
+        max_abs_speeds3(p, x, y, z, a);
+        a0 = double(a[0]);
+        a1 = double(a[1]);
+        a2 = double(a[2]);
         if (entrance) {
             T pin = T(phi_in);
             T jz = T(rf) * pin;

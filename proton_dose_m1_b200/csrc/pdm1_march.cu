@@ -572,7 +572,10 @@ __global__ void __launch_bounds__(NT) rebox_kernel(const ConfigDev *cfp, const C
     const size_t N = (size_t)d.nx * d.ny * d.nz, NP = (size_t)p.nx * p.ny * p.nz;
     double m = 0.0, inv = 0.0;
     for (size_t o = (size_t)blockIdx.x * NT + threadIdx.x; o < N; o += (size_t)gridDim.x * NT) {
-        const int lk = (int)(o % d.nz), lj = (int)((o / d.nz) % d.ny), li = (int)(o / ((size_t)d.nz * d.ny));
+        // a box holds fewer than 2^32 cells: 32-bit index arithmetic
+        const unsigned uo = (unsigned)o, unz = (unsigned)d.nz, uny = (unsigned)d.ny;
+        const unsigned row = uo / unz;
+        const int lk = (int)(uo - row * unz), lj = (int)(row % uny), li = (int)(row / uny);
         double u[4];
         if (moved) {
             int pi = d.i0 + li - p.i0, pj = d.j0 + lj - p.j0, pk = d.k0 + lk - p.k0;
@@ -1569,8 +1572,11 @@ int pdm1_march(pdm1_plan *pl, double *U, double *dose, double *energies, int max
 
 int pdm1_march_steps(pdm1_plan *pl, double *U, double *dose, double *energies, int max_steps,
                      int step_limit, pdm1_march_info *info, pdm1_stream_t stream) {
-    if (!pl || pl->field) return set_error(PDM1_ERR_ARGUMENT, "pdm1_march_steps takes a one-beam plan");
+    if (!pl) return set_error(PDM1_ERR_ARGUMENT, "plan is NULL");
     if (step_limit < 0) return set_error(PDM1_ERR_ARGUMENT, "step_limit must be >= 0");
+    if (pl->field)   // a field plan: the prefix of every beam, the field dose of those steps
+        return march_impl(pl, nullptr, dose, nullptr, max_steps, nullptr, 0, nullptr, nullptr, info, stream,
+                          step_limit, nullptr);
     return march_impl(pl, U, dose, energies, max_steps, nullptr, 0, nullptr, nullptr, info, stream,
                       step_limit, nullptr);
 }

@@ -292,6 +292,35 @@ PDM1_HD void eigen(T phi, T jx, T jy, T jz, T jn, int axis, T &lmin, T &lmax) {
     lmax = (T(2) * f * mu + root) / den;
 }
 
+// max(|lambda_min|, |lambda_max|) along x, y and z at once: |J|, f, chi and
+// 5 - 3 chi are formed once per cell instead of once per axis, each with the
+// expressions and order of eigen(), so the speeds are eigen()'s bit for bit.
+template <typename T>
+PDM1_HD void max_abs_speeds3(T phi, T jx, T jy, T jz, T a[3]) {
+    const T iso = T(1) / sqrt(T(3));
+    const T jn = sqrt(jx * jx + jy * jy + jz * jz);
+    if (phi < T(kEigEps)) phi = T(kEigEps);
+    if (jn < T(kEigEps)) {
+        a[0] = a[1] = a[2] = iso;
+        return;
+    }
+    T f = jn / phi;
+    if (f < T(0)) f = T(0);
+    else if (f > T(1.0 - kEigEps)) f = T(1.0 - kEigEps);
+    const T chi = (T(5) - T(2) * sqrt(T(4) - T(3) * f * f)) / T(3);
+    const T den = T(5) - T(3) * chi;
+    const T j[3] = {jx, jy, jz};
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        T mu = j[ax] / jn;
+        T disc = T(4) * f * f * mu * mu - den * (mu * mu * (T(3) * chi - T(1)) - T(2) * (T(1) - chi));
+        if (disc < T(0)) disc = T(0);
+        T root = sqrt(disc);
+        T lo = fabs((T(2) * f * mu - root) / den), hi = fabs((T(2) * f * mu + root) / den);
+        a[ax] = lo > hi ? lo : hi;
+    }
+}
+
 template <typename T>
 PDM1_HD T max_abs_speed(T phi, T jx, T jy, T jz, int axis) {
     T jn = sqrt(jx * jx + jy * jy + jz * jz);

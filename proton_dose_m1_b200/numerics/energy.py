@@ -512,6 +512,22 @@ class FieldPlan:
         steps = self.march_device(dose, max_steps)
         return dose, steps
 
+    def march_steps(self, steps, max_steps=2_000_000):
+        """The first ``steps`` energy steps of every beam (one wave only):
+        the field dose of that prefix; ``last_info`` holds its statistics."""
+        torch = _torch()
+        if len(self.waves) != 1 or 0 not in self._plans:
+            raise ValueError("march_steps needs a field that fits one wave")
+        h = self._plans[0]
+        _apply_tile(self.config, h, self.shape, len(self.waves[0]))
+        dose = torch.empty(self.shape, dtype=torch.float64, device="cuda")
+        info = _native.MarchInfo()
+        _native.check(_native.lib().pdm1_march_steps(
+            h, None, C.c_void_p(dose.data_ptr()), None, int(max_steps), int(steps), C.byref(info),
+            C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        self.last_info = info
+        return dose
+
 
 _STAGING: dict = {}          # device index -> page-locked uint8 tensor
 _STAGING_LOCK = threading.Lock()
