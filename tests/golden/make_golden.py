@@ -408,6 +408,52 @@ def published_schedules(ps, groups):
         np.savez_compressed(out_file, **out)
 
 
+# The first three benchmark configurations, run with the unmodified reference:
+#   cfg1  40x40x200 @1 mm water, 150 MeV, sigma 3 mm, CSDA only, full domain;
+#   cfg2  80x80x400 @0.5 mm water + 2 cm bone slab at 8 cm, full physics, moving box;
+#   cfg3  80x80x400 @0.5 mm, bone for x > 0, full physics, moving box.
+# (sigma_E 1 MeV: the reference rejects 0; IF-SSPRK3, cfl 0.9, max dE 0.5.)
+BASELINE_CASES = {
+    "cfg1_static": dict(size=(0.04, 0.04, 0.2), resolution=(40, 40, 200), objects=[], physics={},
+                        moving=False),
+    "cfg2_moving": dict(size=(0.04, 0.04, 0.2), resolution=(80, 80, 400),
+                        objects=[(-0.02, 0.02, -0.02, 0.02, 0.08, 0.10, "BONE_COMPACT")],
+                        physics={"scattering": "WENTZEL", "nuclear": True}, moving=True),
+    "cfg3_moving": dict(size=(0.04, 0.04, 0.2), resolution=(80, 80, 400),
+                        objects=[(0.0, 0.02, -0.02, 0.02, 0.0, 0.2, "BONE_COMPACT")],
+                        physics={"scattering": "WENTZEL", "nuclear": True}, moving=True),
+}
+
+
+def baseline_marches(ps):
+    """Energies, maximum dose and depth-dose curve of the reference's own march of
+    the BASELINE_CASES (baseline_marches.npz + baseline_marches.json).  Cases
+    already in the file are kept."""
+    out_file = OUT / "baseline_marches.npz"
+    out = dict(np.load(out_file)) if out_file.exists() else {}
+    for name, c in BASELINE_CASES.items():
+        if f"{name}/energies" in out:
+            continue
+        objects = [ps.Box(*o[:6], ps.Material[o[6]]) for o in c["objects"]]
+        phys = ps.Physics(**{k: (ps.Scattering[v] if k == "scattering" else v) for k, v in c["physics"].items()})
+        cfg = ps.SolverConfig(
+            geometry=ps.Geometry(size=c["size"], resolution=c["resolution"], objects=objects),
+            beam=ps.Beam(n_protons=1e6, energy=150.0, energy_spread=1.0, sigma=(0.003, 0.003)),
+            physics=phys,
+            numerics=ps.Numerics(energy_scheme=ps.EnergyScheme.IF_SSPRK3, cfl=0.9, max_energy_step=0.5,
+                                 moving_active_domain=c["moving"]),
+            backend=ps.Backend.CPU, references=ps.References(reference=ps.Reference.NONE))
+        r = ps.Solver(cfg).solve()
+        out[f"{name}/energies"] = np.asarray(r.energies, dtype=np.float64)
+        out[f"{name}/max_dose"] = np.float64(r.dose.max())
+        out[f"{name}/depth_dose"] = np.asarray(r.dose.sum(axis=(0, 1)), dtype=np.float64)
+        out[f"{name}/runtime_s"] = np.float64(r.runtime)
+        print(name, len(r.energies) - 1, float(r.dose.max()), r.runtime, flush=True)
+        np.savez_compressed(out_file, **out)
+    (OUT / "baseline_marches.json").write_text(json.dumps(
+        {k: {**v, "objects": [list(o) for o in v["objects"]]} for k, v in BASELINE_CASES.items()}, indent=1))
+
+
 def published_configs(root: Path):
     """The canonical configurations and their hashes from the reference's own
     run directories (config.json, metadata.json of thesis_results/)."""
@@ -422,7 +468,7 @@ def published_configs(root: Path):
 
 if __name__ == "__main__":
     if len(sys.argv) < 2:
-        sys.exit("usage: make_golden.py <reference root> [configs|published|schedules [groups]|schemes|analytical]")
+        sys.exit("usage: make_golden.py <reference root> [configs|published|schedules [groups]|baseline|schemes|analytical]")
     root = Path(sys.argv[1])
     if len(sys.argv) > 2 and sys.argv[2] == "configs":
         published_configs(root)
@@ -432,6 +478,9 @@ if __name__ == "__main__":
         published_full(root)
         sys.exit(0)
     ps = import_reference(root)
+    if len(sys.argv) > 2 and sys.argv[2] == "baseline":
+        baseline_marches(ps)
+        sys.exit(0)
     if len(sys.argv) > 2 and sys.argv[2] == "schedules":
         published_schedules(ps, sys.argv[3].split(",") if len(sys.argv) > 3 else ["coarse_grid_1mm"])
         sys.exit(0)
