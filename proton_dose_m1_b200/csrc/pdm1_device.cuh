@@ -228,7 +228,8 @@ constexpr int NT = 256;   // threads of a stage CTA = cells of a tile
 // one arm.
 template <int X, int Y, int Z>
 struct Tile {
-    static_assert(X * Y * Z == NT, "one cell per thread");
+    static constexpr int NT = X * Y * Z;   // threads of the CTA: one cell each
+    static_assert(NT == 256 || NT == 512, "256- or 512-cell tiles");
     static constexpr int TX = X, TY = Y, TZ = Z;
     static constexpr int NFX = (X + 1) * Y * Z, NFY = X * (Y + 1) * Z, NFZ = X * Y * (Z + 1);
     static constexpr int NF = NFX + NFY + NFZ;
@@ -243,11 +244,12 @@ struct Tile {
 };
 
 // The tile shapes the stage kernels are built for, the autotuner's candidates.
-constexpr int kNumTiles = 3;
+constexpr int kNumTiles = 4;
 using Tile0 = Tile<4, 8, 8>;
 using Tile1 = Tile<8, 8, 4>;
 using Tile2 = Tile<2, 8, 16>;
-constexpr TileDims kTiles[kNumTiles] = {{4, 8, 8}, {8, 8, 4}, {2, 8, 16}};
+using Tile3 = Tile<8, 8, 8>;   // 512 cells: 3.375 faces per cell against 3.5-3.7
+constexpr TileDims kTiles[kNumTiles] = {{4, 8, 8}, {8, 8, 4}, {2, 8, 16}, {8, 8, 8}};
 constexpr int kMaxTileZ = 16;
 
 __host__ __device__ inline DomainDev make_domain(int i0, int j0, int k0, int nx, int ny, int nz, int inflow,
@@ -384,16 +386,17 @@ __device__ __forceinline__ double cfl_term(const ConfigDev &cf, double rf, const
     return a0 / (s * cf.dx) + a1 / (s * cf.dy) + a2 / (s * cf.dz);
 }
 
+template <int THREADS = NT>
 __device__ __forceinline__ void block_max_atomic(double v, unsigned long long *target) {
     // v >= 0 or NaN; NaN never wins (fmax), like the oracle's comparison loop
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-    __shared__ double wmax[NT / 32];
+    __shared__ double wmax[THREADS / 32];
     int w = threadIdx.x >> 5, l = threadIdx.x & 31;
     __syncthreads();
     if (l == 0) wmax[w] = v;
     __syncthreads();
     if (w == 0) {
-        v = l < NT / 32 ? wmax[l] : 0.0;
+        v = l < THREADS / 32 ? wmax[l] : 0.0;
         for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
         if (l == 0 && v > 0.0) atomicMax(target, (unsigned long long)__double_as_longlong(v));
     }
@@ -447,8 +450,9 @@ __device__ __forceinline__ unsigned long long *beam_slab(const ConfigDev &cf, in
 // Learned box: one tile's contribution to the beam's fluence moments, face
 // currents and z-plane currents (acc, plane) from the state u of each cell
 // (cell (li, lj, lk) of domain d, `valid` inside it).  Called by every thread
-// of a CTA of NT threads laid out as the stage tile (k fastest); `part` and
-// `pl` are shared scratch of NT/32 x (ACC_MAX + 1) and kMaxTileZ doubles.
+// of a CTA of THREADS threads laid out as the stage tile (k fastest); `part` and
+// `pl` are shared scratch of THREADS/32 x (ACC_MAX + 1) and kMaxTileZ doubles.
+template <int THREADS = NT>
 __device__ __forceinline__ void tile_moments_cta(const ConfigDev &cf, int b, const DomainDev &d, int k0,
                                                  bool valid, int li, int lj, int lk, const double u[4],
                                                  double (*part)[ACC_MAX + 1], double *pl) {
@@ -487,11 +491,11 @@ __device__ __forceinline__ void tile_moments_cta(const ConfigDev &cf, int b, con
     double *acc = cf.acc + (size_t)b * kAcc;
     if (tid < kSums) {
         double s = 0.0;
-        for (int w = 0; w < NT / 32; ++w) s += part[w][tid];
+        for (int w = 0; w < THREADS / 32; ++w) s += part[w][tid];
         if (s != 0.0) atomicAdd(&acc[tid], s);
     } else if (tid == kSums) {
         double m = 0.0;
-        for (int w = 0; w < NT / 32; ++w) m = fmax(m, part[w][kSums]);
+        for (int w = 0; w < THREADS / 32; ++w) m = fmax(m, part[w][kSums]);
         atomic_max_double(reinterpret_cast<unsigned long long *>(&acc[ACC_MAX]), m);
     } else if (tid >= 32 && tid < 32 + d.tz) {
         const int k = tid - 32;

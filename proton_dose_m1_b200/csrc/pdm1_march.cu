@@ -760,6 +760,7 @@ struct pdm1_plan {
     double *d_acc = nullptr;         // nbeams x kAcc
     double *d_plane = nullptr;       // nbeams x nz
     size_t workspace = 0;
+    int sms = 148;                   // SMs of the plan's device (stage grid sizing)
     std::vector<BeamDev> h_beams;   // host copy (device spatial pointers)
     // per material: [lo, hi] of the stopping-power, transport, nuclear tables
     std::vector<double> range[3][2];
@@ -898,13 +899,14 @@ int cell_blocks(const pdm1_plan *pl) {
 template <class Tl>
 void launch_stage64(int mode, int grid, const StageArgs &a, cudaStream_t stream) {
     const size_t bytes = Tl::template smem_bytes<double>();
+    constexpr int nt = Tl::NT;
     switch (mode) {
-    case MODE_A: stage_kernel<double, MODE_A, Tl><<<grid, NT, bytes, stream>>>(a); break;
-    case MODE_B: stage_kernel<double, MODE_B, Tl><<<grid, NT, bytes, stream>>>(a); break;
-    case MODE_C: stage_kernel<double, MODE_C, Tl><<<grid, NT, bytes, stream>>>(a); break;
-    case MODE_C_LEARN: stage_kernel<double, MODE_C, Tl, true><<<grid, NT, bytes, stream>>>(a); break;
-    case MODE_EULER: stage_kernel<double, MODE_EULER, Tl><<<grid, NT, bytes, stream>>>(a); break;
-    default: stage_kernel<double, MODE_RHS, Tl><<<grid, NT, bytes, stream>>>(a); break;
+    case MODE_A: stage_kernel<double, MODE_A, Tl><<<grid, nt, bytes, stream>>>(a); break;
+    case MODE_B: stage_kernel<double, MODE_B, Tl><<<grid, nt, bytes, stream>>>(a); break;
+    case MODE_C: stage_kernel<double, MODE_C, Tl><<<grid, nt, bytes, stream>>>(a); break;
+    case MODE_C_LEARN: stage_kernel<double, MODE_C, Tl, true><<<grid, nt, bytes, stream>>>(a); break;
+    case MODE_EULER: stage_kernel<double, MODE_EULER, Tl><<<grid, nt, bytes, stream>>>(a); break;
+    default: stage_kernel<double, MODE_RHS, Tl><<<grid, nt, bytes, stream>>>(a); break;
     }
 }
 
@@ -918,6 +920,7 @@ void launch_stage(const pdm1_plan *pl, int mode, int grid, const StageArgs &a, c
     switch (pl->cf.tile_id) {
     case 1: launch_stage64<Tile1>(mode, grid, a, stream); break;
     case 2: launch_stage64<Tile2>(mode, grid, a, stream); break;
+    case 3: launch_stage64<Tile3>(mode, grid, a, stream); break;
     default: launch_stage64<Tile0>(mode, grid, a, stream); break;
     }
 }
@@ -1004,6 +1007,7 @@ int set_smem_attributes() {
     CUDA_TRY(set_attributes64<Tile0>());
     CUDA_TRY(set_attributes64<Tile1>());
     CUDA_TRY(set_attributes64<Tile2>());
+    CUDA_TRY(set_attributes64<Tile3>());
     CUDA_TRY((cudaError_t)stage_fp32_set_attributes());
     done = true;
     return PDM1_OK;
@@ -1074,6 +1078,17 @@ void destroy_plan(pdm1_plan *pl) {
         if (e) cudaEventDestroy(e);
     if (pl->own_stream) cudaStreamDestroy(pl->own_stream);
     delete pl;
+}
+
+// Persistent grid of the stage kernels: resident CTAs per SM x SMs, capped by
+// the tiles of the full grid.  256-cell tiles: 2 CTAs per SM in double, 4 in
+// float (64 registers; 4 x 256 threads hide more of the MUFU and shared-memory
+// latency than 3 x 256 at 80 registers: -4 % stage time on field256); a
+// 512-cell tile holds half as many CTAs.
+int stage_grid(const pdm1_problem &p, TileDims t, int nbeams, int sms) {
+    const int per_sm = (p.precision == PDM1_FP32_FP64 ? 4 : 2) * 256 / (t.x * t.y * t.z);
+    size_t tiles = (size_t)make_domain(0, 0, 0, p.nx, p.ny, p.nz, 1, t).ntiles * nbeams;
+    return (int)std::max<size_t>(1, std::min<size_t>(tiles, (size_t)std::max(1, per_sm) * sms));
 }
 
 // A plan for `nbeams` beams on one phantom; every beam's buffers hold `cap` cells.
@@ -1223,9 +1238,8 @@ int create_plan(const pdm1_problem *problem, const pdm1_beam *beams, int nbeams,
         // resident CTAs per SM of the stage kernel: 2 in double, 4 in float
         // (64 registers; 4 x 256 threads hide more of the MUFU and shared-memory
         // latency than 3 x 256 at 80 registers: -4 % stage time on field256)
-        int per_sm = p.precision == PDM1_FP32_FP64 ? 4 : 2;
-        size_t tiles = (size_t)make_domain(0, 0, 0, p.nx, p.ny, p.nz, 1, cf.tile).ntiles * B;
-        cf.grid_ctas = (int)std::max<size_t>(1, std::min<size_t>(tiles, (size_t)per_sm * sms));
+        pl->sms = sms;
+        cf.grid_ctas = stage_grid(p, cf.tile, B, sms);
     }
     bool ok = cudaMemcpy(pl->d_tables, blob.data(), blob.size() * sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess &&
               cudaMemcpy(pl->d_ids, problem->ids, N * sizeof(int32_t), cudaMemcpyHostToDevice) == cudaSuccess &&
@@ -1451,6 +1465,7 @@ int pdm1_plan_set_tile(pdm1_plan *pl, int tile_id) {
     const TileDims t = kTiles[tile_id];
     pl->cf.tile = t;
     pl->cf.tile_id = tile_id;
+    pl->cf.grid_ctas = stage_grid(pl->p, t, pl->nbeams, pl->sms);
     for (BeamDev &bd : pl->h_beams) {
         const DomainDev &o = bd.init_box;
         bd.init_box = make_domain(o.i0, o.j0, o.k0, o.nx, o.ny, o.nz, o.inflow, t);

@@ -85,7 +85,7 @@ __device__ __forceinline__ void bulk_stage_tile(const float4 *src, const DomainD
     // shared memory read or written by the threads before (the last tile) is
     // overwritten by the async proxy next
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    for (int r = threadIdx.x; r < RX + RY + RZ; r += NT) {
+    for (int r = threadIdx.x; r < RX + RY + RZ; r += Tl::NT) {
         int li, lj, ka, kb, dst_e;
         float4 *arm;
         if (r < RX) {
@@ -131,7 +131,7 @@ __device__ __forceinline__ void patch_zmax(const DomainDev &d, int k0, float4 *Z
     const int over = k0 + TZ + 3 - d.nz;   // cells of each z-arm row beyond nz
     if (over <= 0) return;
     const int last = d.nz - 1 - (k0 - 3);   // arm index of the domain's last z cell
-    for (int e = threadIdx.x; e < TX * TY * over; e += NT) {
+    for (int e = threadIdx.x; e < TX * TY * over; e += Tl::NT) {
         const int row = e / over, kk = last + 1 + e % over;
         Z[row * (TZ + 6) + kk] = Z[row * (TZ + 6) + last];
     }
@@ -140,7 +140,9 @@ __device__ __forceinline__ void patch_zmax(const DomainDev &d, int k0, float4 *Z
 // LEARN (stage C of a plan with a learned box): the tile's fluence moments of
 // the new state are accumulated for the next step's proposer.
 template <typename T, int MODE, class Tl, bool LEARN = false>
-__global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 4) stage_kernel(StageArgs a) {
+__global__ void __launch_bounds__(Tl::NT, (sizeof(T) == sizeof(double) ? 2 : 4) * 256 / Tl::NT)
+    stage_kernel(StageArgs a) {
+    constexpr int NT = Tl::NT;   // threads of this tile shape (one cell each)
     constexpr int TX = Tl::TX, TY = Tl::TY, TZ = Tl::TZ;
     constexpr int NF = Tl::NF, NFX = Tl::NFX, NFY = Tl::NFY;
     constexpr int SX = Tl::SX, SY = Tl::SY, SZ = Tl::SZ;
@@ -539,11 +541,11 @@ __global__ void __launch_bounds__(NT, sizeof(T) == sizeof(double) ? 2 : 4) stage
             // learned box: the moments of the new state feed the next step's proposer
             __shared__ double mom_part[NT / 32][ACC_MAX + 1];
             __shared__ double mom_pl[kMaxTileZ];
-            tile_moments_cta(cf, b, d, k0, valid, li, lj, lk, um, mom_part, mom_pl);
+            tile_moments_cta<NT>(cf, b, d, k0, valid, li, lj, lk, um, mom_part, mom_pl);
         }
         __syncthreads();   // shared memory is reused by the next tile
     }
-    if (MODE == MODE_C && !cf.moving) block_max_atomic(cta_inv, &a.st[0].inv_bits);
+    if (MODE == MODE_C && !cf.moving) block_max_atomic<NT>(cta_inv, &a.st[0].inv_bits);
 }
 
 }  // namespace pdm1

@@ -28,13 +28,14 @@ cudaError_t set_attributes() {
 template <class Tl>
 void launch(int mode, int grid, const StageArgs &a, cudaStream_t stream) {
     const size_t bytes = Tl::template smem_bytes<float>();
+    constexpr int nt = Tl::NT;
     switch (mode) {
-    case MODE_A: stage_kernel<float, MODE_A, Tl><<<grid, NT, bytes, stream>>>(a); break;
-    case MODE_B: stage_kernel<float, MODE_B, Tl><<<grid, NT, bytes, stream>>>(a); break;
-    case MODE_C: stage_kernel<float, MODE_C, Tl><<<grid, NT, bytes, stream>>>(a); break;
-    case MODE_C_LEARN: stage_kernel<float, MODE_C, Tl, true><<<grid, NT, bytes, stream>>>(a); break;
-    case MODE_EULER: stage_kernel<float, MODE_EULER, Tl><<<grid, NT, bytes, stream>>>(a); break;
-    default: stage_kernel<float, MODE_RHS, Tl><<<grid, NT, bytes, stream>>>(a); break;
+    case MODE_A: stage_kernel<float, MODE_A, Tl><<<grid, nt, bytes, stream>>>(a); break;
+    case MODE_B: stage_kernel<float, MODE_B, Tl><<<grid, nt, bytes, stream>>>(a); break;
+    case MODE_C: stage_kernel<float, MODE_C, Tl><<<grid, nt, bytes, stream>>>(a); break;
+    case MODE_C_LEARN: stage_kernel<float, MODE_C, Tl, true><<<grid, nt, bytes, stream>>>(a); break;
+    case MODE_EULER: stage_kernel<float, MODE_EULER, Tl><<<grid, nt, bytes, stream>>>(a); break;
+    default: stage_kernel<float, MODE_RHS, Tl><<<grid, nt, bytes, stream>>>(a); break;
     }
 }
 
@@ -44,6 +45,7 @@ int stage_fp32_set_attributes() {
     cudaError_t e = set_attributes<Tile0>();
     if (e == cudaSuccess) e = set_attributes<Tile1>();
     if (e == cudaSuccess) e = set_attributes<Tile2>();
+    if (e == cudaSuccess) e = set_attributes<Tile3>();
     return (int)e;
 }
 
@@ -51,6 +53,7 @@ void launch_stage_fp32(int mode, int tile_id, int grid, const StageArgs &a, cuda
     switch (tile_id) {
     case 1: launch<Tile1>(mode, grid, a, stream); break;
     case 2: launch<Tile2>(mode, grid, a, stream); break;
+    case 3: launch<Tile3>(mode, grid, a, stream); break;
     default: launch<Tile0>(mode, grid, a, stream); break;
     }
 }

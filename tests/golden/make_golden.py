@@ -429,6 +429,8 @@ def baseline_marches(ps):
     """Energies, maximum dose and depth-dose curve of the reference's own march of
     the BASELINE_CASES (baseline_marches.npz + baseline_marches.json).  Cases
     already in the file are kept."""
+    (OUT / "baseline_marches.json").write_text(json.dumps(
+        {k: {**v, "objects": [list(o) for o in v["objects"]]} for k, v in BASELINE_CASES.items()}, indent=1))
     out_file = OUT / "baseline_marches.npz"
     out = dict(np.load(out_file)) if out_file.exists() else {}
     for name, c in BASELINE_CASES.items():
@@ -450,8 +452,6 @@ def baseline_marches(ps):
         out[f"{name}/runtime_s"] = np.float64(r.runtime)
         print(name, len(r.energies) - 1, float(r.dose.max()), r.runtime, flush=True)
         np.savez_compressed(out_file, **out)
-    (OUT / "baseline_marches.json").write_text(json.dumps(
-        {k: {**v, "objects": [list(o) for o in v["objects"]]} for k, v in BASELINE_CASES.items()}, indent=1))
 
 
 def published_configs(root: Path):

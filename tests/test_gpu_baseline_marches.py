@@ -32,9 +32,9 @@ from tests import cases
 
 pytestmark = pytest.mark.gpu
 
-_FILE = cases.GOLDEN / "baseline_marches.npz"
-MARCHES = dict(np.load(_FILE)) if _FILE.exists() else {}
-SPECS = json.loads((cases.GOLDEN / "baseline_marches.json").read_text()) if MARCHES else {}
+_FILE, _SPEC = cases.GOLDEN / "baseline_marches.npz", cases.GOLDEN / "baseline_marches.json"
+MARCHES = dict(np.load(_FILE)) if _FILE.exists() and _SPEC.exists() else {}
+SPECS = json.loads(_SPEC.read_text()) if MARCHES else {}
 NAMES = sorted(k.rsplit("/", 1)[0] for k in MARCHES if k.endswith("/energies"))
 
 
