@@ -240,15 +240,14 @@ int pdm1_plan_set_staging(pdm1_plan *plan, int bulk);
 
 /* ---- Tile shape of the stage kernels ---------------------------------------
  * No reference counterpart.  The fused stage kernels are built for
- * PDM1_NUM_TILES tile shapes, one cell per thread: 4x8x8 (the default), 8x8x4
- * and 2x8x16 of 256 cells, and 8x8x8 of 512 cells (x, y, z; z is the
- * contiguous axis; fewer halo faces per cell, half as many CTAs per SM).  The
+ * PDM1_NUM_TILES tile shapes of 256 cells (one per thread): 4x8x8 (the
+ * default), 8x8x4 and 2x8x16 (x, y, z; z is the contiguous axis).  The
  * autotuner marches the first `steps` energy steps of the plan's problem with
  * every shape (in scratch buffers it allocates; the plan's results are not
  * touched), measures the stage-kernel time per cell-step with CUDA events,
  * keeps the fastest shape for the plan and reports it in *best_tile and the
  * measurements in ns_per_cell_step (host, PDM1_NUM_TILES, may be NULL). */
-#define PDM1_NUM_TILES 4
+#define PDM1_NUM_TILES 3
 int pdm1_tile_shape(int tile_id, int *tx, int *ty, int *tz);
 int pdm1_plan_set_tile(pdm1_plan *plan, int tile_id);
 int pdm1_plan_autotune(pdm1_plan *plan, int steps, int *best_tile, double *ns_per_cell_step,

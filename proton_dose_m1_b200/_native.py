@@ -151,4 +151,4 @@ EXPORTED_SYMBOLS = (
     "pdm1_pool_cached_bytes", "pdm1_pool_release", "pdm1_plan_set_staging",
     "pdm1_plan_set_schedule",
 )
-NUM_TILES = 4
+NUM_TILES = 3

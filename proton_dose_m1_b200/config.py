@@ -106,7 +106,7 @@ class OutputConfig:
     store_final_state: bool = True
 
 
-TILE_SHAPES = ((4, 8, 8), (8, 8, 4), (2, 8, 16), (8, 8, 8))
+TILE_SHAPES = ((4, 8, 8), (8, 8, 4), (2, 8, 16))
 
 
 @dataclass(frozen=True)

@@ -246,12 +246,14 @@ struct Tile {
 };
 
 // The tile shapes the stage kernels are built for, the autotuner's candidates.
-constexpr int kNumTiles = 4;
+// (An 8x8x8 tile of 512 threads, 3.375 faces per cell against 3.5-3.7, was
+// measured slower: 0.674 against 0.606 ns per cell-step on a 51-spot pelvis batch
+// in the FP32 form, with half as many CTAs per SM and twice the warps per barrier.)
+constexpr int kNumTiles = 3;
 using Tile0 = Tile<4, 8, 8>;
 using Tile1 = Tile<8, 8, 4>;
 using Tile2 = Tile<2, 8, 16>;
-using Tile3 = Tile<8, 8, 8>;   // 512 cells: 3.375 faces per cell against 3.5-3.7
-constexpr TileDims kTiles[kNumTiles] = {{4, 8, 8}, {8, 8, 4}, {2, 8, 16}, {8, 8, 8}};
+constexpr TileDims kTiles[kNumTiles] = {{4, 8, 8}, {8, 8, 4}, {2, 8, 16}};
 constexpr int kMaxTileZ = 16;
 
 __host__ __device__ inline DomainDev make_domain(int i0, int j0, int k0, int nx, int ny, int nz, int inflow,

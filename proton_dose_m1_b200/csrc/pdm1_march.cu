@@ -909,7 +909,10 @@ StageArgs make_args(pdm1_plan *pl, double *dose, double *edep, double *snap) {
 // blocks of the per-cell kernels, per beam: enough for the largest domain
 int cell_blocks(const pdm1_plan *pl) {
     size_t b = (pl->cap + NT - 1) / NT;
-    return (int)std::max<size_t>(1, std::min<size_t>(b, pl->nbeams > 1 ? 64 : 148 * 8));
+    // about 8 CTAs per SM over all beams (at least 64 per beam): these kernels are
+    // latency-bound on loads and dependent FP64 arithmetic and want every warp
+    const size_t per = pl->nbeams > 1 ? std::max<size_t>(64, (size_t)148 * 8 / pl->nbeams) : (size_t)148 * 8;
+    return (int)std::max<size_t>(1, std::min<size_t>(b, per));
 }
 
 template <class Tl>
@@ -936,7 +939,6 @@ void launch_stage(const pdm1_plan *pl, int mode, int grid, const StageArgs &a, c
     switch (pl->cf.tile_id) {
     case 1: launch_stage64<Tile1>(mode, grid, a, stream); break;
     case 2: launch_stage64<Tile2>(mode, grid, a, stream); break;
-    case 3: launch_stage64<Tile3>(mode, grid, a, stream); break;
     default: launch_stage64<Tile0>(mode, grid, a, stream); break;
     }
 }
@@ -1023,7 +1025,6 @@ int set_smem_attributes() {
     CUDA_TRY(set_attributes64<Tile0>());
     CUDA_TRY(set_attributes64<Tile1>());
     CUDA_TRY(set_attributes64<Tile2>());
-    CUDA_TRY(set_attributes64<Tile3>());
     CUDA_TRY((cudaError_t)stage_fp32_set_attributes());
     done = true;
     return PDM1_OK;

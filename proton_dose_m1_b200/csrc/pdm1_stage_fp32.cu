@@ -45,7 +45,6 @@ int stage_fp32_set_attributes() {
     cudaError_t e = set_attributes<Tile0>();
     if (e == cudaSuccess) e = set_attributes<Tile1>();
     if (e == cudaSuccess) e = set_attributes<Tile2>();
-    if (e == cudaSuccess) e = set_attributes<Tile3>();
     return (int)e;
 }
 
@@ -53,7 +52,6 @@ void launch_stage_fp32(int mode, int tile_id, int grid, const StageArgs &a, cuda
     switch (tile_id) {
     case 1: launch<Tile1>(mode, grid, a, stream); break;
     case 2: launch<Tile2>(mode, grid, a, stream); break;
-    case 3: launch<Tile3>(mode, grid, a, stream); break;
     default: launch<Tile0>(mode, grid, a, stream); break;
     }
 }
