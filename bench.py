@@ -602,22 +602,25 @@ def run_field(args, rank, world, local_rank):
 
         gate = None
         plain_spots_per_s = None
-        if rank == 0 and args.gate_spots != 0:
-            # gate: a sample of the field's spots, accelerated (batched) vs the
-            # plain FP64 full-domain path one spot at a time
+        if args.gate_spots != 0:
+            # gate: a sample of the field's spots, accelerated (batched, rank 0)
+            # vs the plain FP64 full-domain path one spot at a time; over N
+            # ranks the plain marches go round-robin by energy, so every rank
+            # waits in the sums below for the others' last spot only
             sample = gate_sample(beams, args.gate_spots if args.gate_spots > 0
                                  else FIELDS[args.workload]["gate_beams"])
             sub = [beams[k] for k in sample]
-            sp = FieldPlan(run_cfg, mm, grid, sub)
-            dose_acc = torch.empty(grid.shape, dtype=torch.float64, device=dev)
-            sp.march_device(dose_acc)
-            sp.close()
+            dose_acc = torch.zeros(grid.shape, dtype=torch.float64, device=dev)
+            if rank == 0:
+                sp = FieldPlan(run_cfg, mm, grid, sub)
+                sp.march_device(dose_acc)
+                sp.close()
             dose_plain = torch.zeros_like(dose_acc)
             d1 = torch.empty_like(dose_acc)
             U = torch.empty((4, *grid.shape), dtype=torch.float64, device=dev)
             energies = torch.empty(200_001, dtype=torch.float64, device=dev)
             plain_ms = 0.0
-            for b in sub:
+            for b in sub[rank::world]:
                 pplan = M1Plan(static_config(cfg, b), mm, grid, BeamInflow.from_beam(b, grid))
                 U.zero_()
                 s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -629,7 +632,14 @@ def run_field(args, rank, world, local_rank):
                 dose_plain += d1
                 pplan.close()
             del U
+            if world > 1:
+                t = torch.tensor([plain_ms], dtype=torch.float64, device=dev)
+                dist.all_reduce(t)
+                plain_ms = float(t.item())
+                dist.all_reduce(dose_plain)
+            # one GPU's rate: the plain marches' summed device time
             plain_spots_per_s = len(sub) / (plain_ms / 1e3)
+        if rank == 0 and args.gate_spots != 0:
             score = metrics.compare(dose_acc, dose_plain, grid)
             gate = {"vs": f"plain FP64 GPU path (full domain, one spot at a time) on {len(sub)} spots "
                           f"of the field (energy quantiles: {[round(b.energy, 1) for b in sub]} MeV)",

@@ -101,7 +101,6 @@ struct ConfigDev {
     double *bufA, *bufB;        // compact-state ping-pong, 4*cap per beam
     unsigned long long *slab;   // max phi per x | y | z slab of the box (double bits), per beam
     unsigned char *active;      // vacuum-aware activity mask on the box, cap per beam
-    double *cflterm;            // moving box: each cell's CFL term from the last stage C, cap per beam
     int grid_ctas;              // persistent grid of the stage kernels
     TileDims tile;              // tile shape of the stage kernels (kTiles[tile_id])
     int tile_id;
@@ -153,7 +152,6 @@ struct MarchState {
     double *Ua;                    // state on `dom`
     double *Uprev;                 // state on `prev`
     int reboxed;
-    int terms_valid;               // cflterm holds the terms of the state on `dom` (before a rebox)
     unsigned long long newmax_bits;   // max phi over the new box (vacuum-aware CFL)
     double pin_max;                // max inflow phi over the new box
     double cell_steps;             // sum over steps of the cells marched (domain volume)

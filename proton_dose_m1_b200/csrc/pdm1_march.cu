@@ -84,7 +84,6 @@ __global__ void init_kernel(const ConfigDev *cfp, Coeffs *cos, MarchState *sts, 
         st->taken = 0;
         st->error = 0;
         st->reboxed = 0;
-        st->terms_valid = 0;
         st->newmax_bits = 0ull;
         st->pin_max = 0.0;
         st->cell_steps = 0.0;
@@ -566,7 +565,6 @@ __global__ void __launch_bounds__(NT) rebox_kernel(const ConfigDev *cfp, const C
     const DomainDev p = st->prev;
     const double *Up = st->Uprev;
     double *Ua = st->Ua;
-    const double *terms = cf.cflterm + (size_t)b * cf.cap;   // on `prev` (== `dom` without a move)
     const BeamDev &bm = cf.beams[b];
     const double *S = cos[b].S_cfl;
     const double ed = cos[b].ed_cfl;
@@ -593,20 +591,7 @@ __global__ void __launch_bounds__(NT) rebox_kernel(const ConfigDev *cfp, const C
             for (int c = 0; c < 4; ++c) u[c] = Ua[c * N + o];
         }
         m = fmax(m, u[0]);
-        if (with_cfl) {
-            // a cell that stage C marched: the term it computed from the same state
-            // and the same S; here the box's first z layer (whose z speeds join the
-            // inflow's, zero inflow for a box away from the entrance) and cells new
-            // to the box (zero state)
-            bool stored = st->terms_valid && lk != 0;
-            size_t so = o;
-            if (stored && moved) {
-                int pi = d.i0 + li - p.i0, pj = d.j0 + lj - p.j0, pk = d.k0 + lk - p.k0;
-                stored = pi >= 0 && pi < p.nx && pj >= 0 && pj < p.ny && pk >= 0 && pk < p.nz;
-                so = ((size_t)pi * p.ny + pj) * p.nz + pk;
-            }
-            inv = fmax(inv, stored ? terms[so] : cell_cfl(cf, bm, d, S, ed, u, li, lj, lk, all_axes));
-        }
+        if (with_cfl) inv = fmax(inv, cell_cfl(cf, bm, d, S, ed, u, li, lj, lk, all_axes));
     }
     if (cf.vacuum_aware) block_max_atomic(m, &st->newmax_bits);
     if (with_cfl) {
@@ -771,7 +756,6 @@ struct pdm1_plan {
     double *d_bufA = nullptr, *d_bufB = nullptr;   // moving box: compact-state ping-pong
     unsigned long long *d_slab = nullptr;
     unsigned char *d_active = nullptr;
-    double *d_cflterm = nullptr;     // moving box: per-cell CFL terms written by stage C
     BoxModelDev *d_model = nullptr;  // learned box
     double *d_acc = nullptr;         // nbeams x kAcc
     double *d_plane = nullptr;       // nbeams x nz
@@ -1087,7 +1071,6 @@ void destroy_plan(pdm1_plan *pl) {
     pool_free(pl->d_bufB);
     pool_free(pl->d_slab);
     pool_free(pl->d_active);
-    pool_free(pl->d_cflterm);
     pool_free(pl->d_model);
     pool_free(pl->d_acc);
     pool_free(pl->d_plane);
@@ -1205,10 +1188,9 @@ int create_plan(const pdm1_problem *problem, const pdm1_beam *beams, int nbeams,
         ALLOC(pl->d_bufA, B * 4 * cap * sizeof(double));
         ALLOC(pl->d_bufB, B * 4 * cap * sizeof(double));
         ALLOC(pl->d_active, B * cap);
-        ALLOC(pl->d_cflterm, B * cap * sizeof(double));
     }
 #undef ALLOC
-    pl->workspace = B * cap * ((p.moving_active_domain ? 22 : 13) * sizeof(double) + (p.moving_active_domain ? 1 : 0));
+    pl->workspace = B * cap * ((p.moving_active_domain ? 21 : 13) * sizeof(double) + (p.moving_active_domain ? 1 : 0));
     if (pool_malloc_host((void **)&pl->h_st, B * sizeof(MarchState)) != cudaSuccess ||
         pool_malloc_host((void **)&pl->h_sum, sizeof(MarchSummary)) != cudaSuccess ||
         cudaStreamCreateWithFlags(&pl->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
@@ -1245,7 +1227,6 @@ int create_plan(const pdm1_problem *problem, const pdm1_beam *beams, int nbeams,
     cf.bufB = pl->d_bufB;
     cf.slab = pl->d_slab;
     cf.active = pl->d_active;
-    cf.cflterm = pl->d_cflterm;
     cf.learned = 0;
     cf.model = nullptr;
     cf.acc = pl->d_acc;

@@ -526,13 +526,6 @@ __global__ void __launch_bounds__(Tl::NT, (sizeof(T) == sizeof(double) ? 2 : 4) 
                                 phi_in = bm.spatial[(size_t)(d.i0 + li) * cf.ny + (d.j0 + lj)] * co.ed_next;
                             double v = cfl_term<T>(cf, bm.rf, unew, co.S1[m], lk == 0, phi_in, all_axes);
                             cta_inv = fmax(cta_inv, v);
-                        } else if (!cf.vacuum_aware) {
-                            // the cell's CFL term for the next step's box move, with the
-                            // precision and S that rebox_kernel uses (S at the new energy;
-                            // the entrance layer is evaluated there with the inflow)
-                            cf.cflterm[boff + o] = cf.fp32 && !cf.cfl_floor
-                                                       ? cfl_term<float>(cf, bm.rf, unew, co.S1[m], false, 0.0, all_axes)
-                                                       : cfl_term<double>(cf, bm.rf, unew, co.S1[m], false, 0.0, all_axes);
                         }
                         phi_new = unew[0];
                     }
@@ -540,7 +533,6 @@ __global__ void __launch_bounds__(Tl::NT, (sizeof(T) == sizeof(double) ? 2 : 4) 
             }
         }
         if (MODE == MODE_C && cf.moving) {
-            if (tid == 0 && !cf.vacuum_aware) stb.terms_valid = 1;
             slab_buf[tid] = phi_new;
             __syncthreads();
             tile_slab_max(cf, beam_slab(cf, b), d, slab_buf, i0, j0, k0);

@@ -290,8 +290,8 @@ class M1Plan:
 
 # Device bytes per box cell of one beam in a field plan: U on the box (double
 # buffered), the two stage states, V (4 components each, double), the dose
-# quadrature part, the cell's CFL term, and the activity mask byte.
-FIELD_BYTES_PER_BOX_CELL = 22 * 8 + 1
+# quadrature part, and the activity mask byte.
+FIELD_BYTES_PER_BOX_CELL = 21 * 8 + 1
 
 
 def estimate_box_cells(config, grid, beam) -> int:
