@@ -36,6 +36,16 @@ FREE_STREAMING_DOSE_RTOL = 2e-9
 # coarse_grid/reduced_physics/transversal_slabs.  The full-size bar is 1e-7.
 FULL_SIZE_DOSE_RTOL = 1e-7
 
+# A material interface parallel to the beam (bone for x > 0 in 80x80x400 at
+# 0.5 mm) makes the fluence at a given energy jump across the beam, where
+# WENO-Z's nonlinear weights amplify rounding: through the same 853 energies,
+# two oracle builds differing only in FMA contraction end 6.0e-4 of the
+# maximum apart in some voxel and 3.4e-6 of its maximum apart in the
+# depth-dose curve (the reference run is 4.9e-4 / 2.4e-6 from the committed
+# build), while the maximum dose agrees to 2e-8.  On a z slab of the same
+# size the spread stays at the 1e-10 floor.  The depth-dose bar there is 1e-5.
+LATERAL_INTERFACE_DEPTH_DOSE_RTOL = 1e-5
+
 
 def reference_rtol(cfg) -> float:
     """The parity bar against the reference for configuration ``cfg``."""
