@@ -553,7 +553,10 @@ __global__ void __launch_bounds__(256) box_kernel(const ConfigDev *cfp, Coeffs *
 // moving_active_domain.py:196-232); for the vacuum-aware CFL also the max phi
 // of the new box.  With `with_cfl` (no vacuum-aware masks) the CFL bound of
 // the new box as cfl_kernel computes it, from the values in registers.
-__global__ void __launch_bounds__(NT) rebox_kernel(const ConfigDev *cfp, const Coeffs *cos, MarchState *sts,
+// Four CTAs per SM (64 registers, a few spilled to L1): the kernel waits on
+// loads and dependent FP64 arithmetic, and at its natural 89 registers only two
+// CTAs fit (25 % of the warp slots).
+__global__ void __launch_bounds__(NT, 4) rebox_kernel(const ConfigDev *cfp, const Coeffs *cos, MarchState *sts,
                                                    int with_cfl) {
     const ConfigDev &cf = *cfp;
     const int b = blockIdx.y;
