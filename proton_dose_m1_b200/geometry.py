@@ -37,6 +37,48 @@ class Box:
             raise ValueError("Box minima must be smaller than maxima.")
 
 
+def _check_ct_orientation(spacing, axis_order, flip_axes) -> None:
+    """A CT's voxel spacing (three positive metres), axis permutation and
+    per-axis flips, as the reference validates them."""
+    if len(spacing) != 3 or not all(math.isfinite(s) and s > 0 for s in spacing):
+        raise ValueError("CT spacing must contain three positive finite metres.")
+    if sorted(axis_order) != [0, 1, 2]:
+        raise ValueError("axis_order must be a permutation of (0, 1, 2).")
+    if len(flip_axes) != 3 or not all(type(f) is bool for f in flip_axes):
+        raise ValueError("flip_axes must contain three booleans.")
+
+
+def _read_ct_npz(path) -> tuple[np.ndarray, np.ndarray | None]:
+    """(HU volume, body mask or None) of a CT stored as NPZ.
+
+    The volume is the array named ``HU``, else ``hu``, else the only array of
+    a file that holds one unnamed array (NumPy stores those as ``arr_0``); an
+    optional boolean ``body_mask`` of the same shape marks the patient.  The
+    volume must be numeric, three-dimensional and finite."""
+    with np.load(path, allow_pickle=False) as npz:
+        names = list(npz.files)
+        key = next((k for k in ("HU", "hu") if k in names), "arr_0" if names == ["arr_0"] else None)
+        if key is None:
+            raise ValueError("CT NPZ needs a 'HU', 'hu', or single 'arr_0' array.")
+        hu = np.asarray(npz[key])
+        mask = np.asarray(npz["body_mask"]) if "body_mask" in names else None
+    if hu.ndim != 3 or not np.issubdtype(hu.dtype, np.number):
+        raise ValueError("CT HU must be a numeric 3D array.")
+    if not np.isfinite(hu).all():
+        raise ValueError("CT HU contains non-finite values.")
+    if mask is not None and mask.shape != hu.shape:
+        raise ValueError("body_mask shape must match the HU array.")
+    return hu, mask
+
+
+def _orient(volume: np.ndarray, axis_order, flip_axes) -> np.ndarray:
+    """``volume`` with its axes taken in ``axis_order`` (solver axis i is
+    source axis ``axis_order[i]``), then the solver axes marked in
+    ``flip_axes`` reversed; one strided view, copied once to C order."""
+    reverse = tuple(slice(None, None, -1) if f else slice(None) for f in flip_axes)
+    return np.ascontiguousarray(volume.transpose(axis_order)[reverse])
+
+
 @dataclass(frozen=True)
 class HUPartition:
     """Map HU values to transport materials with half-open bins."""
@@ -77,38 +119,16 @@ class CTScan:
     spacing: tuple[float, float, float] = field(init=False)
 
     def __post_init__(self):
-        if len(self.source_spacing_m) != 3 or not all(
-                math.isfinite(s) and s > 0 for s in self.source_spacing_m):
-            raise ValueError("CT spacing must contain three positive finite metres.")
-        if tuple(sorted(self.axis_order)) != (0, 1, 2):
-            raise ValueError("axis_order must be a permutation of (0, 1, 2).")
-        if len(self.flip_axes) != 3 or any(type(f) is not bool for f in self.flip_axes):
-            raise ValueError("flip_axes must contain three booleans.")
-        with np.load(self.path, allow_pickle=False) as data:
-            key = "HU" if "HU" in data else "hu" if "hu" in data else None
-            if key is None and data.files == ["arr_0"]:
-                key = "arr_0"
-            if key is None:
-                raise ValueError("CT NPZ needs a 'HU', 'hu', or single 'arr_0' array.")
-            hu = np.asarray(data[key])
-            mask = np.asarray(data["body_mask"]) if "body_mask" in data else None
-        if hu.ndim != 3 or not np.issubdtype(hu.dtype, np.number):
-            raise ValueError("CT HU must be a numeric 3D array.")
-        if not np.all(np.isfinite(hu)):
-            raise ValueError("CT HU contains non-finite values.")
-        if mask is not None and mask.shape != hu.shape:
-            raise ValueError("body_mask shape must match the HU array.")
-        hu = np.transpose(hu, self.axis_order)
-        if mask is not None:
-            mask = np.transpose(mask.astype(bool), self.axis_order)
-        for axis, flip in enumerate(self.flip_axes):
-            if flip:
-                hu = np.flip(hu, axis=axis)
-                if mask is not None:
-                    mask = np.flip(mask, axis=axis)
-        object.__setattr__(self, "hu", np.ascontiguousarray(hu))
-        object.__setattr__(self, "body_mask", None if mask is None else np.ascontiguousarray(mask))
-        object.__setattr__(self, "spacing", tuple(self.source_spacing_m[i] for i in self.axis_order))
+        # The orientation is checked before the file is opened, the volume
+        # after it; the messages are the reference's, in its order
+        # (proton_solver/geometry.py:91-130), so a bad configuration raises the
+        # same error under either library.
+        _check_ct_orientation(self.source_spacing_m, self.axis_order, self.flip_axes)
+        hu, mask = _read_ct_npz(self.path)
+        set_ = object.__setattr__
+        set_(self, "hu", _orient(hu, self.axis_order, self.flip_axes))
+        set_(self, "body_mask", None if mask is None else _orient(mask.astype(bool), self.axis_order, self.flip_axes))
+        set_(self, "spacing", tuple(self.source_spacing_m[a] for a in self.axis_order))
 
     @property
     def shape(self) -> tuple[int, int, int]:
