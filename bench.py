@@ -14,8 +14,10 @@ the plain FP64 full-domain GPU march (gamma 1%/1 mm, max dose).
 Single-spot workloads (slab80, water40): a step is one complete march of
 the spot.
 
-``--impl reference`` times the CPU restatement of the reference algorithm
-(oracle/) on the host cores: one complete moving-box spot march per step.
+``--impl reference`` times the reference's own CPU path on the host cores:
+one complete moving-box spot march per step, through the unmodified
+reference's Numba energy_march where baseline/install_reference.sh installed
+it under baseline/_ref, else through the CPU restatement (oracle/).
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
        [--workload pelvis1024|field256|slab80|water40] [--box heuristic|learned]
@@ -306,13 +308,149 @@ def cpu_baseline(workload_name: str, n: int = 2):
                       f"{wall:.1f} s, {workers} at a time x {tpw} OpenMP threads"}
 
 
+# The unmodified reference, installed by baseline/install_reference.sh: the
+# package under lib/ and its material tables under data/, where the package's
+# own path lookups (physics/materials.py:13 and its siblings: three directories
+# above the module) find them.
+REF_LIB = ROOT / "baseline" / "_ref" / "lib"
+# Numba threads per reference worker process: the reference's parallel loops
+# scale poorly past ~4 threads (a 89.5 MeV pelvis spot: 18.9 s on 4 threads,
+# 16.9 s on 8), so several spots at once on 4 threads each use the cores better.
+REF_THREADS_PER_WORKER = 4
+
+
+def reference_installed() -> bool:
+    import importlib.util
+    return ((REF_LIB / "proton_solver" / "__init__.py").exists()
+            and (REF_LIB.parent / "data" / "materials.csv").exists()
+            and importlib.util.find_spec("numba") is not None)
+
+
+def import_installed_reference():
+    """Import the installed reference.  Its package imports plotting and
+    gamma-index modules at import time that are not on the energy-march path
+    and not in this image (matplotlib, pymedphys): empty stand-ins take their
+    names; no reference code is changed."""
+    import types
+    os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/pdm1_numba_cache")
+    for name in ("matplotlib", "matplotlib.pyplot", "matplotlib.lines", "matplotlib.patches",
+                 "mpl_toolkits", "mpl_toolkits.mplot3d", "mpl_toolkits.mplot3d.art3d", "pymedphys"):
+        sys.modules.setdefault(name, types.ModuleType(name))
+    sys.modules["matplotlib.lines"].Line2D = object
+    sys.modules["matplotlib.patches"].Patch = object
+    sys.modules["mpl_toolkits.mplot3d.art3d"].Poly3DCollection = object
+    if str(REF_LIB) not in sys.path:
+        sys.path.insert(0, str(REF_LIB))
+    import proton_solver
+    return proton_solver
+
+
+def reference_material_map(cfg, mm):
+    """The reference's MaterialMap of a workload's phantom, built from its
+    voxel ids (``mm``; None: voxelised from ``cfg.geometry``).  Materials are
+    keyed by Geant4 name, the key of the reference's coefficient tables
+    (physics/materials.py:26-60): its Material enum lists only water, compact
+    bone and lung, and its data/ tables also hold skeletal muscle and air.
+    ADIPOSE_SYNTH (water scaled to 950 kg/m3, no reference table) marches as
+    water."""
+    import enum
+    from proton_solver.physics.materials import MaterialMap as RefMap
+    from proton_dose_m1_b200.numerics.grid import Grid
+    from proton_dose_m1_b200.physics.materials import MaterialMap
+    if mm is None:
+        mm = MaterialMap.from_geometry(cfg.geometry, Grid.from_geometry(cfg.geometry))
+    names = ["G4_WATER" if m.value == "ADIPOSE_SYNTH" else m.value for m in mm.materials]
+    uniq = list(dict.fromkeys(names))
+    G4 = enum.Enum("G4", {n: n for n in uniq})
+    remap = np.array([uniq.index(n) for n in names], dtype=np.int32)
+    return RefMap(ids=np.ascontiguousarray(remap[np.asarray(mm.ids)]), materials=tuple(G4(n) for n in uniq))
+
+
+def reference_spot(ps, cfg):
+    """The reference's own (config, grid, inflow) for one spot of a workload,
+    on its moving active box."""
+    from proton_solver.numerics.boundary import BeamInflow as RefInflow
+    from proton_solver.numerics.grid import Grid as RefGrid
+    b, n = cfg.beam, cfg.numerics
+    beam = ps.Beam(n_protons=b.n_protons, energy=b.energy, energy_spread=b.energy_spread,
+                   sigma=tuple(b.sigma), center=tuple(b.center), angular_spread=b.angular_spread,
+                   cutoff_sigma=b.cutoff_sigma)
+    rcfg = ps.SolverConfig(
+        geometry=ps.Geometry(size=tuple(cfg.geometry.size), resolution=tuple(cfg.geometry.resolution)),
+        beam=beam,
+        physics=ps.Physics(scattering=ps.Scattering[cfg.physics.scattering.name],
+                           nuclear=cfg.physics.nuclear),
+        numerics=ps.Numerics(energy_scheme=ps.EnergyScheme[n.energy_scheme.name], cfl=n.cfl,
+                             max_energy_step=n.max_energy_step, moving_active_domain=True),
+        backend=ps.Backend.CPU, references=ps.References(reference=ps.Reference.NONE))
+    grid = RefGrid.from_geometry(rcfg.geometry, np)
+    return rcfg, grid, RefInflow.from_beam(beam, grid, np)
+
+
+def _reference_warm_inputs(ps):
+    """(config, grid, material map, inflow) of a small problem with the
+    workloads' physics and scheme (24x24x60 at 1 mm, water with a compact-bone
+    block, 45 MeV): marching it compiles every Numba kernel of the reference's
+    moving march, untimed."""
+    from proton_dose_m1_b200 import Beam, Box, Geometry, Numerics, Physics, SolverConfig
+    from proton_dose_m1_b200.enums import EnergyScheme, Material, Scattering
+    cfg = SolverConfig(
+        geometry=Geometry(size=(0.024, 0.024, 0.06), resolution=(24, 24, 60),
+                          objects=[Box(-0.012, 0.012, -0.012, 0.012, 0.01, 0.014, Material.BONE_COMPACT)]),
+        beam=Beam(n_protons=1e6, energy=45.0, energy_spread=1.0, sigma=(0.003, 0.003)),
+        physics=Physics(scattering=Scattering.WENTZEL, nuclear=True),
+        numerics=Numerics(energy_scheme=EnergyScheme.IF_SSPRK3, cfl=0.9, max_energy_step=0.5))
+    rcfg, grid, inflow = reference_spot(ps, cfg)
+    return rcfg, grid, reference_material_map(cfg, None), inflow
+
+
+def _reference_worker(workload_name, n_spots, warmup, barrier, todo, done):
+    """One reference worker process: build the spots' inputs and compile the
+    reference (untimed), wait for the others, then march complete spots from
+    ``todo`` with the reference's own energy_march until it is empty."""
+    try:
+        ps = import_installed_reference()
+        from proton_solver.numerics.energy import energy_march as reference_march
+        sample = reference_sample(workload_name, n_spots)
+        warm = _reference_warm_inputs(ps)
+        for _ in range(max(1, warmup)):
+            reference_march(None, warm[2], warm[1], warm[3], warm[0], np)
+        # fields share one phantom: one material map for all their spots
+        ref_map = reference_material_map(sample[0][0], sample[0][1])
+        inputs = [(*reference_spot(ps, cfg), ref_map) for cfg, _, _ in sample]
+    except BaseException as exc:   # tell the parent instead of leaving it waiting
+        barrier.abort()
+        done.put(("error", repr(exc)))
+        return
+    barrier.wait()
+    while True:
+        k = todo.get()
+        if k is None:
+            return
+        rcfg, grid, inflow, rmm = inputs[k]
+        t0 = time.perf_counter()
+        _, dose, energies, _ = reference_march(None, rmm, grid, inflow, rcfg, np)
+        done.put((k, len(energies) - 1, time.perf_counter() - t0, float(dose.max())))
+
+
 def run_reference(args, rank, world):
-    """The oracle (CPU restatement of the reference path) on the host cores:
-    every timed step marches one complete spot of the workload on the
-    reference's moving active box; the K spots run concurrently over the
-    cores (spot-level parallelism on top of the oracle's OpenMP loops)."""
+    """The reference's CPU path on the host cores, rank 0 only: every timed
+    step marches one complete spot of the workload on the reference's moving
+    active box (its fastest CPU mode, numerics/energy.py:1262-1494, with its
+    own CFL rule).  The unmodified reference (Numba) when it is installed under
+    baseline/_ref, else the oracle."""
     if rank != 0:
         return
+    if reference_installed():
+        run_reference_numba(args, world)
+    else:
+        run_reference_port(args, world)
+
+
+def run_reference_port(args, world):
+    """The oracle (CPU restatement of the reference path) on the host cores:
+    the K spots run concurrently over the cores (spot-level parallelism on top
+    of the oracle's OpenMP loops)."""
     desc = FIELDS[args.workload]["desc"] if args.workload in FIELDS else workload(args.workload)[1]
     sample = reference_sample(args.workload, args.steps)
     workers, tpw = host_split(len(sample))
@@ -338,6 +476,77 @@ def run_reference(args, rank, world):
                                    f"{[r[1] for r in rows]} energy steps; "
                                    f"{[round(r[2], 1) for r in rows]} s each), {workers} at a time x "
                                    f"{tpw} OpenMP threads, {wall:.1f} s wall"},
+        "e2e": {"value": value, "unit": "spots/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_reference_numba(args, world):
+    """The unmodified reference's Numba march (its own energy_march, moving
+    active box) in ``cores / 4`` spawned worker processes of 4 Numba threads
+    each.  The workers build their inputs and compile the reference before the
+    clock starts; the K spots go out largest energy first to whichever worker
+    is free, and ``value`` = K / the wall time until the last one is done."""
+    import multiprocessing as mp
+    import queue
+    desc = FIELDS[args.workload]["desc"] if args.workload in FIELDS else workload(args.workload)[1]
+    k_spots = args.steps
+    cores = os.cpu_count() or 1
+    threads = min(REF_THREADS_PER_WORKER, cores)
+    workers = max(1, min(k_spots, cores // threads))
+    # Numba reads its thread count when it is first imported: the spawned
+    # workers inherit it from this environment
+    os.environ["NUMBA_NUM_THREADS"] = str(threads)
+    os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/pdm1_numba_cache")
+    ctx = mp.get_context("spawn")
+    barrier = ctx.Barrier(workers + 1)
+    todo, done = ctx.Queue(), ctx.Queue()
+    energies = [e for _, _, e in reference_sample(args.workload, k_spots)]
+    for k in sorted(range(k_spots), key=lambda i: -energies[i]):
+        todo.put(k)
+    for _ in range(workers):
+        todo.put(None)
+    procs = [ctx.Process(target=_reference_worker, args=(args.workload, k_spots, args.warmup, barrier, todo, done),
+                         daemon=True) for _ in range(workers)]
+    for p in procs:
+        p.start()
+    try:
+        barrier.wait(timeout=1800)
+    except Exception:
+        err = done.get(timeout=5) if not done.empty() else ("error", "a reference worker did not start")
+        raise SystemExit(f"reference workers failed before timing: {err[1]}")
+    t0 = time.perf_counter()
+    rows = {}
+    while len(rows) < k_spots:
+        try:
+            item = done.get(timeout=30)
+        except queue.Empty:
+            if not all(p.is_alive() for p in procs) and done.empty():
+                raise SystemExit("a reference worker exited before marching its spots")
+            continue
+        if item[0] == "error":
+            raise SystemExit(f"reference worker failed: {item[1]}")
+        rows[item[0]] = item[1:]
+    wall = time.perf_counter() - t0
+    for p in procs:
+        p.join(timeout=60)
+    value = k_spots / wall
+    order = range(k_spots)
+    sample = (f"{k_spots} complete moving-box spot marches of the unmodified reference "
+              f"(proton_solver energy_march, Numba, NUMBA_NUM_THREADS={threads}), one per timed step: "
+              f"energies {[round(energies[k], 1) for k in order]} MeV, "
+              f"{[rows[k][0] for k in order]} energy steps, {[round(rows[k][1], 1) for k in order]} s each; "
+              f"{workers} worker processes at a time, {wall:.1f} s wall after JIT warm-up"
+              + ("; ADIPOSE_SYNTH marched as water (no reference table)" if args.workload == "pelvis1024" else ""))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "spots/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": wall / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "strong" if args.workload in FIELDS else "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded phantom, no dataset)",
+        "config": {"workload": args.workload, "description": desc},
+        "cpu_baseline": {"value": value, "unit": "spots/s", "cores": workers * threads, "kind": "reference",
+                         "sample": sample},
         "e2e": {"value": value, "unit": "spots/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
