@@ -7,7 +7,8 @@
 # baseline/_ref/data: the package finds its tables three directories above its
 # physics modules, which is baseline/_ref/data for this layout.  Only the four
 # tables the energy march reads are copied (materials.csv, stopping_power,
-# nuclear_attenuation, wentzel_transport; not the CT volumes).
+# nuclear_attenuation, wentzel_transport; not the CT volumes), and
+# baseline/synth_tables.py adds this library's synthetic materials to them.
 #
 # The install is offline (--no-index, the image's wheelhouse).  --no-deps: the
 # reference pins matplotlib>=3.11.1, numba>=0.67 and numpy>=2.4.6, which the
@@ -29,4 +30,6 @@ mkdir -p "$here/_ref/data"
 for t in materials.csv stopping_power nuclear_attenuation wentzel_transport; do
     cp -r "$src/data/$t" "$here/_ref/data/"
 done
+# this library's synthetic materials (ADIPOSE_SYNTH), in the reference's table formats
+python "$here/synth_tables.py" "$here/_ref/data"
 echo "reference installed under $here/_ref"

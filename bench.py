@@ -348,18 +348,21 @@ def import_installed_reference():
 def reference_material_map(cfg, mm):
     """The reference's MaterialMap of a workload's phantom, built from its
     voxel ids (``mm``; None: voxelised from ``cfg.geometry``).  Materials are
-    keyed by Geant4 name, the key of the reference's coefficient tables
+    keyed by table name, the key of the reference's coefficient tables
     (physics/materials.py:26-60): its Material enum lists only water, compact
     bone and lung, and its data/ tables also hold skeletal muscle and air.
-    ADIPOSE_SYNTH (water scaled to 950 kg/m3, no reference table) marches as
-    water."""
+    ADIPOSE_SYNTH (water scaled to 950 kg/m3) takes the tables that
+    baseline/synth_tables.py wrote into the installed data, or, where they
+    are missing, marches as water."""
     import enum
     from proton_solver.physics.materials import MaterialMap as RefMap
     from proton_dose_m1_b200.numerics.grid import Grid
     from proton_dose_m1_b200.physics.materials import MaterialMap
     if mm is None:
         mm = MaterialMap.from_geometry(cfg.geometry, Grid.from_geometry(cfg.geometry))
-    names = ["G4_WATER" if m.value == "ADIPOSE_SYNTH" else m.value for m in mm.materials]
+    data = REF_LIB.parent / "data"
+    names = [m.value if m.value != "ADIPOSE_SYNTH" or (data / "stopping_power" / f"{m.value}.csv").exists()
+             else "G4_WATER" for m in mm.materials]
     uniq = list(dict.fromkeys(names))
     G4 = enum.Enum("G4", {n: n for n in uniq})
     remap = np.array([uniq.index(n) for n in names], dtype=np.int32)
@@ -532,12 +535,14 @@ def run_reference_numba(args, world):
         p.join(timeout=60)
     value = k_spots / wall
     order = range(k_spots)
+    adipose = (REF_LIB.parent / "data" / "stopping_power" / "ADIPOSE_SYNTH.csv").exists()
     sample = (f"{k_spots} complete moving-box spot marches of the unmodified reference "
               f"(proton_solver energy_march, Numba, NUMBA_NUM_THREADS={threads}), one per timed step: "
               f"energies {[round(energies[k], 1) for k in order]} MeV, "
               f"{[rows[k][0] for k in order]} energy steps, {[round(rows[k][1], 1) for k in order]} s each; "
               f"{workers} worker processes at a time, {wall:.1f} s wall after JIT warm-up"
-              + ("; ADIPOSE_SYNTH marched as water (no reference table)" if args.workload == "pelvis1024" else ""))
+              + (f"; ADIPOSE_SYNTH shell {'on the tables of baseline/synth_tables.py' if adipose else 'marched as water'}"
+                 if args.workload == "pelvis1024" else ""))
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "spots/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,

@@ -1,12 +1,12 @@
 """The benchmark's reference arm: the unmodified reference, installed under
 baseline/_ref by baseline/install_reference.sh, given this library's inputs.
 
-Its own moving-box march (numerics/energy.py:1262-1494) of a small phantom with
-water, compact bone and skeletal muscle is compared with the oracle's march of
-the same inputs: the same energy steps and the dose within the parity bar.
-This checks the conversion bench.py makes (material map by Geant4 name, beam,
-physics, numerics) on the path its timing runs.  Skipped where the reference
-is not installed.
+Its own moving-box march (numerics/energy.py:1262-1494) of a small phantom of
+water, compact bone, skeletal muscle and synthetic adipose is compared with the
+oracle's march of the same inputs: the same energy steps and the dose within
+the parity bar.  This checks the conversion bench.py makes (material map by
+table name, beam, physics, numerics, the synthetic adipose tables) on the path
+its timing runs.  Skipped where the reference is not installed.
 """
 
 from __future__ import annotations
@@ -27,8 +27,10 @@ def _phantom():
     ids = np.zeros((16, 14, 40), dtype=np.int32)
     ids[:, :, 12:16] = 1                  # compact-bone slab across the beam
     ids[9:, :, 20:] = 2                   # muscle block beside the axis, deeper
+    ids[:, :, :3] = 3                     # adipose entrance layer (this library's synthetic table)
     geo = Geometry.from_ids((0.016, 0.014, 0.04), ids,
-                            (Material.WATER, Material.BONE_COMPACT, Material.MUSCLE_SKELETAL))
+                            (Material.WATER, Material.BONE_COMPACT, Material.MUSCLE_SKELETAL,
+                             Material.ADIPOSE_SYNTH))
     cfg = SolverConfig(
         geometry=geo,
         beam=Beam(n_protons=1e6, energy=40.0, energy_spread=1.0, sigma=(0.002, 0.0025), center=(0.001, -0.0005)),
@@ -40,12 +42,35 @@ def _phantom():
     return cfg, MaterialMap.from_geometry(geo, Grid.from_geometry(geo))
 
 
-def test_reference_material_map_keys_tables_by_geant4_name():
+def test_reference_material_map_keys_tables_by_name():
     bench.import_installed_reference()
     cfg, mm = _phantom()
     rmm = bench.reference_material_map(cfg, mm)
-    assert [m.value for m in rmm.materials] == ["G4_WATER", "G4_BONE_COMPACT_ICRU", "G4_MUSCLE_SKELETAL_ICRP"]
+    assert [m.value for m in rmm.materials] == ["G4_WATER", "G4_BONE_COMPACT_ICRU", "G4_MUSCLE_SKELETAL_ICRP",
+                                                "ADIPOSE_SYNTH"]
     assert np.array_equal(rmm.ids, mm.ids)
+
+
+def test_synthetic_tables_read_back_exactly():
+    """The reference's own loaders read the ADIPOSE_SYNTH tables back as the
+    same doubles this library marches with."""
+    bench.import_installed_reference()
+    from proton_solver.physics.materials import density, radiation_length
+    from proton_solver.physics.nuclear import _load_nuclear_table
+    from proton_solver.physics.scattering import _load_transport_table
+    from proton_solver.physics.stopping_power import load_stopping_power_table
+    from proton_dose_m1_b200.physics.tables import material_tables
+    cfg, mm = _phantom()
+    adipose = bench.reference_material_map(cfg, mm).materials[3]
+    t = material_tables("ADIPOSE_SYNTH")
+    sp = load_stopping_power_table(adipose)
+    assert np.array_equal(sp["energy_mev"], t.sp_energy)
+    assert np.array_equal(sp["electronic_stopping_power_mev_per_m"], t.sp_value)
+    e, v = _load_transport_table(adipose)
+    assert np.array_equal(e, t.tr_energy) and np.array_equal(v, t.tr_value)
+    e, v = _load_nuclear_table(adipose)[:2]
+    assert np.array_equal(e, t.nuc_energy) and np.array_equal(v, t.nuc_value)
+    assert density(adipose) == t.density and radiation_length(adipose) == t.radiation_length
 
 
 def test_reference_march_of_converted_inputs_matches_the_oracle():
