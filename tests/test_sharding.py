@@ -1,6 +1,6 @@
 """Spot sharding across ranks: the assignment on the host, and the sharded
-field sum with world_size 2 over gloo (CPU processes, a stand-in march that
-deposits a known pattern per spot)."""
+field sum over gloo (CPU processes): with a stand-in march that deposits a
+known pattern per spot, and with the oracle's march of a small field."""
 
 import os
 import socket
@@ -90,3 +90,70 @@ def test_sharded_field_sum_over_gloo(n_spots):
         np.testing.assert_allclose(dose, expect, rtol=1e-15, atol=0)
         shares += share
     assert sorted(shares) == list(range(n_spots))
+
+
+def _field():
+    """Three spots on a small water phantom with a bone slab (moving box)."""
+    from proton_dose_m1_b200 import Beam, Box, Geometry, Numerics, Physics, SolverConfig
+    from proton_dose_m1_b200.enums import EnergyScheme, Material, Scattering
+    geo = Geometry(size=(0.012, 0.010, 0.03), resolution=(12, 10, 30),
+                   objects=[Box(-0.006, 0.006, -0.005, 0.005, 0.006, 0.009, Material.BONE_COMPACT)])
+    beams = [Beam(n_protons=1e6, energy=e, energy_spread=1.0, sigma=(s, s), center=c)
+             for e, s, c in ((34.0, 0.0015, (-0.002, 0.0)), (40.0, 0.002, (0.0, 0.001)),
+                             (28.0, 0.0012, (0.002, -0.001)))]
+    cfg = SolverConfig(geometry=geo, beam=beams[0], physics=Physics(scattering=Scattering.WENTZEL, nuclear=True),
+                       numerics=Numerics(energy_scheme=EnergyScheme.IF_SSPRK3, cfl=0.9, max_energy_step=0.5,
+                                         moving_active_domain=True))
+    return cfg, beams
+
+
+def _oracle_spots(cfg, beams, idx):
+    from dataclasses import replace
+    from oracle.oracle import OracleProblem, set_threads
+    set_threads(1)   # one core per rank: the ranks share the host
+    out = np.zeros(tuple(cfg.geometry.resolution))
+    for k in idx:
+        out += OracleProblem(replace(cfg, beam=beams[k])).march(None)[1]
+    return out
+
+
+def _oracle_rank(rank, world, port, result):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        cfg, beams = _field()
+        grid = Grid.from_geometry(cfg.geometry)
+        costs = [spot_cost(b, cfg, grid) for b in beams]
+        dose, share = sharded_field_dose(beams, costs, rank, world,
+                                         lambda idx: torch.from_numpy(_oracle_spots(cfg, beams, idx)),
+                                         dist.all_reduce)
+        result[rank] = (dose.numpy().copy(), share)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 4])
+def test_sharded_field_of_oracle_marches_over_gloo(world):
+    """Each rank marches its share of a three-spot field with the oracle (the
+    CPU restatement of the march; the product marches it on the GPU); the
+    all-reduced field dose equals the sum of the single-spot marches.  With
+    four ranks one share is empty and its rank still takes the reduction."""
+    ctx = mp.get_context("spawn")
+    result = ctx.Manager().dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_oracle_rank, args=(r, world, port, result)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(300)
+        assert p.exitcode == 0
+    cfg, beams = _field()
+    expect = _oracle_spots(cfg, beams, range(len(beams)))
+    assert expect.max() > 0.0
+    shares = []
+    for r in range(world):
+        dose, share = result[r]
+        np.testing.assert_allclose(dose, expect, rtol=0, atol=1e-14 * expect.max())
+        shares += share
+    assert sorted(shares) == [0, 1, 2]
+    assert world < 4 or any(len(result[r][1]) == 0 for r in range(world))
