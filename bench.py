@@ -494,7 +494,8 @@ def run_reference_numba(args, world):
     import queue
     desc = FIELDS[args.workload]["desc"] if args.workload in FIELDS else workload(args.workload)[1]
     k_spots = args.steps
-    cores = os.cpu_count() or 1
+    # the CPUs this process may run on (a container can see more than it gets)
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
     threads = min(REF_THREADS_PER_WORKER, cores)
     workers = max(1, min(k_spots, cores // threads))
     # Numba reads its thread count when it is first imported: the spawned

@@ -26,8 +26,10 @@ import numpy as np
 from . import learned_box, metrics
 
 
-def march(config, box_model=None, moving=True, phantom_cfl=False):
-    """(dose, energy steps, cell-steps, grow events, fallbacks, seconds, grid)."""
+def march(config, box_model=None, moving=True, phantom_cfl=False, schedule=None, energies=None):
+    """(dose, energy steps, cell-steps, grow events, fallbacks, seconds, grid).
+    ``schedule``: march through these energies instead of the CFL steps;
+    ``energies``: a list that receives the march's energies."""
     import torch
     from .config import Accel, SolverConfig
     from .numerics.boundary import BeamInflow
@@ -41,6 +43,8 @@ def march(config, box_model=None, moving=True, phantom_cfl=False):
     grid = Grid.from_geometry(cfg.geometry)
     mm = MaterialMap.from_geometry(cfg.geometry, grid)
     plan = M1Plan(cfg, mm, grid, BeamInflow.from_beam(cfg.beam, grid))
+    if schedule is not None:
+        plan.set_schedule(schedule)
     U = None if moving else torch.zeros((4, *grid.shape), dtype=torch.float64, device="cuda")
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -49,6 +53,8 @@ def march(config, box_model=None, moving=True, phantom_cfl=False):
     dt = time.perf_counter() - t0
     info = plan.last_info
     plan.close()
+    if energies is not None:
+        energies.extend(float(e) for e in E)
     return dose, len(E) - 1, info.cell_steps, info.box_grow_events, info.box_fallbacks, dt, grid
 
 
@@ -89,6 +95,52 @@ def evaluate(model, seeds, phantom_cfl=False):
     return rows
 
 
+def interface_case():
+    """The reference's extended lateral-interface case of its moving-box study
+    (thesis_results/robustness/moving_active_domain/scattering_nuclear/
+    transversal_slabs/weno_z/config.json): 100 x 100 x 400 cells on
+    24 x 24 x 200 mm, compact bone for x < 0 over the full depth, 150 MeV,
+    sigma 2 mm, sigma_E 1 MeV, Wentzel-VI + nuclear, WENO-Z/HLL/IF-SSPRK3,
+    cfl 0.9, max dE 0.25, on the reference's moving box (guard 9 cells,
+    truncation at 5 sigma).  FP64."""
+    from .beam import Beam
+    from .config import Numerics, Physics, SolverConfig
+    from .enums import EnergyScheme, Material, Scattering
+    from .geometry import Box, Geometry
+    return SolverConfig(
+        geometry=Geometry(size=(0.024, 0.024, 0.2), resolution=(100, 100, 400),
+                          objects=[Box(-0.012, 0.0, -0.012, 0.012, 0.0, 0.2, Material.BONE_COMPACT)]),
+        beam=Beam(n_protons=1e6, energy=150.0, energy_spread=1.0, sigma=(0.002, 0.002)),
+        physics=Physics(scattering=Scattering.WENTZEL, nuclear=True),
+        numerics=Numerics(energy_scheme=EnergyScheme.IF_SSPRK3, cfl=0.9, max_energy_step=0.25,
+                          moving_active_domain=True, active_guard_cells=9, active_truncation_sigma=5.0))
+
+
+def evaluate_interface(model):
+    """Heuristic and learned boxes on the extended lateral-interface case,
+    each against the full-domain march: on their own CFL steps, with the
+    phantom-wide CFL bound, and through the full-domain march's energies
+    (which separates the box's own error from the energy-step sequence)."""
+    cfg = interface_case()
+    full_E = []
+    full, n_full, cs_full, _, _, t_full, grid = march(cfg, moving=False, energies=full_E)
+    out = {"full": {"steps": n_full, "cell_steps": cs_full, "seconds": t_full}}
+    spacing = (grid.dx * 1e3, grid.dy * 1e3, grid.dz * 1e3)
+    m = float(full.max())
+    for box, bm in (("heuristic", None), ("learned", model)):
+        for mode, kw in (("own", {}), ("phantom_cfl", {"phantom_cfl": True}), ("full_energies", {"schedule": full_E})):
+            E = []
+            d, n, cs, grows, fb, t, _ = march(cfg, box_model=bm, energies=E, **kw)
+            out[f"{box}_{mode}"] = {
+                "steps": n, "cell_steps_vs_full": cs / cs_full, "grow_events": grows, "fallbacks": fb,
+                "seconds": t, "max_abs_diff_over_max": float((d - full).abs().max()) / m,
+                "max_dose_rel_diff": float(d.max()) / m - 1.0,
+                "gamma_1pct_1mm": metrics.gamma(d, full, spacing, 1.0, 1.0)[0],
+                "energies_equal_full": E == full_E}
+            print(json.dumps({f"{box}_{mode}": out[f"{box}_{mode}"]}), flush=True)
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--solves", type=int, default=200)
@@ -103,7 +155,15 @@ def main(argv=None):
     ap.add_argument("--rows", default=None, help="recorded rows: load from this npz if it exists, else save to it")
     ap.add_argument("--evaluate", default=None, help="only evaluate this model file on the test seeds")
     ap.add_argument("--phantom-cfl", action="store_true", help="evaluate with the phantom-wide CFL bound")
+    ap.add_argument("--interface-case", action="store_true",
+                    help="with --evaluate: the reference's extended lateral-interface case instead of the seeds")
     args = ap.parse_args(argv)
+    if args.evaluate and args.interface_case:
+        report = {"model": args.evaluate, "interface_case": evaluate_interface(learned_box.BoxModel.load(args.evaluate))}
+        if args.report:
+            with open(args.report, "w") as f:
+                json.dump(report, f, indent=1)
+        return report
     if args.evaluate:
         report = {"model": args.evaluate, "phantom_cfl": args.phantom_cfl,
                   "evaluation": evaluate(learned_box.BoxModel.load(args.evaluate), args.test_seeds,

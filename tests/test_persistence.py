@@ -79,3 +79,16 @@ def test_solver_refuses_reference_solutions_it_does_not_hold():
                        references=References(reference=Reference.ANALYTICAL))
     with pytest.raises(ValueError, match="Analytical reference is not available"):
         Solver(cfg).solve()
+
+
+def test_interface_case_is_the_published_lateral_interface_run():
+    """The box study's extended lateral-interface case (train_box_model
+    --interface-case) has the geometry, beam, physics and numerics of the
+    reference's own published moving-box run."""
+    from proton_dose_m1_b200.train_box_model import interface_case
+    src = "thesis_results/robustness/moving_active_domain/scattering_nuclear/transversal_slabs/weno_z"
+    run = next(r for r in _published() if r["source"] == src)
+    published = cases.published_config(run)
+    mine = interface_case()
+    for part in ("geometry", "beam", "physics", "numerics"):
+        assert getattr(mine, part) == getattr(published, part), part
