@@ -317,6 +317,8 @@ REF_LIB = ROOT / "baseline" / "_ref" / "lib"
 # scale poorly past ~4 threads (a 89.5 MeV pelvis spot: 18.9 s on 4 threads,
 # 16.9 s on 8), so several spots at once on 4 threads each use the cores better.
 REF_THREADS_PER_WORKER = 4
+# seconds between the reference arm's checks on its workers while it waits
+REF_POLL_S = 30.0
 
 
 def reference_installed() -> bool:
@@ -523,10 +525,15 @@ def run_reference_numba(args, world):
     rows = {}
     while len(rows) < k_spots:
         try:
-            item = done.get(timeout=30)
+            item = done.get(timeout=REF_POLL_S)
         except queue.Empty:
-            if not all(p.is_alive() for p in procs) and done.empty():
-                raise SystemExit("a reference worker exited before marching its spots")
+            # a worker with no spot left exits with status 0 while the others
+            # still march: only a failed worker, or all of them gone with
+            # spots missing, ends the run
+            if any(p.exitcode not in (None, 0) for p in procs):
+                raise SystemExit("a reference worker failed while marching")
+            if all(p.exitcode is not None for p in procs) and done.empty():
+                raise SystemExit("the reference workers exited before marching every spot")
             continue
         if item[0] == "error":
             raise SystemExit(f"reference worker failed: {item[1]}")

@@ -87,3 +87,21 @@ def test_reference_march_of_converted_inputs_matches_the_oracle():
     scale = float(np.max(dose_r))
     assert scale > 0.0
     assert float(np.max(np.abs(np.asarray(dose_o) - dose_r))) <= reference_rtol(cfg) * scale
+
+
+def test_reference_arm_waits_for_the_last_spots(monkeypatch, capsys):
+    """Three spots on two workers, polled every half second: one worker runs
+    out of spots and exits while the other still marches; the arm waits for
+    it and prints one line with every spot."""
+    import argparse
+    import json
+    import os
+    if len(os.sched_getaffinity(0)) < 2 * bench.REF_THREADS_PER_WORKER:
+        pytest.skip("needs two reference workers")
+    monkeypatch.setattr(bench, "REF_POLL_S", 0.5)
+    args = argparse.Namespace(workload="water40", steps=3, warmup=1)
+    bench.run_reference_numba(args, 1)
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["cpu_baseline"]["kind"] == "reference"
+    assert line["value"] > 0.0 and line["steps"] == 3
+    assert "[458, 458, 458] energy steps" in line["cpu_baseline"]["sample"]
