@@ -104,4 +104,8 @@ def test_reference_arm_waits_for_the_last_spots(monkeypatch, capsys):
     line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
     assert line["impl"] == "reference" and line["cpu_baseline"]["kind"] == "reference"
     assert line["value"] > 0.0 and line["steps"] == 3
-    assert "[458, 458, 458] energy steps" in line["cpu_baseline"]["sample"]
+    # three marches of the same spot on the same thread count; the count itself
+    # (458 here) may move by a step with the host CPU's evaluation order
+    import re
+    steps = json.loads(re.search(r"(\[[0-9, ]+\]) energy steps", line["cpu_baseline"]["sample"]).group(1))
+    assert len(steps) == 3 and len(set(steps)) == 1 and 440 <= steps[0] <= 480
