@@ -109,3 +109,26 @@ def test_reference_arm_waits_for_the_last_spots(monkeypatch, capsys):
     import re
     steps = json.loads(re.search(r"(\[[0-9, ]+\]) energy steps", line["cpu_baseline"]["sample"]).group(1))
     assert len(steps) == 3 and len(set(steps)) == 1 and 440 <= steps[0] <= 480
+
+
+def test_pelvis_spot_through_the_reference_energies():
+    """A spot of the benchmark's pelvis field (256x256x320 at 1 mm, the
+    synthetic adipose shell on its written tables; 89.5 MeV, the lowest of four
+    energy quantiles), marched by the reference on its moving box and by the
+    oracle through the reference's own energies: the dose within the parity
+    bar.  (With the CFL rule the two step sequences part by ~1e-11 MeV after a
+    few steps: the bound's sensitivity to evaluation order.)"""
+    from oracle.oracle import OracleProblem
+    ps = bench.import_installed_reference()
+    from proton_solver.numerics.energy import energy_march as reference_march
+    cfg, mm, _ = bench.reference_sample("pelvis1024", 4)[0]
+    rcfg, grid, inflow = bench.reference_spot(ps, cfg)
+    _, dose_r, energies_r, _ = reference_march(None, bench.reference_material_map(cfg, mm), grid, inflow, rcfg, np)
+    energies_r = np.asarray(energies_r)
+    prob = OracleProblem(cfg, mm)
+    prob.set_schedule(energies_r)
+    _, dose_o, energies_o, _ = prob.march(None)
+    assert np.array_equal(np.asarray(energies_o), energies_r)
+    scale = float(np.max(dose_r))
+    assert scale > 0.0
+    assert float(np.max(np.abs(np.asarray(dose_o) - dose_r))) <= reference_rtol(cfg) * scale
