@@ -519,8 +519,11 @@ def run_reference_numba(args, world):
     try:
         barrier.wait(timeout=1800)
     except Exception:
-        err = done.get(timeout=5) if not done.empty() else ("error", "a reference worker did not start")
-        raise SystemExit(f"reference workers failed before timing: {err[1]}")
+        try:   # a failed worker's message may still be on its way
+            err = done.get(timeout=30)[1]
+        except queue.Empty:
+            err = "a reference worker did not reach the start"
+        raise SystemExit(f"reference workers failed before timing: {err}")
     t0 = time.perf_counter()
     rows = {}
     while len(rows) < k_spots:
